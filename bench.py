@@ -1,0 +1,498 @@
+#!/usr/bin/env python
+"""Benchmark: batched grid-kNN queries/s at K=16 on one B200.
+
+Workload (BASELINE configuration "batched uneven sizes"): 16 synthetic
+clouds, room-like and LiDAR-like alternately, point counts log-uniform in
+[20k, 200k] (1.464M points), offset-concatenated, self query, K=16, 5 cm
+voxels, parent cell = 4 voxels.  One step = one pass of the whole path over
+the batch: grid construction + candidate gather + top-K + remap, replayed
+from a CUDA graph, inputs already in HBM.  L2 is flushed (256 MiB memset)
+before every timed step, outside its events.
+
+Also reported on the same line: ``e2e`` (the public ``knn_query`` call with
+host buffers, H2D and D2H inside the timed region), the loop of plain
+per-cloud calls, forward+backward time, the query kernel's roofline and the
+CPU oracle timed on the host cores.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--k 16]
+Under torchrun every rank takes a share of the clouds (whole clouds, largest
+first onto the least-loaded rank); there is no collective in the data path.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+L2_FLUSH_BYTES = 256 << 20
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--k", type=int, default=16)
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the per-cloud, fwd+bwd and CPU-baseline legs")
+    return ap.parse_args()
+
+
+# ----------------------------------------------------------------- helpers
+
+def shard_clouds(counts, world):
+    """Greedy longest-first assignment of whole clouds to ranks."""
+    load = [0] * world
+    owner = [0] * len(counts)
+    for c in sorted(range(len(counts)), key=lambda i: -int(counts[i])):
+        r = min(range(world), key=lambda j: load[j])
+        owner[c] = r
+        load[r] += int(counts[c])
+    return owner
+
+
+def take_clouds(batch, ids):
+    starts = np.concatenate([[0], batch.offsets[:-1]])
+    parts = [batch.xyz[starts[i]:batch.offsets[i]] for i in ids]
+    counts = np.array([len(p) for p in parts], np.int64)
+    xyz = np.ascontiguousarray(np.concatenate(parts)) if parts else np.zeros((0, 3), np.float32)
+    return xyz, np.cumsum(counts)
+
+
+class ClockSampler:
+    """nvidia-smi samples (SM clock, max clock, throttle reasons) while running."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, ValueError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx.append(float(parts[1]))
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[4:8]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peak_hbm():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def cpu_cores():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def cpu_oracle_rate(xyz, offsets, k, voxel, budget_s=20.0):
+    """The oracle (C restatement of the reference path, OpenMP on every host
+    core) on a bounded sample: whole clouds, largest prefix of the batch that
+    fits the time budget after one probe run on the first cloud."""
+    from oracle import oracle as O
+    cores = cpu_cores()
+    starts = np.concatenate([[0], offsets[:-1]])
+    t0 = time.perf_counter()
+    O.knn_offsets(xyz[: offsets[0]], offsets[:1], k, voxel, 2, nthreads=cores)
+    per_point = (time.perf_counter() - t0) / max(int(offsets[0]), 1)
+    take = 1
+    while take < len(offsets) and per_point * offsets[take] < budget_s * 0.5:
+        take += 1
+    sub_xyz = xyz[: offsets[take - 1]]
+    sub_off = offsets[:take]
+    t0 = time.perf_counter()
+    O.knn_offsets(sub_xyz, sub_off, k, voxel, 2, nthreads=cores)
+    dt = time.perf_counter() - t0
+    n = int(sub_off[-1])
+    return {"value": n / dt, "unit": "queries/s", "cores": cores, "kind": "port",
+            "sample": f"first {take} of {len(offsets)} clouds ({n} points, construction + "
+                      f"query), one pass, OpenMP x{cores}", "seconds": dt}
+
+
+# --------------------------------------------------------------- our arm
+
+def run_ours(args, rank, world, local_rank, dist):
+    import torch
+
+    import flashknn_exprepo_b200 as fk
+    from flashknn_exprepo_b200 import _lib, synthetic
+
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    k = args.k
+    batch = synthetic.uneven_batch()
+    voxel = synthetic.C4_VOXEL
+    # Weak scaling: the job is `world` copies of the 16-cloud batch; whole
+    # clouds are assigned to ranks, largest first onto the least-loaded rank.
+    job_counts = np.tile(batch.counts, world)
+    owner = shard_clouds(job_counts, world)
+    mine = [c % len(batch.counts) for c in range(len(job_counts)) if owner[c] == rank]
+    xyz_h, off_h = take_clouds(batch, mine)
+    n = len(xyz_h)
+    xyz = torch.from_numpy(xyz_h).to(dev)
+    off = torch.from_numpy(off_h).to(dev)
+    lib = _lib.load()
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
+
+    # --- capture the batched pipeline in a CUDA graph
+    stream = torch.cuda.Stream(dev)
+    stream.wait_stream(torch.cuda.current_stream(dev))
+    with torch.cuda.stream(stream):
+        fk.ops.knn_offsets(xyz, off, k, voxel, 2)  # workspace sized, kernels loaded
+        torch.cuda.synchronize(dev)
+        launches_per_step = fk.ops.last_launch_count()
+        lib.fknn_profile_enable(1)
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph, stream=stream):
+            idx_g, dist_g = fk.ops.knn_offsets(xyz, off, k, voxel, 2)
+    torch.cuda.current_stream(dev).wait_stream(stream)
+    torch.cuda.synchronize(dev)
+
+    prof_buf = ctypes_float_array(1)
+    for _ in range(args.warmup):
+        graph.replay()
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        dist.barrier()
+    step_ms, kern_ms = [], []
+    with ClockSampler(local_rank) as clocks:
+        for _ in range(args.steps):
+            flush.zero_()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            graph.replay()
+            e1.record()
+            e1.synchronize()
+            step_ms.append(e0.elapsed_time(e1))
+            if lib.fknn_profile_read(ctypes.cast(prof_buf, ctypes.c_void_p), 1) == 1:
+                kern_ms.append(prof_buf[0])
+    torch.cuda.synchronize(dev)
+    lib.fknn_profile_enable(0)
+    total_ms = sum(step_ms)
+    if world > 1:
+        t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+        q = torch.tensor([n], dtype=torch.int64, device=dev)
+        dist.all_reduce(q)
+        total_queries = int(q.item())
+        dist.barrier()
+    else:
+        total_queries = n
+    value = total_queries * args.steps / (total_ms / 1e3)
+
+    # parity of the timed graph against a fresh eager call
+    ei, ed = fk.ops.knn_offsets(xyz, off, k, voxel, 2, validate=True)
+    graph_matches = bool(torch.equal(ei, idx_g) and torch.equal(ed, dist_g))
+
+    out = {"value": value, "ms_per_step": total_ms / args.steps, "n_points": total_queries,
+           "clocks": clocks.summary(), "kernel_ms": kern_ms, "launches_per_step": launches_per_step,
+           "graph_matches_eager": graph_matches, "local_n": n}
+    del graph
+
+    # --- e2e through the public API: pinned host in, pinned host out
+    xyz_pin = torch.from_numpy(xyz_h).pin_memory()
+    off_pin = torch.from_numpy(off_h).pin_memory()
+    idx_pin = torch.empty((n, k), dtype=torch.int32).pin_memory()
+    dist_pin = torch.empty((n, k), dtype=torch.float32).pin_memory()
+
+    def e2e_step():
+        x = xyz_pin.to(dev, non_blocking=True)
+        o = off_pin.to(dev, non_blocking=True)
+        i, d = fk.knn_query(k, x, o, voxel_size=voxel, num_down=2)
+        idx_pin.copy_(i, non_blocking=True)
+        dist_pin.copy_(d, non_blocking=True)
+
+    for _ in range(max(2, args.warmup)):
+        e2e_step()
+    torch.cuda.synchronize(dev)
+    e2e_ms = []
+    for _ in range(args.steps):
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        e2e_step()
+        e1.record()
+        e1.synchronize()
+        e2e_ms.append(e0.elapsed_time(e1))
+    e2e_total = sum(e2e_ms)
+    if world > 1:
+        t = torch.tensor([e2e_total], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_total = float(t.item())
+    out["e2e"] = {"value": total_queries * args.steps / (e2e_total / 1e3), "unit": "queries/s",
+                  "h2d_bytes_per_step": int(xyz_pin.numel() * 4 + off_pin.numel() * 8),
+                  "d2h_bytes_per_step": int(n * k * 8)}
+
+    if not args.no_extras and world == 1:
+        out.update(extras_single_gpu(args, fk, torch, dev, batch, voxel, flush))
+    return out
+
+
+def ctypes_float_array(n):
+    return (ctypes.c_float * n)()
+
+
+def extras_single_gpu(args, fk, torch, dev, batch, voxel, flush):
+    """Per-cloud loop, forward+backward, recall sample (rank 0, N=1)."""
+    from flashknn_exprepo_b200 import synthetic
+    k = args.k
+    res = {}
+    starts = np.concatenate([[0], batch.offsets[:-1]])
+    clouds = [torch.from_numpy(batch.xyz[s:e]).to(dev) for s, e in zip(starts, batch.offsets)]
+    offs = [torch.tensor([len(c)], dtype=torch.int64, device=dev) for c in clouds]
+
+    def per_cloud():
+        for c, o in zip(clouds, offs):
+            fk.ops.knn_offsets(c, o, k, voxel, 2)
+
+    for _ in range(2):
+        per_cloud()
+    torch.cuda.synchronize(dev)
+    reps = max(3, args.steps // 4)
+    ms = []
+    for _ in range(reps):
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        per_cloud()
+        e1.record()
+        e1.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    n = len(batch.xyz)
+    res["per_cloud"] = {"value": n * reps / (sum(ms) / 1e3), "unit": "queries/s",
+                        "ms_per_step": sum(ms) / reps,
+                        "what": "loop of 16 plain fknn_knn_offsets calls, one per cloud, eager"}
+
+    # forward + backward (loss = sum(w * d), w ~ N(0,1))
+    xyz = torch.from_numpy(batch.xyz).to(dev)
+    off = torch.from_numpy(batch.offsets).to(dev)
+    w = torch.from_numpy(synthetic.backward_weights(n, k)).to(dev)
+
+    def fwd_bwd():
+        x = xyz.detach().requires_grad_(True)
+        _, d = fk.knn_query(k, x, off, voxel_size=voxel, num_down=2)
+        (w * d.masked_fill(~torch.isfinite(d), 0)).sum().backward()
+        return x.grad
+
+    for _ in range(2):
+        fwd_bwd()
+    torch.cuda.synchronize(dev)
+    ms = []
+    for _ in range(reps):
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        fwd_bwd()
+        e1.record()
+        e1.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    res["fwd_bwd_ms"] = sum(ms) / reps
+    return res
+
+
+# ---------------------------------------------------------- reference arm
+
+def run_reference(args):
+    """CPU arm: the oracle port of the reference path on every host core,
+    plus (when a GPU and the sm_100a reference build are present) the
+    reference's own per-cloud GPU pipeline for context."""
+    from flashknn_exprepo_b200 import synthetic
+    batch = synthetic.uneven_batch()
+    k = args.k
+    voxel = synthetic.C4_VOXEL
+    rates = []
+    cpu = None
+    for _ in range(max(1, args.steps)):
+        cpu = cpu_oracle_rate(batch.xyz, batch.offsets, k, voxel,
+                              budget_s=max(2.0, 60.0 / max(1, args.steps)))
+        rates.append(cpu["value"])
+    value = statistics.median(rates)
+    line = {"impl": "reference", "metric": "kNN queries/s at K=16 (batched uneven 16-cloud, "
+                                           "construction + query)",
+            "value": value, "unit": "queries/s", "higher_is_better": True,
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "dtype": "f32", "data": "synthetic (seeded, stands in for S3DIS/SemanticKITTI)",
+            "config": {"workload": "uneven_batch_16clouds_k16", "n_points": int(len(batch.xyz)),
+                       "k": k, "voxel_m": voxel, "num_down": 2},
+            "cpu_baseline": {"value": value, "unit": "queries/s", "cores": cpu["cores"],
+                             "kind": cpu["kind"], "sample": cpu["sample"]},
+            "e2e": {"value": value, "unit": "queries/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    try:
+        line["reference_gpu_per_cloud"] = reference_gpu_per_cloud(batch, k, voxel)
+    except Exception as exc:  # context only: never fails the CPU arm
+        line["reference_gpu_per_cloud"] = {"unavailable": f"{type(exc).__name__}: {exc}"[:200]}
+    return line
+
+
+def reference_gpu_per_cloud(batch, k, voxel):
+    import torch
+    from oracle import ref_kernels, ref_pipeline
+    if not torch.cuda.is_available():
+        return {"unavailable": "no CUDA device"}
+    if not ref_kernels.available():
+        return {"unavailable": "reference kernels not built (oracle/build_ref.py)"}
+    cufun = ref_kernels.load()
+    dev = torch.device("cuda", 0)
+    starts = np.concatenate([[0], batch.offsets[:-1]])
+    clouds = []
+    for s, e in zip(starts, batch.offsets):
+        x = torch.from_numpy(batch.xyz[s:e]).to(dev)
+        g = torch.floor(x / voxel).long()
+        clouds.append((g, torch.zeros(len(x), dtype=torch.long, device=dev), x))
+    for g, b, x in clouds[:2]:
+        ref_pipeline.reference_query(cufun, g, b, x, k)
+    torch.cuda.synchronize()
+    reps = 3
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        for g, b, x in clouds:
+            ref_pipeline.reference_query(cufun, g, b, x, k)
+    dt = (time.perf_counter() - t0) / reps
+    return {"value": len(batch.xyz) / dt, "unit": "queries/s", "ms_per_step": dt * 1e3,
+            "what": "reference FlashKNN.query pipeline (ATen construction + "
+                    "FlashKNN_Query_Dynamic_Load built for sm_100a), one call per cloud, "
+                    "wall clock incl. its device synchronisations"}
+
+
+# -------------------------------------------------------------------- main
+
+def main():
+    args = parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        print(json.dumps(run_reference(args)))
+        return
+
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    try:
+        out = run_ours(args, rank, world, local_rank, dist)
+    finally:
+        if dist is not None:
+            dist.barrier()
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+
+    k = args.k
+    peak, peak_kind = measured_peak_hbm()
+    kern = out["kernel_ms"]
+    n_local = out["local_n"]
+    algo_bytes = n_local * (12 + 8 * k) + 8 * n_local
+    roofline = None
+    if kern:
+        avg = sum(kern) / len(kern)
+        achieved = algo_bytes / (avg * 1e-3) / 1e9
+        roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                    "frac": achieved / peak, "traffic": None,
+                    "kernel": "fknn::k_query<16>", "kernel_ms": avg,
+                    "algorithmic_bytes_per_launch": algo_bytes,
+                    "peak_source": f"{peak_kind} hbm_gbs"}
+    line = {
+        "metric": "kNN queries/s at K=16 (batched uneven 16-cloud, construction + query)",
+        "value": out["value"], "unit": "queries/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": out["ms_per_step"], "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded; stands in for S3DIS/SemanticKITTI crops)",
+        "config": {"workload": "uneven_batch_16clouds_k16", "n_points": out["n_points"],
+                   "n_clouds": 16, "k": k, "voxel_m": 0.05, "num_down": 2,
+                   "step": "CUDA-graph replay of construction + query",
+                   "l2": "flushed (256 MiB memset) before every timed step",
+                   "parallelism": f"{world} x 16 clouds, whole clouds per GPU, no collective"},
+        "e2e": out["e2e"], "gpu_launches": out["launches_per_step"] * args.steps,
+        "clocks": out["clocks"], "roofline": roofline,
+        "graph_matches_eager": out["graph_matches_eager"],
+    }
+    if "per_cloud" in out:
+        line["per_cloud"] = out["per_cloud"]
+        line["batched_vs_per_cloud"] = out["value"] / out["per_cloud"]["value"]
+    if "fwd_bwd_ms" in out:
+        line["fwd_bwd_ms"] = out["fwd_bwd_ms"]
+    if world == 1 and not args.no_extras:
+        from flashknn_exprepo_b200 import synthetic
+        b = synthetic.uneven_batch()
+        line["cpu_baseline"] = cpu_oracle_rate(b.xyz, b.offsets, k, synthetic.C4_VOXEL)
+        line["cpu_baseline"].pop("seconds", None)
+    print(json.dumps(line))
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

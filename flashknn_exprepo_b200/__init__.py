@@ -1,0 +1,20 @@
+"""FlashKNN-B200: grid k-nearest neighbours on sm_100a behind FlashKNN's API.
+
+Public entry points (mirroring the reference's ``FlashKNN/functions``):
+  FlashKNN              -- query / selected_query drop-in (wrapper.py)
+  knn_query, KNNQuery   -- Pointcept-style offset batching with a
+                           differentiable squared distance (pointops.py)
+  xyz2key               -- Morton keys (z_order.py)
+  BatchedKNNPlan        -- CUDA-graph captured batched query (plan.py)
+  ops                   -- tensor-level C-ABI calls, incl. the reference
+                           table ABI (query_tables, build_tables, ...)
+The CUDA library is libfknn.so next to this file (``python -m
+flashknn_exprepo_b200.build``); nothing falls back to the CPU.
+"""
+from . import ops
+from ._lib import FknnError
+from .pointops import KNNQuery, knn_query
+from .wrapper import FlashKNN
+from .z_order import xyz2key
+
+__all__ = ["FlashKNN", "KNNQuery", "knn_query", "xyz2key", "ops", "FknnError"]

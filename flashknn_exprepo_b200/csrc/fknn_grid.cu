@@ -1,0 +1,687 @@
+// Grid construction and the fused query pipelines (self / selected / general).
+//
+// The reference builds its tables with ~15 ATen calls and host syncs
+// (FlashKNN/functions/FlashKnnWrapper.py:220-337).  Here the whole pipeline
+// is a fixed sequence of launches with every data-dependent size kept on the
+// device, so it is CUDA-graph capturable:
+//
+//   k_init          zero the Meta block, empty the per-cloud boxes
+//   k_bbox          parent cell (grid >> num_down) and cloud of each point,
+//                   range checks, per-cloud bounding boxes (block-aggregated
+//                   atomics)
+//   k_meta          bits per axis of the translated parent coordinates
+//   k_keys          cell key = cloud << 3*bpa | morton(parent - cloud min)
+//   radix sort      stable LSD sort of (cell key, point id), only as many
+//                   8-bit passes as the key has significant bits
+//   k_gather        cell-sorted float4 records (x, y, z, point id) + cell
+//                   heads per 2048-point tile
+//   k_scan_tiles    tile offsets -> number of cells
+//   k_cells         cell keys and starts (cells stay in key order)
+//   k_runs          27 (start, count) candidate runs per cell / query group,
+//                   centre first, (0,-1,+1)^3 in ij order like the reference
+//                   neighbour table (flash_knn_construction.cu:42-63)
+//   k_items         work items (<= 32 queries of one group) for the query
+//                   kernel, allocated with warp-aggregated atomics
+//
+// Parent cells and their 3x3x3 adjacency are those of the reference: for grid
+// coordinates inside [-2^15, 2^15) the reference's key >> 3*num_down groups
+// exactly the points with equal grid >> num_down, and its neighbour lookup
+// finds exactly the integer-adjacent parent cells.  The per-cloud translation
+// only shortens the keys; it changes neither the cells nor their adjacency.
+#include <climits>
+
+#include "fknn_common.cuh"
+#include "fknn_internal.h"
+#include "fknn_sort.cuh"
+#include "fknn_grid.h"
+
+namespace fknn {
+
+// ---------------------------------------------------------------- sources
+
+struct PointSrc {
+  const float* xyz;        // f32 [n,3]
+  const int64_t* grid;     // int64 [n,3] or null: floor(xyz / voxel)
+  const int64_t* batch;    // int64 [n] or null
+  const int64_t* offsets;  // cumulative cloud ends or null
+  int64_t n_clouds;        // clouds addressable by this source
+  int64_t n;
+  float voxel;
+  int num_down;
+};
+
+__device__ __forceinline__ int grid_axis(const PointSrc& p, int64_t i, int a, int* status) {
+  int64_t g;
+  if (p.grid) {
+    g = p.grid[3 * i + a];
+  } else {
+    const float f = floorf(__fdiv_rn(p.xyz[3 * i + a], p.voxel));
+    if (!(f >= -32768.f && f <= 32767.f)) {
+      raise_status(status, kStatusRange);
+      return 0;
+    }
+    g = static_cast<int64_t>(f);
+  }
+  if (g < -32768 || g > 32767) {
+    raise_status(status, kStatusRange);
+    g = g < 0 ? -32768 : 32767;
+  }
+  return static_cast<int>(g);
+}
+
+__device__ __forceinline__ int cloud_of(const PointSrc& p, int64_t i, int* status) {
+  int64_t b = 0;
+  if (p.batch) {
+    b = p.batch[i];
+  } else if (p.offsets) {
+    int64_t lo = 0, hi = p.n_clouds;  // first cloud whose end exceeds i
+    while (lo < hi) {
+      const int64_t mid = (lo + hi) >> 1;
+      if (p.offsets[mid] > i) hi = mid; else lo = mid + 1;
+    }
+    b = lo;
+  }
+  if (b < 0 || b >= p.n_clouds) {
+    raise_status(status, kStatusBatch);
+    b = b < 0 ? 0 : p.n_clouds - 1;
+  }
+  return static_cast<int>(b);
+}
+
+// ------------------------------------------------------------------ init
+
+__global__ void k_init(Meta* meta, int* bbox, int64_t n_clouds, uint32_t* totals, int n_totals) {
+  const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  if (t < static_cast<int64_t>(sizeof(Meta) / sizeof(int))) reinterpret_cast<int*>(meta)[t] = 0;
+  for (int64_t i = t; i < n_clouds * 6; i += stride) bbox[i] = (i % 6) < 3 ? INT_MAX : INT_MIN;
+  for (int64_t i = t; i < n_totals; i += stride) totals[i] = 0u;
+}
+
+// ------------------------------------------------------------------ bbox
+
+struct Box6 {
+  int v[6];  // min x, y, z, max x, y, z
+  __device__ void reset() {
+    v[0] = v[1] = v[2] = INT_MAX;
+    v[3] = v[4] = v[5] = INT_MIN;
+  }
+  __device__ void add(int x, int y, int z) {
+    v[0] = min(v[0], x); v[1] = min(v[1], y); v[2] = min(v[2], z);
+    v[3] = max(v[3], x); v[4] = max(v[4], y); v[5] = max(v[5], z);
+  }
+};
+
+__device__ __forceinline__ void box_atomic(int* bbox, int b, const Box6& box) {
+  if (box.v[0] > box.v[3]) return;  // empty
+  int* dst = bbox + 6 * b;
+  atomicMin(dst + 0, box.v[0]); atomicMin(dst + 1, box.v[1]); atomicMin(dst + 2, box.v[2]);
+  atomicMax(dst + 3, box.v[3]); atomicMax(dst + 4, box.v[4]); atomicMax(dst + 5, box.v[5]);
+}
+
+// Block-wide reduction of a box; result valid in thread 0.
+__device__ __forceinline__ Box6 box_reduce(Box6 box, int (*sh)[6]) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    box.v[a] = __reduce_min_sync(kFull, box.v[a]);
+    box.v[a + 3] = __reduce_max_sync(kFull, box.v[a + 3]);
+  }
+  if (lane == 0)
+#pragma unroll
+    for (int a = 0; a < 6; ++a) sh[warp][a] = box.v[a];
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const int nw = blockDim.x >> 5;
+    for (int w = 1; w < nw; ++w) {
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        box.v[a] = min(box.v[a], sh[w][a]);
+        box.v[a + 3] = max(box.v[a + 3], sh[w][a + 3]);
+      }
+    }
+  }
+  __syncthreads();
+  return box;
+}
+
+// 256 threads x 8 points.  Writes the parent cell and cloud of every point
+// and grows the per-cloud boxes.  Most tiles hold one or two clouds (offset
+// batching): those are reduced in the block, other clouds go straight to
+// global atomics.
+__global__ void __launch_bounds__(256) k_bbox(PointSrc p, int4* __restrict__ pc,
+                                              int* __restrict__ bbox, Meta* meta) {
+  __shared__ int sh[8][6];
+  int* status = &meta->status;
+  const int64_t base = static_cast<int64_t>(blockIdx.x) * 2048;
+  const int64_t last = min(base + 2047, p.n - 1);
+  const int b_lo = cloud_of(p, base, status);
+  const int b_hi = cloud_of(p, last, status);
+  Box6 lo, hi;
+  lo.reset();
+  hi.reset();
+#pragma unroll 2
+  for (int r = 0; r < 8; ++r) {
+    const int64_t i = base + r * 256 + threadIdx.x;
+    if (i >= p.n) break;
+    const int gx = grid_axis(p, i, 0, status) >> p.num_down;
+    const int gy = grid_axis(p, i, 1, status) >> p.num_down;
+    const int gz = grid_axis(p, i, 2, status) >> p.num_down;
+    const int b = cloud_of(p, i, status);
+    pc[i] = make_int4(gx, gy, gz, b);
+    if (b == b_lo) {
+      lo.add(gx, gy, gz);
+    } else if (b == b_hi) {
+      hi.add(gx, gy, gz);
+    } else {
+      Box6 one;
+      one.reset();
+      one.add(gx, gy, gz);
+      box_atomic(bbox, b, one);
+    }
+  }
+  lo = box_reduce(lo, sh);
+  hi = box_reduce(hi, sh);
+  if (threadIdx.x == 0) {
+    box_atomic(bbox, b_lo, lo);
+    if (b_hi != b_lo) box_atomic(bbox, b_hi, hi);
+  }
+}
+
+// One CTA: bits per axis of the largest per-cloud extent, batch bits.
+__global__ void __launch_bounds__(1024) k_meta(const int* __restrict__ bbox, int64_t n_clouds,
+                                               Meta* meta) {
+  __shared__ int s_ext[32], s_b[32];
+  int ext = 0, maxb = 0;
+  for (int64_t c = threadIdx.x; c < n_clouds; c += blockDim.x) {
+    const int* bx = bbox + 6 * c;
+    if (bx[0] <= bx[3]) {
+      ext = max(ext, max(bx[3] - bx[0], max(bx[4] - bx[1], bx[5] - bx[2])));
+      maxb = max(maxb, static_cast<int>(c));
+    }
+  }
+  ext = __reduce_max_sync(kFull, ext);
+  maxb = __reduce_max_sync(kFull, maxb);
+  if ((threadIdx.x & 31) == 0) {
+    s_ext[threadIdx.x >> 5] = ext;
+    s_b[threadIdx.x >> 5] = maxb;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < static_cast<int>(blockDim.x >> 5); ++w) {
+      ext = max(ext, s_ext[w]);
+      maxb = max(maxb, s_b[w]);
+    }
+    const int bpa = ext > 0 ? 32 - __clz(ext) : 0;
+    const int bb = maxb > 0 ? 32 - __clz(maxb) : 0;
+    meta->bpa = bpa;
+    meta->batch_bits = bb;
+    meta->max_extent = ext;
+    meta->key_bits = 3 * bpa + bb;
+  }
+}
+
+__device__ __forceinline__ uint64_t cell_key_of(int4 c, const int* bbox, int bpa) {
+  const int* bx = bbox + 6 * c.w;
+  const uint32_t x = static_cast<uint32_t>(c.x - bx[0]);
+  const uint32_t y = static_cast<uint32_t>(c.y - bx[1]);
+  const uint32_t z = static_cast<uint32_t>(c.z - bx[2]);
+  return (static_cast<uint64_t>(c.w) << (3 * bpa)) | morton3(x, y, z);
+}
+
+__global__ void __launch_bounds__(256) k_keys(const int4* __restrict__ pc, int64_t n,
+                                              const int* __restrict__ bbox, const Meta* meta,
+                                              uint64_t* __restrict__ keys,
+                                              uint32_t* __restrict__ vals) {
+  const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  keys[i] = cell_key_of(pc[i], bbox, meta->bpa);
+  vals[i] = static_cast<uint32_t>(i);
+}
+
+// --------------------------------------------------------- sorted records
+
+// Which ping-pong buffer holds the sorted data after a sort over `bits`.
+__device__ __forceinline__ int sorted_buffer(int bits) { return sort_passes_for_bits(bits) & 1; }
+
+template <typename KeyT>
+__device__ __forceinline__ bool is_head(const KeyT* keys, int64_t s) {
+  return s == 0 || keys[s] != keys[s - 1];
+}
+
+// Tile of 2048 sorted positions per 256-thread CTA, blocked (8 per thread).
+// rec[s] = (xyz[id], id) with id = sorted value; optional pos_of[id] = s;
+// tile_counts[tile] = number of cell heads in the tile.
+template <typename KeyT>
+__global__ void __launch_bounds__(256)
+    k_gather(const float* __restrict__ xyz, int64_t n, SortPair<KeyT> sp, const int* bits_ptr,
+             float4* __restrict__ rec, int32_t* __restrict__ pos_of,
+             uint32_t* __restrict__ tile_counts) {
+  __shared__ uint32_t warp_sums[32];
+  __shared__ uint32_t s_total;
+  const int buf = sorted_buffer(*bits_ptr);
+  const KeyT* keys = sp.keys[buf];
+  const uint32_t* vals = sp.vals[buf];
+  const int64_t base = static_cast<int64_t>(blockIdx.x) * 2048 + threadIdx.x * 8;
+  uint32_t heads = 0;
+#pragma unroll
+  for (int r = 0; r < 8; ++r) {
+    const int64_t s = base + r;
+    if (s >= n) break;
+    const uint32_t id = vals[s];
+    rec[s] = make_float4(xyz[3 * static_cast<int64_t>(id)], xyz[3 * static_cast<int64_t>(id) + 1],
+                         xyz[3 * static_cast<int64_t>(id) + 2], __int_as_float(static_cast<int>(id)));
+    if (pos_of) pos_of[id] = static_cast<int32_t>(s);
+    heads += is_head(keys, s) ? 1u : 0u;
+  }
+  block_inclusive_scan(heads, warp_sums, &s_total);
+  if (threadIdx.x == 0) tile_counts[blockIdx.x] = s_total;
+}
+
+// Cell (group) ids from the scanned tile counts.  head_key[c], head_start[c]
+// for every head; cell_of[s] (optional) = cell of sorted position s;
+// head_start[count] = n.
+template <typename KeyT>
+__global__ void __launch_bounds__(256)
+    k_cells(int64_t n, SortPair<KeyT> sp, const int* bits_ptr,
+            const uint32_t* __restrict__ tile_offsets, const int* count_ptr,
+            KeyT* __restrict__ head_key, int32_t* __restrict__ head_start,
+            int32_t* __restrict__ cell_of) {
+  __shared__ uint32_t warp_sums[32];
+  const KeyT* keys = sp.keys[sorted_buffer(*bits_ptr)];
+  const int64_t base = static_cast<int64_t>(blockIdx.x) * 2048 + threadIdx.x * 8;
+  uint32_t flags = 0, heads = 0;
+#pragma unroll
+  for (int r = 0; r < 8; ++r) {
+    const int64_t s = base + r;
+    if (s < n && is_head(keys, s)) {
+      flags |= 1u << r;
+      ++heads;
+    }
+  }
+  const uint32_t incl = block_inclusive_scan(heads, warp_sums, nullptr);
+  int c = static_cast<int>(tile_offsets[blockIdx.x] + incl - heads) - 1;
+#pragma unroll
+  for (int r = 0; r < 8; ++r) {
+    const int64_t s = base + r;
+    if (s >= n) break;
+    if (flags & (1u << r)) {
+      ++c;
+      head_key[c] = keys[s];
+      head_start[c] = static_cast<int32_t>(s);
+    }
+    if (cell_of) cell_of[s] = c;
+    if (s == n - 1) head_start[*count_ptr] = static_cast<int32_t>(n);
+  }
+}
+
+// ------------------------------------------------------------- neighbours
+
+__device__ __forceinline__ int axis_offset(int position) {
+  return position == 0 ? 0 : (position == 1 ? -1 : 1);
+}
+
+__device__ __forceinline__ int64_t find_key(const uint64_t* keys, int n, uint64_t key) {
+  int lo = 0, hi = n;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (keys[mid] < key) lo = mid + 1; else hi = mid;
+  }
+  return (lo < n && keys[lo] == key) ? lo : -1;
+}
+
+// One thread per (group, neighbour position).  group_key[g] is a key in the
+// support key space; runs[g*27 + j] = (start, count) of the support cell at
+// offset j, or (0, 0) when that cell is empty.
+__global__ void __launch_bounds__(256)
+    k_runs(const uint64_t* __restrict__ group_key, const int* group_count_ptr,
+           const uint64_t* __restrict__ cell_key, const int32_t* __restrict__ cell_start,
+           const int* cell_count_ptr, const Meta* meta, int2* __restrict__ runs) {
+  const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  const int n_groups = *group_count_ptr;
+  if (t >= static_cast<int64_t>(n_groups) * kNeighbours) return;
+  const int g = static_cast<int>(t / kNeighbours), j = static_cast<int>(t % kNeighbours);
+  const int bpa = meta->bpa;
+  const uint64_t key = group_key[g];
+  const uint64_t mask = bpa ? ((1ull << (3 * bpa)) - 1) : 0ull;
+  const uint64_t cloud = key >> (3 * bpa);
+  const uint64_t m = key & mask;
+  const int x = static_cast<int>(compact3(m >> 2)) + axis_offset(j / 9);
+  const int y = static_cast<int>(compact3(m >> 1)) + axis_offset((j / 3) % 3);
+  const int z = static_cast<int>(compact3(m)) + axis_offset(j % 3);
+  const int lim = 1 << bpa;
+  int2 run = make_int2(0, 0);
+  if (x >= 0 && y >= 0 && z >= 0 && x < lim && y < lim && z < lim) {
+    const uint64_t nk = (cloud << (3 * bpa)) |
+                        morton3(static_cast<uint32_t>(x), static_cast<uint32_t>(y),
+                                static_cast<uint32_t>(z));
+    const int64_t hit = find_key(cell_key, *cell_count_ptr, nk);
+    if (hit >= 0) run = make_int2(cell_start[hit], cell_start[hit + 1] - cell_start[hit]);
+  }
+  runs[t] = run;
+}
+
+// One thread per group: ceil(count / 32) items, slots taken with one atomic
+// per warp so the queue keeps the groups' key order within each warp.
+__global__ void __launch_bounds__(256)
+    k_items(const int32_t* __restrict__ group_start, const int32_t* __restrict__ group_row,
+            const int* group_count_ptr, Meta* meta, int4* __restrict__ items) {
+  const int64_t g = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  const int n_groups = *group_count_ptr;
+  const int lane = threadIdx.x & 31;
+  int q_start = 0, q_count = 0, row = 0;
+  if (g < n_groups) {
+    q_start = group_start[g];
+    q_count = group_start[g + 1] - q_start;
+    row = group_row ? group_row[g] : static_cast<int>(g);
+  }
+  const int n_it = q_count > 0 ? (q_count + 31) >> 5 : 0;
+  const int incl = warp_inclusive_scan(n_it);
+  int base = 0;
+  if (lane == 31 && incl > 0) base = atomicAdd(&meta->n_items, incl);
+  base = __shfl_sync(kFull, base, 31) + incl - n_it;
+  for (int t = 0; t < n_it; ++t) {
+    const int qs = q_start + 32 * t;
+    items[base + t] = make_int4(row, qs, min(32, q_start + q_count - qs), 0);
+  }
+}
+
+// ------------------------------------------------------ selected queries
+
+// key = cell of the queried support point, value = output row.
+__global__ void __launch_bounds__(256)
+    k_sel_keys(const int64_t* __restrict__ query_indices, int64_t m, int64_t n,
+               const int32_t* __restrict__ pos_of, const int32_t* __restrict__ cell_of,
+               Meta* meta, uint32_t* __restrict__ keys, uint32_t* __restrict__ vals) {
+  const int64_t r = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (r == 0) {
+    const int p = meta->n_cells;
+    meta->qkey_bits = p > 1 ? 32 - __clz(p - 1) : 0;
+  }
+  if (r >= m) return;
+  int64_t qi = query_indices[r];
+  if (qi < 0 || qi >= n) {
+    raise_status(&meta->status, kStatusTable);
+    qi = 0;
+  }
+  keys[r] = static_cast<uint32_t>(cell_of[pos_of[qi]]);
+  vals[r] = static_cast<uint32_t>(r);
+}
+
+// qrec[j] = (support xyz of the query, output row) in cell order + heads.
+__global__ void __launch_bounds__(256)
+    k_sel_gather(int64_t m, int64_t n, SortPair<uint32_t> sp, const int* bits_ptr,
+                 const int64_t* __restrict__ query_indices, const int32_t* __restrict__ pos_of,
+                 const float4* __restrict__ srec, float4* __restrict__ qrec,
+                 uint32_t* __restrict__ tile_counts) {
+  __shared__ uint32_t warp_sums[32];
+  __shared__ uint32_t s_total;
+  const int buf = sorted_buffer(*bits_ptr);
+  const uint32_t* keys = sp.keys[buf];
+  const uint32_t* vals = sp.vals[buf];
+  const int64_t base = static_cast<int64_t>(blockIdx.x) * 2048 + threadIdx.x * 8;
+  uint32_t heads = 0;
+#pragma unroll
+  for (int r = 0; r < 8; ++r) {
+    const int64_t j = base + r;
+    if (j >= m) break;
+    const uint32_t row = vals[j];
+    int64_t qi = query_indices[row];
+    if (qi < 0 || qi >= n) qi = 0;  // reported by k_sel_keys
+    float4 v = srec[pos_of[qi]];
+    v.w = __int_as_float(static_cast<int>(row));
+    qrec[j] = v;
+    heads += is_head(keys, j) ? 1u : 0u;
+  }
+  block_inclusive_scan(heads, warp_sums, &s_total);
+  if (threadIdx.x == 0) tile_counts[blockIdx.x] = s_total;
+}
+
+// ------------------------------------------------------------ host side
+
+namespace {
+
+// Bits needed to hold any value in [0, count).
+int bits_for_count(int64_t count) {
+  int b = 0;
+  while ((1ll << b) < count) ++b;
+  return b;
+}
+
+int batch_bits_upper(int64_t n_clouds) { return bits_for_count(n_clouds); }
+
+struct Bufs {
+  Meta* meta;
+  int* bbox;
+  int4* pc_s;
+  int4* pc_q;
+  uint64_t* keys64[2];
+  uint32_t* keys32[2];
+  uint32_t* vals[2];
+  uint32_t* hist;
+  uint32_t* totals;         // [3][8*256]
+  uint32_t* tile_counts;
+  float4* srec;
+  float4* qrec;
+  int32_t* pos_of;
+  int32_t* cell_of;
+  uint64_t* cell_key;
+  int32_t* cell_start;
+  int2* runs;
+  uint64_t* group_key;
+  int32_t* group_start;
+  int32_t* group_row;
+  int4* items;
+};
+
+Bufs layout(void* ws, int64_t n, int64_t m, int64_t n_clouds, int kind, size_t* bytes) {
+  Arena a(ws);
+  Bufs b{};
+  const int64_t nm = n > m ? n : m;
+  b.meta = a.take<Meta>(1);
+  // Sized for every valid batch id (< 2^15) so one size serves all callers.
+  b.bbox = a.take<int>(6 * static_cast<size_t>(n_clouds > 32768 ? n_clouds : 32768));
+  b.pc_s = a.take<int4>(n);
+  b.pc_q = kind == FKNN_QUERY_GENERAL ? a.take<int4>(m) : nullptr;
+  b.keys64[0] = a.take<uint64_t>(nm);
+  b.keys64[1] = a.take<uint64_t>(nm);
+  // 32-bit keys (selected queries) alias the 64-bit key buffers.
+  b.keys32[0] = reinterpret_cast<uint32_t*>(b.keys64[0]);
+  b.keys32[1] = reinterpret_cast<uint32_t*>(b.keys64[1]);
+  b.vals[0] = a.take<uint32_t>(nm);
+  b.vals[1] = a.take<uint32_t>(nm);
+  b.hist = a.take<uint32_t>(sort_hist_elems(nm));
+  b.totals = a.take<uint32_t>(3 * kSortMaxPasses * 256);
+  b.tile_counts = a.take<uint32_t>(static_cast<size_t>(ceil_div(nm > 0 ? nm : 1, 2048)));
+  b.srec = a.take<float4>(n);
+  b.cell_key = a.take<uint64_t>(n);
+  b.cell_start = a.take<int32_t>(n + 1);
+  if (kind == FKNN_QUERY_SELECTED) {
+    b.pos_of = a.take<int32_t>(n);
+    b.cell_of = a.take<int32_t>(n);
+  }
+  if (kind == FKNN_QUERY_GENERAL) {
+    b.runs = a.take<int2>(static_cast<size_t>(m) * kNeighbours);
+    b.group_key = a.take<uint64_t>(m);
+  } else {
+    b.runs = a.take<int2>(static_cast<size_t>(n) * kNeighbours);
+  }
+  if (kind != FKNN_QUERY_SELF) {
+    b.qrec = a.take<float4>(m);
+    b.group_start = a.take<int32_t>(m + 1);
+    b.group_row = kind == FKNN_QUERY_SELECTED ? a.take<int32_t>(m) : nullptr;
+  }
+  const int64_t q = kind == FKNN_QUERY_SELF ? n : m;
+  b.items = a.take<int4>(static_cast<size_t>(q + q / 32 + 32));
+  if (bytes) *bytes = a.used + 256;
+  return b;
+}
+
+inline int blocks_for(int64_t n, int per_block) {
+  return static_cast<int>(ceil_div(n > 0 ? n : 1, per_block));
+}
+
+}  // namespace
+
+size_t fused_workspace_bytes(int64_t n, int64_t m, int64_t n_clouds, int kind) {
+  size_t bytes = 0;
+  layout(nullptr, n, m, n_clouds, kind, &bytes);
+  return bytes;
+}
+
+int run_fused(const FusedArgs& f, void* ws, size_t ws_bytes, const QueryShape& shape,
+              cudaStream_t s, int* launches) {
+  const int64_t n = f.n;
+  const int kind = f.kind;
+  const int64_t m = kind == FKNN_QUERY_SELF ? n : f.m;
+  const int64_t n_clouds = f.n_clouds;
+  size_t need = 0;
+  Bufs b = layout(ws, n, m, n_clouds, kind, &need);
+  if (ws_bytes < need) return FKNN_ERR_WORKSPACE;
+  int nl = 0;
+  cudaError_t e;
+  const SortPair<uint64_t> sp64{{b.keys64[0], b.keys64[1]}, {b.vals[0], b.vals[1]}};
+  const SortPair<uint32_t> sp32{{b.keys32[0], b.keys32[1]}, {b.vals[0], b.vals[1]}};
+
+  k_init<<<64, 256, 0, s>>>(b.meta, b.bbox, n_clouds, b.totals, 3 * kSortMaxPasses * 256);
+  ++nl;
+
+  PointSrc ps{f.xyz, f.grid, f.batch, f.offsets, n_clouds, n, f.voxel, f.num_down};
+  if (n > 0) {
+    k_bbox<<<blocks_for(n, 2048), 256, 0, s>>>(ps, b.pc_s, b.bbox, b.meta);
+    ++nl;
+  }
+  PointSrc pq{f.qxyz, nullptr, nullptr, f.qoffsets, n_clouds, m, f.voxel, f.num_down};
+  if (kind == FKNN_QUERY_GENERAL && m > 0) {
+    k_bbox<<<blocks_for(m, 2048), 256, 0, s>>>(pq, b.pc_q, b.bbox, b.meta);
+    ++nl;
+  }
+  k_meta<<<1, 1024, 0, s>>>(b.bbox, n_clouds, b.meta);
+  ++nl;
+
+  const int max_bits = 3 * (16 - f.num_down) + batch_bits_upper(n_clouds);
+  const int max_passes = sort_passes_for_bits(max_bits);
+  const int* key_bits = &b.meta->key_bits;
+
+  // --- support cells
+  if (n > 0) {
+    k_keys<<<blocks_for(n, 256), 256, 0, s>>>(b.pc_s, n, b.bbox, b.meta, b.keys64[0], b.vals[0]);
+    ++nl;
+    SortBuffers<uint64_t> sb{{b.keys64[0], b.keys64[1]}, {b.vals[0], b.vals[1]}, b.hist, b.totals};
+    nl += launch_radix_sort(sb, n, key_bits, max_passes, s);
+    const int tiles = blocks_for(n, 2048);
+    k_gather<uint64_t><<<tiles, 256, 0, s>>>(f.xyz, n, sp64, key_bits, b.srec,
+                                             b.pos_of, b.tile_counts);
+    k_scan_tiles<<<1, 1024, 0, s>>>(b.tile_counts, tiles, &b.meta->n_cells);
+    k_cells<uint64_t><<<tiles, 256, 0, s>>>(n, sp64, key_bits, b.tile_counts,
+                                            &b.meta->n_cells, b.cell_key, b.cell_start, b.cell_of);
+    nl += 3;
+  }
+
+  const float4* qrec = b.srec;
+  int n_qrec = static_cast<int>(n);
+  const int2* runs = b.runs;
+  int pad_mode = kPadSelf;
+  const void* pad = nullptr;
+
+  if (kind == FKNN_QUERY_SELF) {
+    if (n > 0) {
+      k_runs<<<blocks_for(n * kNeighbours, 256), 256, 0, s>>>(
+          b.cell_key, &b.meta->n_cells, b.cell_key, b.cell_start, &b.meta->n_cells, b.meta, b.runs);
+      k_items<<<blocks_for(n, 256), 256, 0, s>>>(b.cell_start, nullptr, &b.meta->n_cells, b.meta,
+                                                 b.items);
+      nl += 2;
+    }
+  } else if (kind == FKNN_QUERY_SELECTED) {
+    pad_mode = kPadArray64;
+    pad = f.query_indices;
+    qrec = b.qrec;
+    n_qrec = static_cast<int>(m);
+    if (n > 0) {
+      k_runs<<<blocks_for(n * kNeighbours, 256), 256, 0, s>>>(
+          b.cell_key, &b.meta->n_cells, b.cell_key, b.cell_start, &b.meta->n_cells, b.meta, b.runs);
+      ++nl;
+    }
+    if (m > 0 && n > 0) {
+      k_sel_keys<<<blocks_for(m, 256), 256, 0, s>>>(f.query_indices, m, n, b.pos_of, b.cell_of,
+                                                    b.meta, b.keys32[0], b.vals[0]);
+      ++nl;
+      SortBuffers<uint32_t> qb{{b.keys32[0], b.keys32[1]}, {b.vals[0], b.vals[1]}, b.hist,
+                               b.totals + kSortMaxPasses * 256};
+      const int qpasses = sort_passes_for_bits(bits_for_count(n));
+      nl += launch_radix_sort(qb, m, &b.meta->qkey_bits, qpasses, s);
+      const int tiles = blocks_for(m, 2048);
+      k_sel_gather<<<tiles, 256, 0, s>>>(m, n, sp32, &b.meta->qkey_bits,
+                                         f.query_indices, b.pos_of, b.srec, b.qrec, b.tile_counts);
+      k_scan_tiles<<<1, 1024, 0, s>>>(b.tile_counts, tiles, &b.meta->n_groups);
+      k_cells<uint32_t><<<tiles, 256, 0, s>>>(m, sp32, &b.meta->qkey_bits, b.tile_counts,
+                                              &b.meta->n_groups,
+                                              reinterpret_cast<uint32_t*>(b.group_row),
+                                              b.group_start, nullptr);
+      k_items<<<blocks_for(m, 256), 256, 0, s>>>(b.group_start, b.group_row, &b.meta->n_groups,
+                                                 b.meta, b.items);
+      nl += 4;
+    }
+  } else {  // general queries
+    pad_mode = kPadMinusOne;
+    qrec = b.qrec;
+    n_qrec = static_cast<int>(m);
+    runs = b.runs;
+    if (m > 0) {
+      k_keys<<<blocks_for(m, 256), 256, 0, s>>>(b.pc_q, m, b.bbox, b.meta, b.keys64[0], b.vals[0]);
+      ++nl;
+      SortBuffers<uint64_t> qb{{b.keys64[0], b.keys64[1]}, {b.vals[0], b.vals[1]}, b.hist,
+                               b.totals + kSortMaxPasses * 256};
+      nl += launch_radix_sort(qb, m, key_bits, max_passes, s);
+      const int tiles = blocks_for(m, 2048);
+      k_gather<uint64_t><<<tiles, 256, 0, s>>>(f.qxyz, m, sp64, key_bits, b.qrec, nullptr,
+                                               b.tile_counts);
+      k_scan_tiles<<<1, 1024, 0, s>>>(b.tile_counts, tiles, &b.meta->n_groups);
+      k_cells<uint64_t><<<tiles, 256, 0, s>>>(m, sp64, key_bits, b.tile_counts,
+                                              &b.meta->n_groups, b.group_key, b.group_start,
+                                              nullptr);
+      k_runs<<<blocks_for(m * kNeighbours, 256), 256, 0, s>>>(
+          b.group_key, &b.meta->n_groups, b.cell_key, b.cell_start, &b.meta->n_cells, b.meta,
+          b.runs);
+      k_items<<<blocks_for(m, 256), 256, 0, s>>>(b.group_start, nullptr, &b.meta->n_groups, b.meta,
+                                                 b.items);
+      nl += 5;
+    }
+  }
+
+  e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    note_cuda_error(e);
+    return FKNN_ERR_CUDA;
+  }
+  if (m > 0) {
+    QueryLaunch q{};
+    q.srec = b.srec;
+    q.n_support = static_cast<int>(n);
+    q.qrec = qrec;
+    q.n_qrec = n_qrec;
+    q.runs = runs;
+    q.items = b.items;
+    q.meta = b.meta;
+    q.k = f.k;
+    q.cut_r2 = f.cut_r2;
+    q.idx_bits = f.idx_bits;
+    q.idx_out = f.idx_out;
+    q.dist_out = f.dist_out;
+    q.n_rows = m;
+    q.pad = pad;
+    q.pad_mode = pad_mode;
+    q.vec_ok = (reinterpret_cast<uintptr_t>(f.idx_out) % 16 == 0) &&
+               (reinterpret_cast<uintptr_t>(f.dist_out) % 16 == 0);
+    const int rc = launch_query(q, shape, s);
+    if (rc != 0) {
+      note_cuda_error(static_cast<cudaError_t>(rc));
+      return FKNN_ERR_CUDA;
+    }
+    ++nl;
+  }
+  if (launches) *launches = nl;
+  return FKNN_OK;
+}
+
+}  // namespace fknn

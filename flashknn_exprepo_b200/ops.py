@@ -1,0 +1,242 @@
+"""Tensor-level entry points over the C ABI (one call = one stream of launches).
+
+Every function takes CUDA tensors, launches on the current stream, and
+returns new tensors.  Nothing here synchronises unless ``validate=True``,
+which reads the device status word once and raises on any device-side
+problem (coordinates outside the Morton range, bad tables, ...).
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+
+import torch
+
+from . import _lib
+from ._lib import FknnError, check, ptr, stream_handle
+
+
+def _require(t: torch.Tensor, name: str, dtype, ndim=None, cols=None) -> torch.Tensor:
+    if not isinstance(t, torch.Tensor):
+        raise TypeError(f"{name} must be a torch.Tensor")
+    if not t.is_cuda:
+        raise FknnError(f"{name} must be a CUDA tensor (FlashKNN-B200 has no CPU path)")
+    if t.dtype != dtype:
+        t = t.to(dtype)
+    if ndim is not None and t.dim() != ndim:
+        raise ValueError(f"{name} must have {ndim} dimensions, got shape {tuple(t.shape)}")
+    if cols is not None and t.shape[-1] != cols:
+        raise ValueError(f"{name} must have shape [N, {cols}], got {tuple(t.shape)}")
+    return t.contiguous()
+
+
+def _config_ptr(config):
+    if config is None:
+        return None, None
+    if isinstance(config, _lib.FknnConfig):
+        c = config
+    else:
+        c = _lib.FknnConfig(*config)
+    return c, ctypes.byref(c)
+
+
+def knn_offsets(xyz, offset, k, voxel, num_down=2, new_xyz=None, new_offset=None,
+                cut_r2=math.inf, config=None, validate=False):
+    """Pointcept-style batched grid kNN.  Returns (idx int32 [m,k], dist2 f32 [m,k])."""
+    lib = _lib.load()
+    xyz = _require(xyz, "xyz", torch.float32, 2, 3)
+    dev = xyz.device
+    offset = _require(offset, "offset", torch.int64, 1)
+    general = new_xyz is not None
+    if general:
+        new_xyz = _require(new_xyz, "new_xyz", torch.float32, 2, 3)
+        if new_offset is None:
+            raise ValueError("new_offset is required with new_xyz")
+        new_offset = _require(new_offset, "new_offset", torch.int64, 1)
+        if new_offset.numel() != offset.numel():
+            raise ValueError("offset and new_offset must describe the same number of clouds")
+    n = xyz.shape[0]
+    m = new_xyz.shape[0] if general else n
+    b = offset.numel()
+    idx = torch.empty((m, k), dtype=torch.int32, device=dev)
+    dist = torch.empty((m, k), dtype=torch.float32, device=dev)
+    kind = _lib.QUERY_GENERAL if general else _lib.QUERY_SELF
+    nbytes = lib.fknn_workspace_bytes(n, m, max(b, 1), kind)
+    ws = _lib.WORKSPACE.get(nbytes, dev)
+    _, cfg = _config_ptr(config)
+    rc = lib.fknn_knn_offsets(ptr(xyz), n, ptr(offset), b, ptr(new_xyz), m, ptr(new_offset), k,
+                              float(voxel), num_down, float(cut_r2), ptr(idx), ptr(dist),
+                              ptr(ws), ws.numel(), cfg, stream_handle(dev))
+    check(rc, "fknn_knn_offsets")
+    if validate:
+        _lib.raise_on_status(ws, "knn_offsets")
+    return idx, dist
+
+
+def knn_grid(xyz, grid_coord, batch_idx, k, num_down=2, cut_r2=math.inf, query_indices=None,
+             idx_dtype=torch.int64, config=None, validate=False):
+    """FlashKNN.query / selected_query on caller-voxelised grid coordinates.
+
+    Returns (idx [m,k] of ``idx_dtype`` in original point numbering, dist2 f32).
+    """
+    lib = _lib.load()
+    grid_coord = _require(grid_coord, "grid_coord", torch.int64, 2, 3)
+    dev = grid_coord.device
+    xyz = _require(xyz, "xyz", torch.float32, 2, 3)
+    if batch_idx is not None:
+        batch_idx = _require(batch_idx, "batch_idx", torch.int64, 1)
+        if batch_idx.numel() != grid_coord.shape[0]:
+            raise ValueError("batch_idx must have one entry per point")
+    if xyz.shape[0] != grid_coord.shape[0]:
+        raise ValueError("xyz and grid_coord must have the same number of points")
+    n = grid_coord.shape[0]
+    selected = query_indices is not None
+    if selected:
+        query_indices = _require(query_indices, "query_indices", torch.int64, 1)
+    m = query_indices.numel() if selected else n
+    if idx_dtype not in (torch.int32, torch.int64):
+        raise ValueError("idx_dtype must be torch.int32 or torch.int64")
+    idx = torch.empty((m, k), dtype=idx_dtype, device=dev)
+    dist = torch.empty((m, k), dtype=torch.float32, device=dev)
+    kind = _lib.QUERY_SELECTED if selected else _lib.QUERY_SELF
+    nbytes = lib.fknn_workspace_bytes(n, m, 32768, kind)
+    ws = _lib.WORKSPACE.get(nbytes, dev)
+    _, cfg = _config_ptr(config)
+    rc = lib.fknn_knn_grid(ptr(xyz), ptr(grid_coord), ptr(batch_idx), n, ptr(query_indices), m, k,
+                           num_down, float(cut_r2), 64 if idx_dtype == torch.int64 else 32,
+                           ptr(idx), ptr(dist), ptr(ws), ws.numel(), cfg, stream_handle(dev))
+    check(rc, "fknn_knn_grid")
+    if validate:
+        _lib.raise_on_status(ws, "knn_grid")
+    return idx, dist
+
+
+def query_tables(xyz_sorted, steps, neigh, cnt, k, cut_r2=math.inf, config=None,
+                 validate=False):
+    """Reference table ABI (FlashKNN_Query_Dynamic_Load): sorted-space (idx, dist)."""
+    lib = _lib.load()
+    xyz_sorted = _require(xyz_sorted, "xyz_sorted", torch.float32, 2, 3)
+    dev = xyz_sorted.device
+    steps = _require(steps, "steps", torch.int32, 1)
+    neigh = _require(neigh, "neigh", torch.int32, 2, 27)
+    cnt = _require(cnt, "cnt", torch.int32, 2, 28)
+    n, p = xyz_sorted.shape[0], neigh.shape[0]
+    if steps.numel() != p + 1 or cnt.shape[0] != p:
+        raise ValueError("steps must have P+1 entries and cnt P rows")
+    idx = torch.empty((n, k), dtype=torch.int32, device=dev)
+    dist = torch.empty((n, k), dtype=torch.float32, device=dev)
+    ws = _lib.WORKSPACE.get(lib.fknn_tables_workspace_bytes(n, n, p), dev)
+    _, cfg = _config_ptr(config)
+    rc = lib.fknn_query_tables(ptr(xyz_sorted), n, ptr(steps), ptr(neigh), ptr(cnt), p, k,
+                               float(cut_r2), ptr(idx), ptr(dist), ptr(ws), ws.numel(), cfg,
+                               stream_handle(dev))
+    check(rc, "fknn_query_tables")
+    if validate:
+        _lib.raise_on_status(ws, "query_tables")
+    return idx, dist
+
+
+def selected_query_tables(xyz_sorted, qindex, steps, steps_query, neigh, cnt, k,
+                          cut_r2=math.inf, config=None, validate=False):
+    """Reference table ABI (FlashKNN_Selected_Query_DL): rows follow qindex."""
+    lib = _lib.load()
+    xyz_sorted = _require(xyz_sorted, "xyz_sorted", torch.float32, 2, 3)
+    dev = xyz_sorted.device
+    qindex = _require(qindex, "qindex", torch.int32, 1)
+    steps = _require(steps, "steps", torch.int32, 1)
+    steps_query = _require(steps_query, "steps_query", torch.int32, 1)
+    neigh = _require(neigh, "neigh", torch.int32, 2, 27)
+    cnt = _require(cnt, "cnt", torch.int32, 2, 28)
+    n, m, p = xyz_sorted.shape[0], qindex.numel(), neigh.shape[0]
+    idx = torch.empty((m, k), dtype=torch.int32, device=dev)
+    dist = torch.empty((m, k), dtype=torch.float32, device=dev)
+    ws = _lib.WORKSPACE.get(lib.fknn_tables_workspace_bytes(n, m, p), dev)
+    _, cfg = _config_ptr(config)
+    rc = lib.fknn_selected_query_tables(ptr(xyz_sorted), n, ptr(qindex), m, ptr(steps),
+                                        ptr(steps_query), ptr(neigh), ptr(cnt), p, k,
+                                        float(cut_r2), ptr(idx), ptr(dist), ptr(ws), ws.numel(),
+                                        cfg, stream_handle(dev))
+    check(rc, "fknn_selected_query_tables")
+    if validate:
+        _lib.raise_on_status(ws, "selected_query_tables")
+    return idx, dist
+
+
+def morton_encode(grid_coord, batch_idx=None):
+    """FlashKNN_Morton_Encode: int64 keys of [N,3] grid coordinates."""
+    lib = _lib.load()
+    grid_coord = _require(grid_coord, "grid_coord", torch.int64, 2, 3)
+    if batch_idx is not None:
+        batch_idx = _require(batch_idx, "batch_idx", torch.int64, 1)
+    keys = torch.empty(grid_coord.shape[0], dtype=torch.int64, device=grid_coord.device)
+    check(lib.fknn_morton_encode(ptr(grid_coord), ptr(batch_idx), grid_coord.shape[0], ptr(keys),
+                                 stream_handle(grid_coord.device)), "fknn_morton_encode")
+    return keys
+
+
+def morton_neighbor_keys(grid_coord_down, parent_batch=None):
+    """FlashKNN_Morton_Neighbor_Keys: [P*27] keys, centre first."""
+    lib = _lib.load()
+    grid_coord_down = _require(grid_coord_down, "grid_coord_down", torch.int64, 2, 3)
+    if parent_batch is not None:
+        parent_batch = _require(parent_batch, "parent_batch", torch.int64, 1)
+    p = grid_coord_down.shape[0]
+    keys = torch.empty(p * 27, dtype=torch.int64, device=grid_coord_down.device)
+    check(lib.fknn_morton_neighbor_keys(ptr(grid_coord_down), ptr(parent_batch), p, ptr(keys),
+                                        stream_handle(grid_coord_down.device)),
+          "fknn_morton_neighbor_keys")
+    return keys
+
+
+def build_tables(grid_coord, batch_idx, num_down):
+    """The reference's table construction on the device.
+
+    Returns dict(order int64 [N], steps int32 [P+1], neigh int32 [P,27],
+    cnt int32 [P,28]).  Reads P back to the host (one synchronisation).
+    """
+    lib = _lib.load()
+    grid_coord = _require(grid_coord, "grid_coord", torch.int64, 2, 3)
+    dev = grid_coord.device
+    if batch_idx is not None:
+        batch_idx = _require(batch_idx, "batch_idx", torch.int64, 1)
+    n = grid_coord.shape[0]
+    order = torch.empty(n, dtype=torch.int64, device=dev)
+    steps = torch.empty(n + 1, dtype=torch.int32, device=dev)
+    neigh = torch.empty(max(n, 1) * 27, dtype=torch.int32, device=dev)
+    cnt = torch.empty(max(n, 1) * 28, dtype=torch.int32, device=dev)
+    n_parents = torch.zeros(1, dtype=torch.int64, device=dev)
+    ws = _lib.WORKSPACE.get(lib.fknn_build_tables_workspace_bytes(n), dev)
+    check(lib.fknn_build_tables(ptr(grid_coord), ptr(batch_idx), n, num_down, ptr(order),
+                                ptr(steps), ptr(neigh), ptr(cnt), ptr(n_parents), ptr(ws),
+                                ws.numel(), stream_handle(dev)), "fknn_build_tables")
+    p = int(n_parents.item())
+    return dict(order=order, steps=steps[: p + 1], neigh=neigh[: p * 27].view(p, 27),
+                cnt=cnt[: p * 28].view(p, 28))
+
+
+def backward(q_xyz, p_xyz, idx, dist, grad_dist, grad_q=None, grad_p=None, accumulate=False):
+    """Gradients of sum(grad_dist * dist) w.r.t. the query and support coordinates.
+
+    grad_q / grad_p: output tensors (allocated when None and requested through
+    the ``want`` semantics of the caller).  Pass the same tensor for both with
+    ``accumulate=True`` to get their sum (self query).
+    """
+    lib = _lib.load()
+    q_xyz = _require(q_xyz, "q_xyz", torch.float32, 2, 3)
+    p_xyz = _require(p_xyz, "p_xyz", torch.float32, 2, 3)
+    dev = q_xyz.device
+    idx = _require(idx, "idx", torch.int32, 2)
+    dist = _require(dist, "dist", torch.float32, 2)
+    grad_dist = _require(grad_dist, "grad_dist", torch.float32, 2)
+    m, k = idx.shape
+    n = p_xyz.shape[0]
+    ws = _lib.WORKSPACE.get(lib.fknn_backward_workspace_bytes(m, n, k), dev)
+    check(lib.fknn_backward(ptr(q_xyz), m, ptr(p_xyz), n, ptr(idx), ptr(dist), ptr(grad_dist), k,
+                            ptr(grad_q), ptr(grad_p), 1 if accumulate else 0, ptr(ws),
+                            ws.numel(), stream_handle(dev)), "fknn_backward")
+    return grad_q, grad_p
+
+
+def last_launch_count() -> int:
+    """Kernels launched by the last successful C-ABI call on this process."""
+    return int(_lib.load().fknn_last_launch_count())

@@ -1,0 +1,181 @@
+/*
+ * FlashKNN-B200: C ABI of the grid k-nearest-neighbour path on sm_100a.
+ *
+ * Every entry point takes plain device pointers, sizes and a CUDA stream
+ * (passed as void*), launches asynchronously on that stream, never
+ * synchronises the device, never allocates, and never throws.  Host-side
+ * argument errors are returned as a negative FKNN_ERR_* code before anything
+ * is launched.  Problems that only the device can see (coordinates outside
+ * the Morton range, inconsistent tables, a bounded wait that gave up) are
+ * OR-ed into a status word inside the caller's workspace; read it with
+ * fknn_read_status().
+ *
+ * Index and distance conventions (same as the reference kernel):
+ *   - squared FP32 distances, ascending per row, ties broken by lower index;
+ *   - a row with fewer than K candidates is padded with (pad index, +inf),
+ *     where the pad index is the query's own index for self / selected
+ *     queries (flash_knn_query_dynamic_load.cu:562,1289) and -1 for general
+ *     queries (Pointcept libs/pointops/functions/query.py:12);
+ *   - K in [1, 64] (flash_knn_query_dynamic_load.cu:694-777 rejects K > 64).
+ *
+ * Reference paths below are relative to the FlashKNN_ExpRepo project root.
+ */
+#ifndef FKNN_H_
+#define FKNN_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define FKNN_API __attribute__((visibility("default")))
+#else
+#define FKNN_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------- return codes */
+#define FKNN_OK 0
+#define FKNN_ERR_ARG (-1)       /* null pointer, negative size, misaligned buffer */
+#define FKNN_ERR_K (-2)         /* K outside [1, 64] */
+#define FKNN_ERR_WORKSPACE (-3) /* workspace smaller than the *_workspace_bytes() size */
+#define FKNN_ERR_CUDA (-4)      /* a launch failed: see fknn_last_cuda_error() */
+#define FKNN_ERR_SIZE (-5)      /* more points than 32-bit indexing allows */
+#define FKNN_ERR_NUM_DOWN (-6)  /* num_down outside [0, 8] */
+
+/* --------------------------------------------------- device status bits */
+#define FKNN_DEVICE_COORD_RANGE 1 /* grid coordinate outside [-2^15, 2^15) */
+#define FKNN_DEVICE_BAD_TABLE 2   /* a table names rows outside the point array */
+#define FKNN_DEVICE_TIMEOUT 4     /* a bounded wait on a bulk copy gave up */
+#define FKNN_DEVICE_BATCH_RANGE 8 /* batch id outside [0, 2^15) */
+
+/* Optional launch shape of the query kernel; NULL selects the defaults.
+ * warps_per_cta in {1,2,4,8}; tile_records (candidate records staged per
+ * warp) a multiple of 32 in [64, 4096]; min_candidates_per_lane >= 1 caps
+ * how many lanes share one query; ctas_per_sm 0 = occupancy maximum. */
+typedef struct fknn_config {
+  int32_t warps_per_cta;
+  int32_t tile_records;
+  int32_t min_candidates_per_lane;
+  int32_t ctas_per_sm;
+} fknn_config;
+
+/* ----------------------------------------------------------- utilities */
+FKNN_API const char* fknn_version(void);
+FKNN_API const char* fknn_error_string(int code);
+/* cudaError_t value of the last launch failure seen by this library. */
+FKNN_API int fknn_last_cuda_error(void);
+/* Copies the workspace's device status word to *status (synchronises
+ * `stream`).  0 means no device-side problem was seen. */
+FKNN_API int fknn_read_status(const void* workspace, int* status, void* stream);
+/* Number of kernels the last successful fused call launched. */
+FKNN_API int fknn_last_launch_count(void);
+/* Kernel timing for benchmarks (no reference counterpart).  With slots > 0
+ * every query-kernel launch is bracketed by a pair of CUDA events on its
+ * stream, taken round-robin from `slots` pairs (inside a CUDA graph capture
+ * the pair becomes event-record nodes of the graph); slots == 0 disables it.
+ * fknn_profile_read waits for the most recent min(max, recorded) pairs and
+ * writes their durations in milliseconds, newest last; returns the count. */
+FKNN_API int fknn_profile_enable(int slots);
+FKNN_API int fknn_profile_read(float* ms_out, int max);
+
+/* --------------------------------------------- fused queries (a1..a9)
+ * Grid construction + candidate gather + top-K + remap in one stream of
+ * launches.  Output rows follow the caller's query order; indices are in
+ * the caller's point numbering.
+ */
+#define FKNN_QUERY_SELF 0     /* queries = support points, pad = own index */
+#define FKNN_QUERY_SELECTED 1 /* queries = a subset of the support points */
+#define FKNN_QUERY_GENERAL 2  /* queries = separate points, pad = -1 */
+
+FKNN_API size_t fknn_workspace_bytes(int64_t n_support, int64_t n_query, int64_t n_clouds,
+                            int32_t query_kind);
+
+/* Pointcept-style offset batching (Pointcept libs/pointops/functions/query.py
+ * :7-24 knn_query(nsample, xyz, offset, new_xyz, new_offset)): offsets are
+ * cumulative cloud ends, grid = floor(xyz / voxel) (FP32 division), parent
+ * cell = grid >> num_down.  new_xyz == NULL selects the self query (m and
+ * new_offsets ignored).  idx_out int32 [m, k], dist_out f32 [m, k]. */
+FKNN_API int fknn_knn_offsets(const float* xyz, int64_t n, const int64_t* offsets, int64_t n_clouds,
+                     const float* new_xyz, int64_t m, const int64_t* new_offsets, int32_t k,
+                     float voxel, int32_t num_down, float cut_r2, int32_t* idx_out,
+                     float* dist_out, void* workspace, size_t workspace_bytes,
+                     const fknn_config* config, void* stream);
+
+/* FlashKNN.query (FlashKNN/functions/FlashKnnWrapper.py:165-449) when
+ * query_indices == NULL, FlashKNN.selected_query (:646-849) otherwise.
+ * grid_coord int64 [n,3], batch_idx int64 [n] (NULL = one cloud), xyz f32
+ * [n,3].  idx_bits 64 writes int64 indices (the reference's return type),
+ * 32 writes int32.  idx_out [m,k] with m = n for the self query. */
+FKNN_API int fknn_knn_grid(const float* xyz, const int64_t* grid_coord, const int64_t* batch_idx,
+                  int64_t n, const int64_t* query_indices, int64_t m, int32_t k,
+                  int32_t num_down, float cut_r2, int32_t idx_bits, void* idx_out,
+                  float* dist_out, void* workspace, size_t workspace_bytes,
+                  const fknn_config* config, void* stream);
+
+/* ------------------------------------------ reference table ABI (a8, a10)
+ * Replaces FlashKNN_Query_Dynamic_Load (FlashKNN/csrc/flash_knn_query.h:144-154):
+ * xyz_sorted f32 [n,3], steps int32 [p+1], neigh int32 [p,27] (-1 = empty),
+ * cnt int32 [p,28]; idx_out int32 [n,k] in sorted-point space, dist_out f32
+ * [n,k].  batch_for_prune is not an argument: the reference accepts and
+ * ignores it (flash_knn_query_dynamic_load.cu:622-624). */
+FKNN_API size_t fknn_tables_workspace_bytes(int64_t n, int64_t m, int64_t p);
+FKNN_API int fknn_query_tables(const float* xyz_sorted, int64_t n, const int32_t* steps,
+                      const int32_t* neigh, const int32_t* cnt, int64_t p, int32_t k,
+                      float cut_r2, int32_t* idx_out, float* dist_out, void* workspace,
+                      size_t workspace_bytes, const fknn_config* config, void* stream);
+
+/* Replaces FlashKNN_Selected_Query_DL (FlashKNN/csrc/flash_knn_query.h:206-218):
+ * qindex int32 [m] (sorted support index of each query, grouped by parent
+ * through steps_query int32 [p+1]); idx_out int32 [m,k], dist_out f32 [m,k]. */
+FKNN_API int fknn_selected_query_tables(const float* xyz_sorted, int64_t n, const int32_t* qindex,
+                               int64_t m, const int32_t* steps, const int32_t* steps_query,
+                               const int32_t* neigh, const int32_t* cnt, int64_t p, int32_t k,
+                               float cut_r2, int32_t* idx_out, float* dist_out,
+                               void* workspace, size_t workspace_bytes,
+                               const fknn_config* config, void* stream);
+
+/* ------------------------------------------------- construction (a1..a6)
+ * Replaces FlashKNN_Morton_Encode (FlashKNN/csrc/flash_knn_construction.h:7-9,
+ * kernel flash_knn_construction.cu:29-40): keys int64 [n]; batch NULL = 0. */
+FKNN_API int fknn_morton_encode(const int64_t* grid_coord, const int64_t* batch_idx, int64_t n,
+                       int64_t* keys, void* stream);
+
+/* Replaces FlashKNN_Morton_Neighbor_Keys (flash_knn_construction.h:11-13,
+ * kernel flash_knn_construction.cu:46-63): keys int64 [p*27], centre first. */
+FKNN_API int fknn_morton_neighbor_keys(const int64_t* grid_down, const int64_t* parent_batch,
+                              int64_t p, int64_t* keys, void* stream);
+
+/* The reference's table construction (FlashKnnWrapper.py:220-337) on the
+ * device: order int64 [n] (stable sort by morton key), steps int32 [n+1],
+ * neigh int32 [n*27], cnt int32 [n*28] (sized for the worst case p = n),
+ * n_parents int64 [1] receives p.  Nothing is read back to the host. */
+FKNN_API size_t fknn_build_tables_workspace_bytes(int64_t n);
+FKNN_API int fknn_build_tables(const int64_t* grid_coord, const int64_t* batch_idx, int64_t n,
+                      int32_t num_down, int64_t* order, int32_t* steps, int32_t* neigh,
+                      int32_t* cnt, int64_t* n_parents, void* workspace,
+                      size_t workspace_bytes, void* stream);
+
+/* ----------------------------------------------------------- backward
+ * No reference counterpart (the reference query is @torch.no_grad,
+ * FlashKnnWrapper.py:165).  For d_ij = |p[idx_ij] - q_i|^2:
+ *   grad_q[i] (+)= sum_j 2 g_ij (q_i - p[idx_ij])
+ *   grad_p[n] (+)= sum_{idx_ij = n} -2 g_ij (q_i - p_n)
+ * summed in a fixed order (grad_p through a stable sort of the neighbour
+ * index and a segmented reduction), so results are bitwise reproducible.
+ * Entries with dist == +inf or idx < 0 (padding) carry no gradient.
+ * accumulate != 0 adds into grad_q / grad_p instead of overwriting them
+ * (grad_q may alias grad_p for a self query only with accumulate != 0). */
+FKNN_API size_t fknn_backward_workspace_bytes(int64_t m, int64_t n, int32_t k);
+FKNN_API int fknn_backward(const float* q_xyz, int64_t m, const float* p_xyz, int64_t n,
+                  const int32_t* idx, const float* dist, const float* grad_dist, int32_t k,
+                  float* grad_q, float* grad_p, int32_t accumulate, void* workspace,
+                  size_t workspace_bytes, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FKNN_H_ */

@@ -1,0 +1,50 @@
+"""Compile the reference's own CUDA kernels for sm_100a into oracle/_ref/.
+
+TEST INFRASTRUCTURE ONLY.  Run it in a container that has the reference
+checkout (default /root/reference, override with FKNN_REFERENCE); the built
+module (oracle/_ref/fknn_ref_cufun*.so) is git-ignored and travels to the
+GPU machine with the working tree.  It compiles the reference sources where
+they lie -- FlashKNN/csrc/flash_knn_query_dynamic_load.cu (production SMPS
+kernel, selected query, back query), flash_knn_query.cu and
+flash_knn_construction.cu -- with the reference's own nvcc flags (-O2
+-lineinfo) plus -gencode arch=compute_100a,code=sm_100a, and binds them with
+oracle/ref_bindings.cpp.  The reference's setup.py is not used.
+
+Load the result with ``oracle.ref_kernels.load()``.
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+OUT = os.path.join(HERE, "_ref")
+NAME = "fknn_ref_cufun"
+
+
+def build(reference: str | None = None, verbose: bool = False) -> str:
+    reference = reference or os.environ.get("FKNN_REFERENCE", "/root/reference")
+    csrc = os.path.join(reference, "FlashKNN", "csrc")
+    if not os.path.isdir(csrc):
+        raise FileNotFoundError(f"reference sources not found under {csrc}")
+    os.environ["TORCH_CUDA_ARCH_LIST"] = "10.0a"
+    os.makedirs(OUT, exist_ok=True)
+    from torch.utils.cpp_extension import load
+    mod = load(
+        name=NAME,
+        sources=[os.path.join(csrc, "flash_knn_query_dynamic_load.cu"),
+                 os.path.join(csrc, "flash_knn_query.cu"),
+                 os.path.join(csrc, "flash_knn_construction.cu"),
+                 os.path.join(HERE, "ref_bindings.cpp")],
+        extra_include_paths=[csrc],
+        extra_cflags=["-O3"],
+        extra_cuda_cflags=["-O2", "-lineinfo"],
+        build_directory=OUT,
+        verbose=verbose,
+        is_python_module=True,
+    )
+    return mod.__file__
+
+
+if __name__ == "__main__":
+    print(build(verbose="--verbose" in sys.argv))

@@ -1,0 +1,484 @@
+/*
+ * CPU restatement of FlashKNN's grid kNN -- TEST INFRASTRUCTURE ONLY.
+ *
+ * Nothing in the product library links or calls this file.  It is the
+ * checker for the CUDA path: the parity tests, the smoke check and the CPU
+ * baseline leg of the benchmark call it through ctypes (oracle/oracle.py).
+ *
+ * What it restates (paths are relative to the reference project root):
+ *   - morton key: FlashKNN/csrc/flash_knn_construction.cu:13-27
+ *     (low 16 bits per axis, x at bit 3b+2, y at 3b+1, z at 3b, batch << 48);
+ *   - 27 neighbour keys, offsets (0,-1,+1) per axis in ij order, centre first:
+ *     FlashKNN/csrc/flash_knn_construction.cu:42-63;
+ *   - table construction (sort, parent grouping by key >> 3*num_down, steps,
+ *     searchsorted neighbour lookup, candidate prefix table):
+ *     FlashKNN/functions/FlashKnnWrapper.py:220-337;
+ *   - the SMPS query semantics: FlashKNN/csrc/flash_knn_query_dynamic_load.cu
+ *     :469-652 (candidate enumeration through CumCntInNeigh :87-155, initial
+ *     fill (self index, +inf) :562, strict acceptance d < K-th and d < cut_r2
+ *     :587-616, ascending output :640-647).  The reference kernel is an exact
+ *     top-K over the candidate set; this restatement computes that top-K
+ *     directly and breaks equal distances by the lower index;
+ *   - the selected-query variant: flash_knn_query_dynamic_load.cu:1211-1370;
+ *   - the output remap order[idx[inverse_order]]: FlashKnnWrapper.py:427-429.
+ *
+ * Distances are FP32.  The contraction order of the reference's expression
+ * dx*dx + dy*dy + dz*dz is not specified by the source; `variant` selects one
+ * of the candidate evaluation orders so the tests can find the one that
+ * reproduces the reference kernel's output bit for bit.
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+/* ------------------------------------------------------------------ keys */
+
+static uint64_t morton16(uint32_t ux, uint32_t uy, uint32_t uz) {
+  uint64_t key = 0;
+  for (int bit = 0; bit < 16; ++bit) {
+    key |= (uint64_t)((ux >> bit) & 1u) << (3 * bit + 2);
+    key |= (uint64_t)((uy >> bit) & 1u) << (3 * bit + 1);
+    key |= (uint64_t)((uz >> bit) & 1u) << (3 * bit);
+  }
+  return key;
+}
+
+int64_t orc_morton_key(int64_t x, int64_t y, int64_t z, int64_t batch) {
+  uint64_t key = morton16((uint32_t)x & 0xffffu, (uint32_t)y & 0xffffu,
+                          (uint32_t)z & 0xffffu);
+  key |= (uint64_t)batch << 48;
+  return (int64_t)key;
+}
+
+void orc_morton_encode(const int64_t* grid, const int64_t* batch, int64_t n,
+                       int64_t* keys) {
+  for (int64_t i = 0; i < n; ++i)
+    keys[i] = orc_morton_key(grid[3 * i], grid[3 * i + 1], grid[3 * i + 2],
+                             batch ? batch[i] : 0);
+}
+
+static int axis_offset(int position) {
+  return position == 0 ? 0 : (position == 1 ? -1 : 1);
+}
+
+void orc_neighbor_keys(const int64_t* grid_down, const int64_t* parent_batch,
+                       int64_t p, int64_t* out) {
+  for (int64_t q = 0; q < p; ++q)
+    for (int j = 0; j < 27; ++j) {
+      const int64_t* g = grid_down + 3 * q;
+      out[q * 27 + j] = orc_morton_key(g[0] + axis_offset(j / 9),
+                                       g[1] + axis_offset((j / 3) % 3),
+                                       g[2] + axis_offset(j % 3),
+                                       parent_batch ? parent_batch[q] : 0);
+    }
+}
+
+/* ------------------------------------------------------- stable argsort */
+
+typedef struct {
+  int64_t key;
+  int64_t index;
+} KeyIndex;
+
+static int cmp_key_index(const void* a, const void* b) {
+  const KeyIndex* x = (const KeyIndex*)a;
+  const KeyIndex* y = (const KeyIndex*)b;
+  if (x->key != y->key) return x->key < y->key ? -1 : 1;
+  return x->index < y->index ? -1 : (x->index > y->index);
+}
+
+/* Stable argsort of signed 64-bit keys (ties keep input order). */
+void orc_argsort_i64(const int64_t* keys, int64_t n, int64_t* order) {
+  KeyIndex* tmp = (KeyIndex*)malloc(sizeof(KeyIndex) * (size_t)(n ? n : 1));
+  for (int64_t i = 0; i < n; ++i) {
+    tmp[i].key = keys[i];
+    tmp[i].index = i;
+  }
+  qsort(tmp, (size_t)n, sizeof(KeyIndex), cmp_key_index);
+  for (int64_t i = 0; i < n; ++i) order[i] = tmp[i].index;
+  free(tmp);
+}
+
+static int64_t search_sorted(const int64_t* keys, int64_t n, int64_t key) {
+  int64_t lo = 0, hi = n;
+  while (lo < hi) {
+    int64_t mid = lo + (hi - lo) / 2;
+    if (keys[mid] < key) lo = mid + 1; else hi = mid;
+  }
+  return (lo < n && keys[lo] == key) ? lo : -1;
+}
+
+/*
+ * Reference table construction (FlashKnnWrapper.py:220-337, fused branch).
+ * Outputs: order[n] (stable argsort of the keys), steps[P+1], neigh[P*27],
+ * cnt[P*28] (exclusive prefix of neighbour counts), and grid_down[P*3] /
+ * parent_batch[P] when non-NULL.  Every output buffer must hold the n-point
+ * worst case (P <= n).  Returns P.
+ */
+int64_t orc_build_tables(const int64_t* grid, const int64_t* batch, int64_t n,
+                         int num_down, int64_t* order, int32_t* steps,
+                         int32_t* neigh, int32_t* cnt, int64_t* grid_down_out,
+                         int64_t* parent_batch_out) {
+  int64_t* keys = (int64_t*)malloc(sizeof(int64_t) * (size_t)(n ? n : 1));
+  orc_morton_encode(grid, batch, n, keys);
+  orc_argsort_i64(keys, n, order);
+  int64_t p = 0;
+  int64_t prev = 0;
+  for (int64_t s = 0; s < n; ++s) {
+    int64_t kd = keys[order[s]] >> (3 * num_down);
+    if (s == 0 || kd != prev) steps[p++] = (int32_t)s;
+    prev = kd;
+  }
+  steps[p] = (int32_t)n;
+  int64_t* gd = (int64_t*)malloc(sizeof(int64_t) * 3 * (size_t)(p ? p : 1));
+  int64_t* pb = (int64_t*)malloc(sizeof(int64_t) * (size_t)(p ? p : 1));
+  for (int64_t q = 0; q < p; ++q) {
+    int64_t src = order[steps[q]];
+    for (int a = 0; a < 3; ++a) gd[3 * q + a] = grid[3 * src + a] >> num_down;
+    pb[q] = batch ? batch[src] : 0;
+  }
+  int64_t* nk = (int64_t*)malloc(sizeof(int64_t) * 27 * (size_t)(p ? p : 1));
+  orc_neighbor_keys(gd, pb, p, nk);
+  int64_t* parent_keys = (int64_t*)malloc(sizeof(int64_t) * (size_t)(p ? p : 1));
+  for (int64_t q = 0; q < p; ++q) parent_keys[q] = nk[27 * q];
+  for (int64_t q = 0; q < p; ++q) {
+    cnt[28 * q] = 0;
+    for (int j = 0; j < 27; ++j) {
+      int64_t hit = search_sorted(parent_keys, p, nk[27 * q + j]);
+      neigh[27 * q + j] = (int32_t)hit;
+      int32_t c = hit >= 0 ? steps[hit + 1] - steps[hit] : 0;
+      cnt[28 * q + j + 1] = cnt[28 * q + j] + c;
+    }
+  }
+  if (grid_down_out) memcpy(grid_down_out, gd, sizeof(int64_t) * 3 * (size_t)p);
+  if (parent_batch_out) memcpy(parent_batch_out, pb, sizeof(int64_t) * (size_t)p);
+  free(parent_keys);
+  free(nk);
+  free(pb);
+  free(gd);
+  free(keys);
+  return p;
+}
+
+/* ------------------------------------------------------------ distances */
+
+/*
+ * FP32 squared distance between candidate c and query q, dx = c - q.
+ * variant 0: fma(dz,dz, fma(dy,dy, dx*dx))
+ * variant 1: fma(dz,dz, fma(dx,dx, dy*dy))
+ * variant 2: ((dx*dx + dy*dy) + dz*dz), every operation rounded
+ */
+static inline float sqdist(const float* c, const float* q, int variant) {
+  float dx = c[0] - q[0];
+  float dy = c[1] - q[1];
+  float dz = c[2] - q[2];
+  switch (variant) {
+    case 0: return fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+    case 1: return fmaf(dz, dz, fmaf(dx, dx, dy * dy));
+    default: {
+      volatile float xx = dx * dx;
+      volatile float yy = dy * dy;
+      volatile float zz = dz * dz;
+      volatile float s = xx + yy;
+      return s + zz;
+    }
+  }
+}
+
+/* Sorted (distance, index) list of length k; insertion keeps the k smallest
+ * under the lexicographic order (d, index). */
+static inline void topk_insert(float d, int64_t id, float* dl, int64_t* il,
+                               int k) {
+  if (d > dl[k - 1] || (d == dl[k - 1] && id >= il[k - 1])) return;
+  int j = k - 1;
+  while (j > 0 && (d < dl[j - 1] || (d == dl[j - 1] && id < il[j - 1]))) {
+    dl[j] = dl[j - 1];
+    il[j] = il[j - 1];
+    --j;
+  }
+  dl[j] = d;
+  il[j] = id;
+}
+
+#define ORC_MAXK 1024
+
+/*
+ * Query over the reference table ABI (FlashKNN_Query_Dynamic_Load).
+ * xyz_sorted[n*3], steps[p+1], neigh[p*27], cnt[p*28].  Output rows are in
+ * sorted-point space; reported indices are idx_map[t] when idx_map is given,
+ * else the sorted position t.  Ties break by the reported index.
+ * Returns 0, or -1 for K out of range, -2 for a table that names an empty
+ * neighbour with a non-zero count.
+ */
+int orc_query_tables(const float* xyz_sorted, const int32_t* steps,
+                     const int32_t* neigh, const int32_t* cnt, int64_t p,
+                     int k, float cut_r2, int variant, const int64_t* idx_map,
+                     int64_t* idx_out, float* dist_out, int nthreads) {
+  if (k < 1 || k > ORC_MAXK) return -1;
+  int bad = 0;
+#ifdef _OPENMP
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+#pragma omp parallel for schedule(dynamic, 16) reduction(| : bad)
+#endif
+  for (int64_t q = 0; q < p; ++q) {
+    float dl[ORC_MAXK];
+    int64_t il[ORC_MAXK];
+    for (int32_t s = steps[q]; s < steps[q + 1]; ++s) {
+      int64_t self = idx_map ? idx_map[s] : s;
+      for (int j = 0; j < k; ++j) { dl[j] = INFINITY; il[j] = INT64_MAX; }
+      for (int j = 0; j < 27; ++j) {
+        int32_t c = cnt[28 * q + j + 1] - cnt[28 * q + j];
+        if (c <= 0) continue;
+        int32_t nb = neigh[27 * q + j];
+        if (nb < 0) { bad = 1; continue; }
+        for (int32_t t = steps[nb]; t < steps[nb] + c; ++t) {
+          float d = sqdist(xyz_sorted + 3 * (int64_t)t, xyz_sorted + 3 * (int64_t)s, variant);
+          if (!(d < cut_r2)) continue;
+          topk_insert(d, idx_map ? idx_map[t] : t, dl, il, k);
+        }
+      }
+      for (int j = 0; j < k; ++j) {
+        idx_out[(int64_t)s * k + j] = (il[j] == INT64_MAX) ? self : il[j];
+        dist_out[(int64_t)s * k + j] = dl[j];
+      }
+    }
+  }
+  return bad ? -2 : 0;
+}
+
+/*
+ * Selected query over the reference table ABI (FlashKNN_Selected_Query_DL).
+ * qindex[m] holds the sorted support index of each query, grouped by parent
+ * through steps_query[p+1].  Output row r belongs to query qindex[r]; the pad
+ * index is the query's own support index (flash_knn_query_dynamic_load.cu:1289).
+ */
+int orc_selected_query_tables(const float* xyz_sorted, const int32_t* qindex,
+                              const int32_t* steps, const int32_t* steps_query,
+                              const int32_t* neigh, const int32_t* cnt,
+                              int64_t p, int k, float cut_r2, int variant,
+                              const int64_t* idx_map, int64_t* idx_out,
+                              float* dist_out, int nthreads) {
+  if (k < 1 || k > ORC_MAXK) return -1;
+  int bad = 0;
+#ifdef _OPENMP
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+#pragma omp parallel for schedule(dynamic, 16) reduction(| : bad)
+#endif
+  for (int64_t q = 0; q < p; ++q) {
+    float dl[ORC_MAXK];
+    int64_t il[ORC_MAXK];
+    for (int32_t r = steps_query[q]; r < steps_query[q + 1]; ++r) {
+      int32_t s = qindex[r];
+      int64_t self = idx_map ? idx_map[s] : s;
+      for (int j = 0; j < k; ++j) { dl[j] = INFINITY; il[j] = INT64_MAX; }
+      for (int j = 0; j < 27; ++j) {
+        int32_t c = cnt[28 * q + j + 1] - cnt[28 * q + j];
+        if (c <= 0) continue;
+        int32_t nb = neigh[27 * q + j];
+        if (nb < 0) { bad = 1; continue; }
+        for (int32_t t = steps[nb]; t < steps[nb] + c; ++t) {
+          float d = sqdist(xyz_sorted + 3 * (int64_t)t, xyz_sorted + 3 * (int64_t)s, variant);
+          if (!(d < cut_r2)) continue;
+          topk_insert(d, idx_map ? idx_map[t] : t, dl, il, k);
+        }
+      }
+      for (int j = 0; j < k; ++j) {
+        idx_out[(int64_t)r * k + j] = (il[j] == INT64_MAX) ? self : il[j];
+        dist_out[(int64_t)r * k + j] = dl[j];
+      }
+    }
+  }
+  return bad ? -2 : 0;
+}
+
+/* ------------------------------------------------------- general queries */
+
+/*
+ * Grid kNN in original-index space, for queries that need not be support
+ * points.  A query's candidates are the support points whose parent cell
+ * (grid >> num_down, same batch) lies in the 3x3x3 block of parent cells
+ * around the query's own parent cell -- for a query that is a support point
+ * this is exactly the reference's candidate set.  Ties break by the lower
+ * support index.  Rows with fewer than K candidates are padded with
+ * (pad[r], +inf); pad == NULL pads with -1.
+ * sgrid/sbatch: support grid coords [n*3] and batch [n]; qgrid/qbatch: query.
+ */
+int orc_knn_general(const float* sxyz, const int64_t* sgrid,
+                    const int64_t* sbatch, int64_t n, const float* qxyz,
+                    const int64_t* qgrid, const int64_t* qbatch, int64_t m,
+                    int num_down, int k, float cut_r2, int variant,
+                    const int64_t* pad, int32_t* idx_out, float* dist_out,
+                    int nthreads) {
+  if (k < 1 || k > ORC_MAXK) return -1;
+  /* Parent-cell keys.  For grid coordinates inside [-2^15, 2^15) the 16-bit
+   * truncation of the morton key is injective on parent cells and a +-1
+   * neighbour key never aliases an occupied cell, so the key lookup below is
+   * integer adjacency of parent cells. */
+  int64_t* pk = (int64_t*)malloc(sizeof(int64_t) * (size_t)(n ? n : 1));
+  int64_t* order = (int64_t*)malloc(sizeof(int64_t) * (size_t)(n ? n : 1));
+  for (int64_t i = 0; i < n; ++i)
+    pk[i] = orc_morton_key(sgrid[3 * i] >> num_down, sgrid[3 * i + 1] >> num_down,
+                           sgrid[3 * i + 2] >> num_down, sbatch ? sbatch[i] : 0);
+  orc_argsort_i64(pk, n, order);
+  int64_t* cell_key = (int64_t*)malloc(sizeof(int64_t) * (size_t)(n ? n : 1));
+  int64_t* cell_start = (int64_t*)malloc(sizeof(int64_t) * (size_t)(n + 1));
+  int64_t p = 0;
+  for (int64_t s = 0; s < n; ++s) {
+    int64_t key = pk[order[s]];
+    if (s == 0 || key != cell_key[p - 1]) { cell_key[p] = key; cell_start[p] = s; ++p; }
+  }
+  cell_start[p] = n;
+#ifdef _OPENMP
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+#pragma omp parallel for schedule(dynamic, 64)
+#endif
+  for (int64_t r = 0; r < m; ++r) {
+    float dl[ORC_MAXK];
+    int64_t il[ORC_MAXK];
+    for (int j = 0; j < k; ++j) { dl[j] = INFINITY; il[j] = INT64_MAX; }
+    int64_t gx = qgrid[3 * r] >> num_down, gy = qgrid[3 * r + 1] >> num_down,
+            gz = qgrid[3 * r + 2] >> num_down;
+    int64_t b = qbatch ? qbatch[r] : 0;
+    for (int j = 0; j < 27; ++j) {
+      int64_t key = orc_morton_key(gx + axis_offset(j / 9), gy + axis_offset((j / 3) % 3),
+                                   gz + axis_offset(j % 3), b);
+      int64_t c = search_sorted(cell_key, p, key);
+      if (c < 0) continue;
+      for (int64_t s = cell_start[c]; s < cell_start[c + 1]; ++s) {
+        int64_t t = order[s];
+        float d = sqdist(sxyz + 3 * t, qxyz + 3 * r, variant);
+        if (!(d < cut_r2)) continue;
+        topk_insert(d, t, dl, il, k);
+      }
+    }
+    int64_t padv = pad ? pad[r] : -1;
+    for (int j = 0; j < k; ++j) {
+      idx_out[r * k + j] = (int32_t)((il[j] == INT64_MAX) ? padv : il[j]);
+      dist_out[r * k + j] = dl[j];
+    }
+  }
+  free(cell_start);
+  free(cell_key);
+  free(order);
+  free(pk);
+  return 0;
+}
+
+/*
+ * Pointcept-style offset batching on top of orc_knn_general: offsets are
+ * cumulative cloud ends, grid = floor(xyz / voxel) in FP32 (the reference
+ * callers' voxelisation, Query/benchmark_s3dis.py:159), batch = cloud id.
+ * qxyz == NULL means a self query (pad = own index); otherwise pad = -1.
+ */
+int orc_knn_offsets(const float* xyz, const int64_t* offsets, int64_t b,
+                    const float* qxyz, const int64_t* qoffsets, float voxel,
+                    int num_down, int k, float cut_r2, int variant,
+                    int32_t* idx_out, float* dist_out, int nthreads) {
+  int64_t n = b ? offsets[b - 1] : 0;
+  int self = qxyz == NULL;
+  if (self) { qxyz = xyz; qoffsets = offsets; }
+  int64_t m = b ? qoffsets[b - 1] : 0;
+  int64_t* sg = (int64_t*)malloc(sizeof(int64_t) * 3 * (size_t)(n ? n : 1));
+  int64_t* sb = (int64_t*)malloc(sizeof(int64_t) * (size_t)(n ? n : 1));
+  int64_t* qg = (int64_t*)malloc(sizeof(int64_t) * 3 * (size_t)(m ? m : 1));
+  int64_t* qb = (int64_t*)malloc(sizeof(int64_t) * (size_t)(m ? m : 1));
+  int64_t* pad = self ? (int64_t*)malloc(sizeof(int64_t) * (size_t)(m ? m : 1)) : NULL;
+  int64_t c = 0;
+  for (int64_t i = 0; i < n; ++i) {
+    while (c < b && i >= offsets[c]) ++c;
+    sb[i] = c;
+    for (int a = 0; a < 3; ++a) sg[3 * i + a] = (int64_t)floorf(xyz[3 * i + a] / voxel);
+  }
+  c = 0;
+  for (int64_t i = 0; i < m; ++i) {
+    while (c < b && i >= qoffsets[c]) ++c;
+    qb[i] = c;
+    for (int a = 0; a < 3; ++a) qg[3 * i + a] = (int64_t)floorf(qxyz[3 * i + a] / voxel);
+    if (pad) pad[i] = i;
+  }
+  int rc = orc_knn_general(xyz, sg, sb, n, qxyz, qg, qb, m, num_down, k, cut_r2,
+                           variant, pad, idx_out, dist_out, nthreads);
+  free(pad);
+  free(qb);
+  free(qg);
+  free(sb);
+  free(sg);
+  return rc;
+}
+
+/* --------------------------------------------------------- brute force */
+
+/*
+ * Exact FP64 k nearest neighbours inside each cloud (offset batching), the
+ * recall reference.  Ties break by the lower index.  Rows with fewer than K
+ * points in their cloud are padded with (-1, +inf).
+ */
+int orc_brute_knn_f64(const float* xyz, const int64_t* offsets, int64_t b,
+                      const float* qxyz, const int64_t* qoffsets, int k,
+                      int32_t* idx_out, double* dist_out, int nthreads) {
+  if (k < 1 || k > ORC_MAXK) return -1;
+  if (qxyz == NULL) { qxyz = xyz; qoffsets = offsets; }
+  int64_t m = b ? qoffsets[b - 1] : 0;
+#ifdef _OPENMP
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+#pragma omp parallel for schedule(dynamic, 64)
+#endif
+  for (int64_t r = 0; r < m; ++r) {
+    double dl[ORC_MAXK];
+    int64_t il[ORC_MAXK];
+    int64_t c = 0;
+    while (c < b && r >= qoffsets[c]) ++c;
+    int64_t s0 = c ? offsets[c - 1] : 0, s1 = offsets[c];
+    for (int j = 0; j < k; ++j) { dl[j] = INFINITY; il[j] = INT64_MAX; }
+    double qx = qxyz[3 * r], qy = qxyz[3 * r + 1], qz = qxyz[3 * r + 2];
+    for (int64_t t = s0; t < s1; ++t) {
+      double dx = (double)xyz[3 * t] - qx, dy = (double)xyz[3 * t + 1] - qy,
+             dz = (double)xyz[3 * t + 2] - qz;
+      double d = dx * dx + dy * dy + dz * dz;
+      if (d > dl[k - 1] || (d == dl[k - 1] && t >= il[k - 1])) continue;
+      int j = k - 1;
+      while (j > 0 && (d < dl[j - 1] || (d == dl[j - 1] && t < il[j - 1]))) {
+        dl[j] = dl[j - 1];
+        il[j] = il[j - 1];
+        --j;
+      }
+      dl[j] = d;
+      il[j] = t;
+    }
+    for (int j = 0; j < k; ++j) {
+      idx_out[r * k + j] = (int32_t)(il[j] == INT64_MAX ? -1 : il[j]);
+      dist_out[r * k + j] = dl[j];
+    }
+  }
+  return 0;
+}
+
+/* ------------------------------------------------------------ backward */
+
+/*
+ * FP64 gradient of L = sum_ij g_ij * d_ij with d_ij = |p_idx_ij - q_i|^2 and
+ * the indices held fixed: grad_q[i] = sum_j 2 g_ij (q_i - p_idx_ij),
+ * grad_p[n] = sum_{idx_ij = n} -2 g_ij (q_i - p_n).  Entries whose distance
+ * is +inf (padding) carry no gradient.
+ */
+void orc_backward_f64(const float* qxyz, int64_t m, const float* pxyz,
+                      int64_t n, const int32_t* idx, const float* dist,
+                      const double* g, int k, double* grad_q, double* grad_p) {
+  memset(grad_q, 0, sizeof(double) * 3 * (size_t)m);
+  memset(grad_p, 0, sizeof(double) * 3 * (size_t)n);
+  for (int64_t i = 0; i < m; ++i)
+    for (int j = 0; j < k; ++j) {
+      int64_t e = i * k + j;
+      if (isinf(dist[e]) || idx[e] < 0) continue;
+      int64_t t = idx[e];
+      for (int a = 0; a < 3; ++a) {
+        double diff = (double)qxyz[3 * i + a] - (double)pxyz[3 * t + a];
+        grad_q[3 * i + a] += 2.0 * g[e] * diff;
+        grad_p[3 * t + a] -= 2.0 * g[e] * diff;
+      }
+    }
+}

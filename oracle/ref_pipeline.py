@@ -1,0 +1,49 @@
+"""The reference's per-cloud query pipeline on the GPU -- TEST/BENCH ONLY.
+
+Restates the fused-construction branch of ``FlashKNN.query``
+(FlashKNN/functions/FlashKnnWrapper.py:220-430) step by step with the same
+ATen calls, and runs the reference's own kernels compiled for sm_100a
+(``oracle.ref_kernels``: FlashKNN_Morton_Encode, FlashKNN_Morton_Neighbor_Keys,
+FlashKNN_Query_Dynamic_Load).  Used as the "plain per-cloud kernel" baseline
+of the benchmark's reference arm and by the parity tests; never by the
+product.
+"""
+from __future__ import annotations
+
+import math
+
+import torch
+import torch.nn.functional as F
+
+
+def reference_query(cufun, grid_coord, batch_idx, xyz, k, num_down=2, cut_radius=math.inf):
+    """Returns (int64 [N,K] original indices, f32 [N,K] distances in sorted
+    order remapped like the indices)."""
+    device = grid_coord.device
+    key = cufun.FlashKNN_Morton_Encode(grid_coord.contiguous(), batch_idx.contiguous())
+    order = torch.argsort(key)
+    key = key[order]
+    grid_coord = grid_coord[order]
+    inverse_order = torch.empty(len(grid_coord), device=device, dtype=torch.long)
+    inverse_order[order] = torch.arange(len(grid_coord), device=device, dtype=torch.long)
+    key_down = key >> (3 * num_down)
+    key_down_unique, count = torch.unique_consecutive(key_down, return_counts=True)
+    steps = F.pad(torch.cumsum(count, dim=0), (1, 0))
+    parent_starts = steps[: len(key_down_unique)]
+    grid_coord_down = (grid_coord[parent_starts] >> num_down).contiguous()
+    parent_batch = batch_idx[order[parent_starts]].contiguous()
+    key_down_nbr = cufun.FlashKNN_Morton_Neighbor_Keys(grid_coord_down, parent_batch)
+    parent_keys = key_down_nbr[::27].contiguous()
+    positions = torch.searchsorted(parent_keys, key_down_nbr)
+    safe_positions = positions.clamp_max(len(parent_keys) - 1)
+    present = (positions < len(parent_keys)) & (parent_keys[safe_positions] == key_down_nbr)
+    neigh = torch.where(present, safe_positions, -1).reshape(-1, 27)
+    cnt_in_neigh = F.pad(torch.cumsum(F.pad(count, (0, 1))[neigh], dim=1), [1, 0])
+    out_indices = torch.zeros((len(grid_coord), k), device=device, dtype=torch.int32)
+    out_dis = torch.zeros((len(grid_coord), k), device=device, dtype=torch.float32)
+    xyz_sorted = xyz[order].float().contiguous()
+    cufun.FlashKNN_Query_Dynamic_Load(xyz_sorted, steps.int(), neigh.int(), cnt_in_neigh.int(), k,
+                                      out_indices, out_dis, 1, cut_radius * cut_radius)
+    out = order[out_indices.long()[inverse_order]]
+    torch.cuda.synchronize()
+    return out, out_dis[inverse_order]

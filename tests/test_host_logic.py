@@ -1,0 +1,44 @@
+"""CPU: argument validation of the drop-in API, mirroring the reference's
+own checks (FlashKNN/functions/FlashKnnWrapper.py:193-219)."""
+import pytest
+
+from flashknn_exprepo_b200.wrapper import FlashKNN
+from flashknn_exprepo_b200 import synthetic as S
+
+
+def test_mode_validation_mirrors_reference():
+    chk = FlashKNN._check_modes
+    chk("SM", "PS", "register", True, None)
+    chk("GM", "SS", "register", True, None)
+    with pytest.raises(ValueError):
+        chk("SM", "PS", "global", True, None)
+    with pytest.raises(ValueError):
+        chk("SM", "PS", "register", True, 12)
+    with pytest.raises(ValueError):
+        chk("GM", "PS", "shared", True, None)
+    with pytest.raises(ValueError):
+        chk("SM", "SS", "register", True, 16)
+    with pytest.raises(ValueError):
+        chk("XX", "PS", "register", True, None)
+
+
+def test_constructor_limits():
+    with pytest.raises(ValueError):
+        FlashKNN(num_nbr=65)
+    with pytest.raises(ValueError):
+        FlashKNN(num_nbr=8, num_down=9)
+    f = FlashKNN(num_nbr=16, num_down=2, debug=True)
+    assert f.time_list == []
+    assert f.rng_grid([0, -1, 1], device="cpu")[0].tolist() == [0, 0, 0]
+    assert f.rng_grid([0, -1, 1], device="cpu").shape == (27, 3)
+
+
+def test_synthetic_generators_are_seeded():
+    a = S.uniform_cube(2048, voxel=0.05)
+    b = S.uniform_cube(2048, voxel=0.05)
+    assert (a == b).all() and a.shape == (2048, 3)
+    r = S.room(target=5000)
+    assert r.shape == (5000, 3)
+    counts, seed = S.draw_counts()
+    assert len(counts) == 16 and abs(counts.sum() - 1.5e6) <= 0.03 * 1.5e6
+    assert counts.min() >= 20000 and counts.max() <= 200000

@@ -1,0 +1,179 @@
+"""CPU: pin the oracle against the reference's own outputs (golden fixtures)
+and check its internal consistency.  No GPU needed."""
+import os
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from tests.conftest import GOLDEN, golden_cases
+
+
+def load(case):
+    return np.load(os.path.join(GOLDEN, f"tables_{case}.npz"))
+
+
+def test_morton_keys_match_reference_lut_encoder():
+    d = np.load(os.path.join(GOLDEN, "morton_keys.npz"))
+    assert np.array_equal(O.morton_encode(d["grid"], d["batch"]), d["keys"])
+    assert np.array_equal(O.morton_encode(d["grid"]), d["keys_nobatch"])
+
+
+def test_morton_key_bit_layout():
+    # x bit b -> 3b+2, y -> 3b+1, z -> 3b, batch << 48
+    assert O.morton_key(1, 0, 0) == 4
+    assert O.morton_key(0, 1, 0) == 2
+    assert O.morton_key(0, 0, 1) == 1
+    assert O.morton_key(2, 0, 0) == 32
+    assert O.morton_key(0, 0, 0, 3) == 3 << 48
+    assert O.morton_key(-1, 0, 0) == O.morton_key(0xFFFF, 0, 0)
+
+
+def test_neighbor_key_order_centre_first():
+    keys = O.neighbor_keys(np.array([[10, 20, 30]]), np.array([2]))
+    offs = [0, -1, 1]
+    expect = [O.morton_key(10 + offs[j // 9], 20 + offs[(j // 3) % 3], 30 + offs[j % 3], 2)
+              for j in range(27)]
+    assert keys.tolist() == expect
+
+
+@pytest.mark.parametrize("case", golden_cases())
+def test_tables_match_reference_wrapper(case):
+    z = load(case)
+    t = O.build_tables(z["grid"], z["batch"], int(z["num_down"]))
+    assert np.array_equal(t["steps"], z["ref_steps"])
+    assert np.array_equal(t["neigh"], z["ref_neigh"])
+    assert np.array_equal(t["cnt"], z["ref_cnt"])
+    keys = O.morton_encode(z["grid"], z["batch"])
+    if len(np.unique(keys)) == len(keys):
+        # unique keys: the reference's (unstable) argsort is the stable order
+        assert np.array_equal(z["xyz"][t["order"]], z["ref_xyz_sorted"])
+    else:
+        # equal keys: same multiset of points inside every run of equal keys
+        ks = keys[t["order"]]
+        a = z["xyz"][t["order"]]
+        b = z["ref_xyz_sorted"]
+        for key in np.unique(ks):
+            m = ks == key
+            assert sorted(map(tuple, a[m])) == sorted(map(tuple, b[m]))
+
+
+def _candidate_sets(steps, neigh, cnt, p):
+    out = []
+    for j in range(27):
+        c = cnt[p, j + 1] - cnt[p, j]
+        if c > 0:
+            s = steps[neigh[p, j]]
+            out.extend(range(s, s + c))
+    return out
+
+
+@pytest.mark.parametrize("case", [c for c in golden_cases() if "selected" not in c])
+def test_oracle_query_is_exact_topk_over_candidates(case):
+    z = load(case)
+    xyz, steps, neigh, cnt = (z["ref_xyz_sorted"], z["ref_steps"], z["ref_neigh"], z["ref_cnt"])
+    k = int(z["k"])
+    idx, dist = O.query_tables(xyz, steps, neigh, cnt, k)
+    rng = np.random.default_rng(0)
+    for p in rng.choice(len(neigh), size=min(40, len(neigh)), replace=False):
+        cand = np.array(_candidate_sets(steps, neigh, cnt, p), np.int64)
+        for s in range(steps[p], steps[p + 1]):
+            dx = (xyz[cand] - xyz[s]).astype(np.float32)
+            # variant: fma(dz,dz, fma(dx,dx, dy*dy)), done in float64 then rounded
+            # twice exactly like the C code is not reproducible in numpy, so check
+            # through the oracle's own distances: they must be the recomputed
+            # squared distances within one FP32 rounding step per operation.
+            d64 = (dx.astype(np.float64) ** 2).sum(1)
+            order = np.lexsort((cand, d64))
+            got = idx[s]
+            valid = np.isfinite(dist[s])
+            assert np.all(np.diff(dist[s][valid]) >= 0)
+            assert np.allclose(dist[s][valid], d64[order][: valid.sum()], rtol=1e-6, atol=1e-12)
+            if len(cand) < k:
+                assert np.all(got[len(cand):] == s)
+                assert np.all(np.isinf(dist[s][len(cand):]))
+            assert set(got[valid]) <= set(cand.tolist())
+
+
+@pytest.mark.parametrize("case", [c for c in golden_cases() if "selected" not in c])
+def test_oracle_general_matches_table_path(case):
+    """Two independent restatements: the table ABI remapped to original
+    indices, and the key-lookup path on original points."""
+    z = load(case)
+    k, nd = int(z["k"]), int(z["num_down"])
+    t = O.build_tables(z["grid"], z["batch"], nd)
+    order = t["order"]
+    xs = z["xyz"][order]
+    idx_s, dist_s = O.query_tables(xs, t["steps"], t["neigh"], t["cnt"], k, idx_map=order)
+    idx_o = np.empty_like(idx_s)
+    dist_o = np.empty_like(dist_s)
+    idx_o[order] = idx_s
+    dist_o[order] = dist_s
+    n = len(z["xyz"])
+    gi, gd = O.knn_general(z["xyz"], z["grid"], z["batch"], z["xyz"], z["grid"], z["batch"], nd,
+                           k, pad=np.arange(n))
+    assert np.array_equal(gi, idx_o.astype(np.int32))
+    assert np.array_equal(gd, dist_o)
+
+
+@pytest.mark.parametrize("case", [c for c in golden_cases() if "selected" in c])
+def test_oracle_selected_matches_general(case):
+    z = load(case)
+    k, nd = int(z["k"]), int(z["num_down"])
+    t = O.build_tables(z["grid"], z["batch"], nd)
+    # the golden call's own selected-query tables
+    ri, rd = O.selected_query_tables(z["ref_xyz_sorted"], z["ref_qindex"], z["ref_steps"],
+                                     z["ref_steps_query"], z["ref_neigh"], z["ref_cnt"], k)
+    # map sorted rows/indices back to original numbering through the wrapper's
+    # own permutation (unique keys in these fixtures)
+    order = t["order"]
+    assert np.array_equal(z["xyz"][order], z["ref_xyz_sorted"])
+    qidx = z["query_indices"]
+    inv = np.empty_like(order)
+    inv[order] = np.arange(len(order))
+    qsorted = inv[qidx]
+    rows = {int(s): r for r, s in enumerate(z["ref_qindex"])}
+    gi, gd = O.knn_general(z["xyz"], z["grid"], z["batch"], z["xyz"][qidx], z["grid"][qidx],
+                           z["batch"][qidx], nd, k, pad=qidx)
+    for r in range(len(qidx)):
+        rr = rows[int(qsorted[r])]
+        assert np.array_equal(order[ri[rr]], gi[r])
+        assert np.array_equal(rd[rr], gd[r])
+
+
+def test_brute_force_matches_grid_when_one_cell_covers_all():
+    rng = np.random.default_rng(3)
+    xyz = rng.random((500, 3), dtype=np.float32)
+    grid = np.floor(xyz / np.float32(0.1)).astype(np.int64)
+    # num_down = 8: every point shares one parent cell -> exact kNN in FP32
+    gi, gd = O.knn_general(xyz, grid, None, xyz, grid, None, 8, 12, pad=np.arange(500))
+    bi, bd = O.brute_knn_f64(xyz, np.array([500]), 12)
+    agree = (gi == bi).mean()
+    assert agree > 0.999
+    assert np.allclose(gd, bd, rtol=1e-6)
+
+
+def test_backward_f64_matches_finite_differences():
+    rng = np.random.default_rng(5)
+    q = rng.random((30, 3), dtype=np.float32)
+    p = rng.random((50, 3), dtype=np.float32)
+    idx = rng.integers(0, 50, size=(30, 4)).astype(np.int32)
+    dist = np.ones((30, 4), np.float32)
+    g = rng.standard_normal((30, 4))
+    gq, gp = O.backward_f64(q, p, idx, dist, g)
+
+    def loss(qq, pp):
+        d = ((pp[idx].astype(np.float64) - qq[:, None, :].astype(np.float64)) ** 2).sum(-1)
+        return (g * d).sum()
+
+    h = 1e-4
+    for (arr, grad) in ((q, gq), (p, gp)):
+        for i in range(0, arr.shape[0], 7):
+            for a in range(3):
+                ap = arr.astype(np.float64).copy()
+                am = arr.astype(np.float64).copy()
+                ap[i, a] += h
+                am[i, a] -= h
+                fd = (loss(ap if arr is q else q, p if arr is q else ap)
+                      - loss(am if arr is q else q, p if arr is q else am)) / (2 * h)
+                assert abs(fd - grad[i, a]) <= 1e-6 * max(1.0, abs(fd))
