@@ -48,6 +48,9 @@ def parse_args():
     ap.add_argument("--k", type=int, default=16)
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the per-cloud, fwd+bwd and CPU-baseline legs")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer e2e leg")
+    ap.add_argument("--clouds", type=int, default=16,
+                    help="use the first N clouds of the batch (small cases for profiling)")
     return ap.parse_args()
 
 
@@ -73,59 +76,62 @@ def take_clouds(batch, ids):
 
 
 class ClockSampler:
-    """nvidia-smi samples (SM clock, max clock, throttle reasons) while running."""
+    """NVML samples of the SM clock and throttle reasons while the timed
+    region runs (a polling thread, 1 ms period)."""
 
-    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = {"sw_power_cap": 0x4, "hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20,
+               "hw_thermal_slowdown": 0x40}
 
-    def __init__(self, index):
-        self.index = index
-        self.proc = None
-        self.lines = []
+    def __init__(self, device_index):
+        self.device_index = device_index
+        self.sm, self.reasons, self.max_mhz = [], set(), None
+        self.err = None
 
     def __enter__(self):
+        self._stop = threading.Event()
         try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "100"],
-                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.thread = threading.Thread(target=self._read, daemon=True)
+            import pynvml
+            import torch
+            pynvml.nvmlInit()
+            uuid = str(torch.cuda.get_device_properties(self.device_index).uuid)
+            try:
+                h = pynvml.nvmlDeviceGetHandleByUUID(uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
+            except pynvml.NVMLError:
+                h = pynvml.nvmlDeviceGetHandleByIndex(self.device_index)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM)
+            self._h, self._nv = h, pynvml
+            self.thread = threading.Thread(target=self._poll, daemon=True)
             self.thread.start()
-        except (OSError, ValueError):
-            self.proc = None
+        except Exception as exc:  # sampling is best effort; recorded in the output
+            self.err = f"{type(exc).__name__}: {exc}"[:120]
+            self._h = None
         return self
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
+    def _poll(self):
+        nv = self._nv
+        while not self._stop.is_set():
+            try:
+                self.sm.append(nv.nvmlDeviceGetClockInfo(self._h, nv.NVML_CLOCK_SM))
+                bits = nv.nvmlDeviceGetCurrentClocksEventReasons(self._h)
+                for name, mask in self.REASONS.items():
+                    if bits & mask:
+                        self.reasons.add(name)
+            except Exception:
+                pass
+            time.sleep(0.001)
 
     def __exit__(self, *exc):
-        if self.proc is not None:
-            self.proc.terminate()
-            try:
-                self.proc.wait(timeout=5)
-            except subprocess.TimeoutExpired:
-                self.proc.kill()
+        self._stop.set()
+        if getattr(self, "_h", None) is not None:
+            self.thread.join(timeout=2)
 
     def summary(self):
-        sm, mx, reasons = [], [], set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
-            parts = [p.strip() for p in ln.split(",")]
-            if len(parts) < 8:
-                continue
-            try:
-                sm.append(float(parts[0]))
-                mx.append(float(parts[1]))
-            except ValueError:
-                continue
-            for name, val in zip(names, parts[4:8]):
-                if val.lower().startswith("active"):
-                    reasons.add(name)
-        return {"sm_mhz": statistics.median(sm) if sm else None,
-                "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
-                "samples": len(sm)}
+        out = {"sm_mhz": statistics.median(self.sm) if self.sm else None,
+               "sm_max_mhz": self.max_mhz, "reasons": sorted(self.reasons),
+               "samples": len(self.sm)}
+        if self.err:
+            out["error"] = self.err
+        return out
 
 
 def measured_peak_hbm():
@@ -179,6 +185,8 @@ def run_ours(args, rank, world, local_rank, dist):
     torch.cuda.set_device(dev)
     k = args.k
     batch = synthetic.uneven_batch()
+    if args.clouds < len(batch.counts):
+        batch = synthetic.first_clouds(batch, args.clouds)
     voxel = synthetic.C4_VOXEL
     # Weak scaling: the job is `world` copies of the 16-cloud batch; whole
     # clouds are assigned to ranks, largest first onto the least-loaded rank.
@@ -248,6 +256,10 @@ def run_ours(args, rank, world, local_rank, dist):
            "clocks": clocks.summary(), "kernel_ms": kern_ms, "launches_per_step": launches_per_step,
            "graph_matches_eager": graph_matches, "local_n": n}
     del graph
+
+    if args.no_e2e:
+        out["e2e"] = None
+        return out
 
     # --- e2e through the public API: pinned host in, pinned host out
     xyz_pin = torch.from_numpy(xyz_h).pin_memory()
@@ -470,8 +482,8 @@ def main():
         "warmup": args.warmup, "ms_per_step": out["ms_per_step"], "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded; stands in for S3DIS/SemanticKITTI crops)",
-        "config": {"workload": "uneven_batch_16clouds_k16", "n_points": out["n_points"],
-                   "n_clouds": 16, "k": k, "voxel_m": 0.05, "num_down": 2,
+        "config": {"workload": f"uneven_batch_{args.clouds}clouds_k{k}", "n_points": out["n_points"],
+                   "n_clouds": args.clouds * world, "k": k, "voxel_m": 0.05, "num_down": 2,
                    "step": "CUDA-graph replay of construction + query",
                    "l2": "flushed (256 MiB memset) before every timed step",
                    "parallelism": f"{world} x 16 clouds, whole clouds per GPU, no collective"},

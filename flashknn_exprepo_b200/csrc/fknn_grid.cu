@@ -20,8 +20,9 @@
 //   k_runs          27 (start, count) candidate runs per cell / query group,
 //                   centre first, (0,-1,+1)^3 in ij order like the reference
 //                   neighbour table (flash_knn_construction.cu:42-63)
-//   k_items         work items (<= 32 queries of one group) for the query
-//                   kernel, allocated with warp-aggregated atomics
+//   items           work items for the query kernel: up to 32 consecutive
+//                   queries of consecutive groups whose candidates fit one
+//                   shared-memory tile (fknn_items.cu)
 //
 // Parent cells and their 3x3x3 adjacency are those of the reference: for grid
 // coordinates inside [-2^15, 2^15) the reference's key >> 3*num_down groups
@@ -361,31 +362,6 @@ __global__ void __launch_bounds__(256)
   runs[t] = run;
 }
 
-// One thread per group: ceil(count / 32) items, slots taken with one atomic
-// per warp so the queue keeps the groups' key order within each warp.
-__global__ void __launch_bounds__(256)
-    k_items(const int32_t* __restrict__ group_start, const int32_t* __restrict__ group_row,
-            const int* group_count_ptr, Meta* meta, int4* __restrict__ items) {
-  const int64_t g = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-  const int n_groups = *group_count_ptr;
-  const int lane = threadIdx.x & 31;
-  int q_start = 0, q_count = 0, row = 0;
-  if (g < n_groups) {
-    q_start = group_start[g];
-    q_count = group_start[g + 1] - q_start;
-    row = group_row ? group_row[g] : static_cast<int>(g);
-  }
-  const int n_it = q_count > 0 ? (q_count + 31) >> 5 : 0;
-  const int incl = warp_inclusive_scan(n_it);
-  int base = 0;
-  if (lane == 31 && incl > 0) base = atomicAdd(&meta->n_items, incl);
-  base = __shfl_sync(kFull, base, 31) + incl - n_it;
-  for (int t = 0; t < n_it; ++t) {
-    const int qs = q_start + 32 * t;
-    items[base + t] = make_int4(row, qs, min(32, q_start + q_count - qs), 0);
-  }
-}
-
 // ------------------------------------------------------ selected queries
 
 // key = cell of the queried support point, value = output row.
@@ -472,6 +448,8 @@ struct Bufs {
   int32_t* group_start;
   int32_t* group_row;
   int4* items;
+  int32_t* cands;
+  uint32_t* seg_counts;
 };
 
 Bufs layout(void* ws, int64_t n, int64_t m, int64_t n_clouds, int kind, size_t* bytes) {
@@ -512,7 +490,10 @@ Bufs layout(void* ws, int64_t n, int64_t m, int64_t n_clouds, int kind, size_t* 
     b.group_row = kind == FKNN_QUERY_SELECTED ? a.take<int32_t>(m) : nullptr;
   }
   const int64_t q = kind == FKNN_QUERY_SELF ? n : m;
-  b.items = a.take<int4>(static_cast<size_t>(q + q / 32 + 32));
+  const int64_t max_groups = kind == FKNN_QUERY_SELF ? n : m;
+  b.items = a.take<int4>(items_capacity(max_groups, q));
+  b.cands = a.take<int32_t>(max_groups);
+  b.seg_counts = a.take<uint32_t>(pack_segments(max_groups));
   if (bytes) *bytes = a.used + 256;
   return b;
 }
@@ -583,20 +564,26 @@ int run_fused(const FusedArgs& f, void* ws, size_t ws_bytes, const QueryShape& s
   const int2* runs = b.runs;
   int pad_mode = kPadSelf;
   const void* pad = nullptr;
+  const int32_t* group_start = b.cell_start;
+  const int32_t* group_row = nullptr;
+  const int* group_count_ptr = &b.meta->n_cells;
 
   if (kind == FKNN_QUERY_SELF) {
     if (n > 0) {
       k_runs<<<blocks_for(n * kNeighbours, 256), 256, 0, s>>>(
           b.cell_key, &b.meta->n_cells, b.cell_key, b.cell_start, &b.meta->n_cells, b.meta, b.runs);
-      k_items<<<blocks_for(n, 256), 256, 0, s>>>(b.cell_start, nullptr, &b.meta->n_cells, b.meta,
-                                                 b.items);
-      nl += 2;
+      ++nl;
+      nl += launch_items(b.runs, b.cell_start, nullptr, &b.meta->n_cells, n, shape.tile_records,
+                         b.cands, b.seg_counts, &b.meta->n_items, b.items, s);
     }
   } else if (kind == FKNN_QUERY_SELECTED) {
     pad_mode = kPadArray64;
     pad = f.query_indices;
     qrec = b.qrec;
     n_qrec = static_cast<int>(m);
+    group_start = b.group_start;
+    group_row = b.group_row;
+    group_count_ptr = &b.meta->n_groups;
     if (n > 0) {
       k_runs<<<blocks_for(n * kNeighbours, 256), 256, 0, s>>>(
           b.cell_key, &b.meta->n_cells, b.cell_key, b.cell_start, &b.meta->n_cells, b.meta, b.runs);
@@ -618,15 +605,17 @@ int run_fused(const FusedArgs& f, void* ws, size_t ws_bytes, const QueryShape& s
                                               &b.meta->n_groups,
                                               reinterpret_cast<uint32_t*>(b.group_row),
                                               b.group_start, nullptr);
-      k_items<<<blocks_for(m, 256), 256, 0, s>>>(b.group_start, b.group_row, &b.meta->n_groups,
-                                                 b.meta, b.items);
-      nl += 4;
+      nl += 3;
+      nl += launch_items(b.runs, b.group_start, b.group_row, &b.meta->n_groups, m,
+                         shape.tile_records, b.cands, b.seg_counts, &b.meta->n_items, b.items, s);
     }
   } else {  // general queries
     pad_mode = kPadMinusOne;
     qrec = b.qrec;
     n_qrec = static_cast<int>(m);
     runs = b.runs;
+    group_start = b.group_start;
+    group_count_ptr = &b.meta->n_groups;
     if (m > 0) {
       k_keys<<<blocks_for(m, 256), 256, 0, s>>>(b.pc_q, m, b.bbox, b.meta, b.keys64[0], b.vals[0]);
       ++nl;
@@ -643,9 +632,9 @@ int run_fused(const FusedArgs& f, void* ws, size_t ws_bytes, const QueryShape& s
       k_runs<<<blocks_for(m * kNeighbours, 256), 256, 0, s>>>(
           b.group_key, &b.meta->n_groups, b.cell_key, b.cell_start, &b.meta->n_cells, b.meta,
           b.runs);
-      k_items<<<blocks_for(m, 256), 256, 0, s>>>(b.group_start, nullptr, &b.meta->n_groups, b.meta,
-                                                 b.items);
-      nl += 5;
+      nl += 4;
+      nl += launch_items(b.runs, b.group_start, nullptr, &b.meta->n_groups, m, shape.tile_records,
+                         b.cands, b.seg_counts, &b.meta->n_items, b.items, s);
     }
   }
 
@@ -661,6 +650,9 @@ int run_fused(const FusedArgs& f, void* ws, size_t ws_bytes, const QueryShape& s
     q.qrec = qrec;
     q.n_qrec = n_qrec;
     q.runs = runs;
+    q.group_start = group_start;
+    q.group_row = group_row;
+    q.group_count_ptr = group_count_ptr;
     q.items = b.items;
     q.meta = b.meta;
     q.k = f.k;

@@ -26,14 +26,12 @@ struct Meta {
 };
 static_assert(sizeof(Meta) == 64, "Meta layout");
 
-// One unit of query work: the queries [q_start, q_start + q_count) of the
-// query-record array share the 27 candidate runs in runs[runs_row].
-struct Item {
-  int runs_row;
-  int q_start;
-  int q_count;
-  int unused;
-};
+// Work items (int4): (q_start, q_count, g_first, g_count | flags) -- the
+// queries [q_start, q_start + q_count) of the query-record array, which
+// belong to the groups [g_first, g_first + g_count).  A chunked item has one
+// group whose candidates exceed a tile; they are streamed tile by tile.
+constexpr int kItemChunked = 1 << 30;
+constexpr int kMaxGroupsPerItem = 32;
 
 // Resolved launch shape of the query kernel.
 struct QueryShape {
@@ -54,7 +52,10 @@ struct QueryLaunch {
   const float4* qrec;  // query records (x, y, z, output-row bits)
   int n_qrec;
   const int2* runs;    // [rows][27] (start, count) into srec
-  const int4* items;   // Item array
+  const int32_t* group_start;  // [groups + 1] query ranges in qrec
+  const int32_t* group_row;    // runs row of each group, or null (row = group)
+  const int* group_count_ptr;  // device: number of groups
+  const int4* items;   // work items (see above)
   Meta* meta;
   int k;
   float cut_r2;
@@ -69,6 +70,14 @@ struct QueryLaunch {
 
 // Launches the persistent query kernel; returns 0 or a cudaError_t.
 int launch_query(const QueryLaunch& q, const QueryShape& shape, cudaStream_t s);
+
+// Item construction (fknn_items.cu): per-group candidate counts, segmented
+// greedy packing; *n_items_ptr receives the item count.  Returns launches.
+int launch_items(const int2* runs, const int32_t* group_start, const int32_t* group_row,
+                 const int* group_count_ptr, int64_t max_groups, int tile, int32_t* cands,
+                 uint32_t* seg_counts, int* n_items_ptr, int4* items, cudaStream_t s);
+size_t items_capacity(int64_t max_groups, int64_t n_queries);
+inline int64_t pack_segments(int64_t max_groups) { return (max_groups + 63) / 64; }
 
 // Bump allocator over a caller-provided workspace (256-byte aligned slices).
 struct Arena {

@@ -1,0 +1,118 @@
+// Work items of the query kernel.
+//
+// A query group is a set of queries (contiguous in the query-record array)
+// that share one candidate set: the 27 runs of a parent cell.  Items pack
+// up to 32 consecutive queries -- possibly from several consecutive groups --
+// so that every lane of a warp owns one query, as long as the candidates of
+// all groups in the item fit one shared-memory tile.  Groups with more
+// candidates than a tile become "chunked" items of up to 32 queries that
+// stream their candidates tile by tile.
+//
+// Packing is a sequential greedy pass over the groups in key order; it runs
+// in parallel over segments of 64 groups (one thread each): a count pass,
+// a scan of the per-segment counts, and a write pass.  Items therefore keep
+// the spatial order of the groups.
+#include "fknn_common.cuh"
+#include "fknn_internal.h"
+#include "fknn_sort.cuh"
+
+namespace fknn {
+
+constexpr int kPackSegment = 64;
+
+// cands[g] = number of candidate records of group g (sum of its 27 runs).
+__global__ void __launch_bounds__(256)
+    k_group_cands(const int2* __restrict__ runs, const int32_t* __restrict__ group_row,
+                  const int* group_count_ptr, int32_t* __restrict__ cands) {
+  const int64_t g = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (g >= *group_count_ptr) return;
+  const int64_t row = group_row ? group_row[g] : g;
+  const int2* r = runs + row * kNeighbours;
+  int total = 0;
+#pragma unroll
+  for (int j = 0; j < kNeighbours; ++j) total += max(r[j].y, 0);
+  cands[g] = total;
+}
+
+// One thread per segment of kPackSegment groups.  With items == nullptr it
+// only counts (seg_counts[seg]); otherwise it writes its items at
+// seg_offsets[seg].  Item = (q_start, q_count, g_first, g_count | flags).
+__global__ void __launch_bounds__(256)
+    k_pack(const int32_t* __restrict__ group_start, const int32_t* __restrict__ cands,
+           const int* group_count_ptr, int64_t n_segs, int tile, uint32_t* __restrict__ seg_counts,
+           const uint32_t* __restrict__ seg_offsets, int4* __restrict__ items) {
+  const int64_t seg = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (seg >= n_segs) return;
+  const int n_groups = *group_count_ptr;
+  const int64_t g_begin = seg * kPackSegment;
+  if (g_begin >= n_groups) {  // segments past the device-side group count hold nothing
+    if (!items) seg_counts[seg] = 0u;
+    return;
+  }
+  const int64_t g_lim = g_begin + kPackSegment;
+  const int g_end = static_cast<int>(g_lim < n_groups ? g_lim : n_groups);
+  uint32_t out = items ? seg_offsets[seg] : 0u;
+  uint32_t count = 0;
+  int cur_q0 = 0, cur_qn = 0, cur_g0 = 0, cur_gn = 0, cur_c = 0;
+  auto emit = [&](int q0, int qn, int g0, int gn, int flags) {
+    if (items) items[out + count] = make_int4(q0, qn, g0, gn | flags);
+    ++count;
+  };
+  auto flush = [&]() {
+    if (cur_gn > 0) emit(cur_q0, cur_qn, cur_g0, cur_gn, 0);
+    cur_qn = cur_gn = cur_c = 0;
+  };
+  for (int g = static_cast<int>(g_begin); g < g_end; ++g) {
+    const int gs = group_start[g], ge = group_start[g + 1];
+    const int c = cands[g];
+    if (ge <= gs) continue;
+    if (c > tile) {  // streams its candidates: items of its own
+      flush();
+      for (int s = gs; s < ge; s += 32) emit(s, min(32, ge - s), g, 1, kItemChunked);
+      continue;
+    }
+    int pos = gs;
+    while (pos < ge) {
+      // An item spans the groups [cur_g0, g]: groups without queries inside
+      // that span still count, because the kernel walks the span.
+      if (cur_gn > 0 && (cur_c + c > tile || cur_qn == 32 ||
+                         g - cur_g0 + 1 > kMaxGroupsPerItem))
+        flush();
+      if (cur_gn == 0) {
+        cur_q0 = pos;
+        cur_g0 = g;
+      }
+      const int take = min(ge - pos, 32 - cur_qn);
+      cur_qn += take;
+      cur_gn = g - cur_g0 + 1;
+      cur_c += c;
+      pos += take;
+    }
+  }
+  flush();
+  if (!items) seg_counts[seg] = count;
+}
+
+int launch_items(const int2* runs, const int32_t* group_start, const int32_t* group_row,
+                 const int* group_count_ptr, int64_t max_groups, int tile, int32_t* cands,
+                 uint32_t* seg_counts, int* n_items_ptr, int4* items, cudaStream_t s) {
+  if (max_groups <= 0) return 0;
+  const int gblocks = static_cast<int>(ceil_div(max_groups, 256));
+  const int64_t n_segs = ceil_div(max_groups, kPackSegment);
+  const int sblocks = static_cast<int>(ceil_div(n_segs, 256));
+  k_group_cands<<<gblocks, 256, 0, s>>>(runs, group_row, group_count_ptr, cands);
+  k_pack<<<sblocks, 256, 0, s>>>(group_start, cands, group_count_ptr, n_segs, tile, seg_counts,
+                                 nullptr, nullptr);
+  k_scan_tiles<<<1, 1024, 0, s>>>(seg_counts, static_cast<int>(n_segs), n_items_ptr);
+  k_pack<<<sblocks, 256, 0, s>>>(group_start, cands, group_count_ptr, n_segs, tile, nullptr,
+                                 seg_counts, items);
+  return 4;
+}
+
+size_t items_capacity(int64_t max_groups, int64_t n_queries) {
+  // every group yields at most ceil(q/32) + 1 items; every item holds >= 1 query
+  const int64_t a = n_queries + max_groups + 32;
+  return static_cast<size_t>(a);
+}
+
+}  // namespace fknn

@@ -8,18 +8,25 @@
 // (the reference leaves their order to its network layout).
 //
 // Execution model (B200-first, not the reference's block-per-parent loop):
-//   * persistent CTAs, one work item per warp at a time, pulled from a device
-//     queue (atomicAdd on Meta::queue_head);
-//   * the item's candidate runs are staged into the warp's shared-memory tile
-//     by non-multicast cp.async.bulk copies (one per run, issued by the lane
-//     that owns the run) completing on the warp's mbarrier; groups with more
-//     candidates than a tile are streamed tile by tile;
-//   * G lanes per query (G * queries <= 32) split the candidates; each lane
-//     keeps its K best as packed u64 keys (float bits << 32 | index) in
-//     registers, inserted by a branch-free shift network; a warp vote skips
-//     the insertion when no lane has an improving candidate;
-//   * the G partial lists are merged with xor-shuffle bitonic merges and the
-//     row is written straight to the caller's row / index space.
+//   * persistent CTAs; each warp pulls work items from a device queue
+//     (atomicAdd on Meta::queue_head);
+//   * packed item: up to 32 consecutive queries from up to 32 consecutive
+//     groups, one query per lane.  Each group's 27 runs are staged into the
+//     warp's shared-memory tile by non-multicast cp.async.bulk copies that
+//     complete on the warp's mbarrier.  Each group's candidates are then
+//     counting-sorted (32 buckets) by distance to the centroid of the
+//     group's queries, so every lane fills its list with near candidates
+//     first: the first KCAP candidates are sorted by a bitonic network, the
+//     rest go through a branch-free insertion network only when some lane
+//     improves (warp vote), and a lane stops at the first bucket whose lower
+//     distance bound exceeds its current K-th distance (triangle
+//     inequality, with a safety margin for FP32 rounding);
+//   * chunked item: one group with more candidates than a tile; G lanes per
+//     query split its candidates, streamed tile by tile, and the G partial
+//     lists are merged with xor-shuffle bitonic merges;
+//   * lists hold packed u64 keys (distance bits << 32 | index), so ordering
+//     is exact including ties; rows are written straight to the caller's
+//     row / index space.
 #include "fknn_common.cuh"
 #include "fknn_internal.h"
 
@@ -27,8 +34,34 @@ namespace fknn {
 
 constexpr uint64_t kEmpty = ~0ull;
 constexpr uint32_t kWaitLimit = 1u << 22;
+constexpr int kBuckets = 32;
+
+// Per-group scratch of the current packed item (shared memory, per warp).
+struct GroupSlot {
+  int seg;    // first tile slot of the group's candidates
+  int len;    // number of candidates
+  int a, b;   // the group's query range inside the item (query-record positions)
+  float cx, cy, cz;  // centroid of those queries
+  float inv_w;       // 1 / bucket width
+  float eps;         // absolute margin of the early-exit bound
+  int pad0, pad1, pad2;
+};
+static_assert(sizeof(GroupSlot) == 48, "GroupSlot layout");
+
+// Bytes of one warp's shared-memory region for a tile of T records.
+__host__ __device__ constexpr size_t warp_smem_bytes(int T) {
+  return ((static_cast<size_t>(T) * 20 + 16 + kMaxGroupsPerItem * sizeof(GroupSlot) +
+           kMaxGroupsPerItem * (kBuckets + 1) * 2 + 32 + kBuckets * 4 + 127) /
+          128) *
+         128;
+}
 
 __device__ __forceinline__ uint64_t umin64(uint64_t a, uint64_t b) { return a < b ? a : b; }
+
+__device__ __forceinline__ uint64_t make_key(float d, float w) {
+  return (static_cast<uint64_t>(__float_as_uint(d)) << 32) |
+         static_cast<uint32_t>(__float_as_int(w));
+}
 
 // Insert x into the ascending list L, dropping the largest entry.  Slot j
 // becomes min(L[j], max(x, L[j-1])): every slot is computed from the old
@@ -45,18 +78,36 @@ __device__ __forceinline__ void list_insert(uint64_t (&L)[KCAP], uint64_t x) {
 }
 
 template <int KCAP>
+__device__ __forceinline__ void cas(uint64_t (&L)[KCAP], int i, int j, bool ascending) {
+  const uint64_t a = L[i], b = L[j];
+  const bool sw = ascending ? (b < a) : (a < b);
+  L[i] = sw ? b : a;
+  L[j] = sw ? a : b;
+}
+
+// Full ascending bitonic sort of the register list.
+template <int KCAP>
+__device__ __forceinline__ void bitonic_sort(uint64_t (&L)[KCAP]) {
+#pragma unroll
+  for (int size = 2; size <= KCAP; size <<= 1) {
+#pragma unroll
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+#pragma unroll
+      for (int j = 0; j < KCAP; ++j) {
+        const int p = j ^ stride;
+        if (p > j) cas<KCAP>(L, j, p, (j & size) == 0);
+      }
+    }
+  }
+}
+
+template <int KCAP>
 __device__ __forceinline__ void bitonic_clean_ascending(uint64_t (&L)[KCAP]) {
 #pragma unroll
   for (int st = KCAP / 2; st > 0; st >>= 1) {
 #pragma unroll
-    for (int j = 0; j < KCAP; ++j) {
-      if ((j & st) == 0) {
-        const uint64_t a = L[j], b = L[j + st];
-        const bool sw = b < a;
-        L[j] = sw ? b : a;
-        L[j + st] = sw ? a : b;
-      }
-    }
+    for (int j = 0; j < KCAP; ++j)
+      if ((j & st) == 0) cas<KCAP>(L, j, j + st, true);
   }
 }
 
@@ -86,14 +137,120 @@ __device__ __forceinline__ void merge_with_lane(uint64_t (&L)[KCAP], int mask) {
 
 __device__ __forceinline__ int ceil_log2(int v) { return v <= 1 ? 0 : 32 - __clz(v - 1); }
 
+__device__ __forceinline__ float warp_sum(float v) {
+#pragma unroll
+  for (int s = 16; s > 0; s >>= 1) v += __shfl_xor_sync(kFull, v, s);
+  return v;
+}
+
+__device__ __forceinline__ float warp_max(float v) {
+#pragma unroll
+  for (int s = 16; s > 0; s >>= 1) v = fmaxf(v, __shfl_xor_sync(kFull, v, s));
+  return v;
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.expect_tx.relaxed.cta.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)),
+               "r"(bytes)
+               : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile(
+      "{\n\t.reg .b64 st;\n\tmbarrier.arrive.shared::cta.b64 st, [%0];\n\t}" ::"r"(smem_addr(bar))
+      : "memory");
+}
+
+// First sorted position whose bucket cannot hold a candidate closer than the
+// lane's current KCAP-th distance.  A candidate in bucket b lies at least
+// b*w from the centroid, hence at least b*w - rq from the query; buckets
+// with b*w > rq + sqrt(thr) (plus margins) are skipped.
+template <int KCAP>
+__device__ __forceinline__ int stop_position(const uint64_t (&L)[KCAP], const GroupSlot& s,
+                                             float rq, const uint16_t* bstart) {
+  const uint64_t last = L[KCAP - 1];
+  if (last == kEmpty) return s.len;
+  const float thr = __uint_as_float(static_cast<uint32_t>(last >> 32));
+  const float bnd = sqrtf(thr) * 1.0001f + s.eps;
+  const float lim = (rq + bnd) * s.inv_w;
+  if (!(lim < static_cast<float>(kBuckets - 1))) return s.len;
+  return bstart[static_cast<int>(lim) + 1];
+}
+
+template <typename IdxT, int KCAP, bool EXACT>
+__device__ __forceinline__ void write_row(const QueryLaunch& a, const uint64_t (&L)[KCAP], int row,
+                                          int k) {
+  if (row < 0 || row >= a.n_rows) {
+    raise_status(&a.meta->status, kStatusTable);
+    return;
+  }
+  int64_t pad;
+  switch (a.pad_mode) {
+    case kPadArray64: pad = static_cast<const int64_t*>(a.pad)[row]; break;
+    case kPadArray32: pad = static_cast<const int32_t*>(a.pad)[row]; break;
+    case kPadMinusOne: pad = -1; break;
+    default: pad = row; break;
+  }
+  IdxT* io = static_cast<IdxT*>(a.idx_out) + static_cast<int64_t>(row) * k;
+  float* dout = a.dist_out + static_cast<int64_t>(row) * k;
+  if (EXACT && (KCAP % 4) == 0 && a.vec_ok) {
+#pragma unroll
+    for (int j = 0; j < KCAP; j += 4) {
+      float4 dv;
+      IdxT iv[4];
+#pragma unroll
+      for (int t = 0; t < 4; ++t) {
+        const uint64_t e = L[j + t];
+        const bool empty = e == kEmpty;
+        iv[t] = empty ? static_cast<IdxT>(pad) : static_cast<IdxT>(static_cast<int32_t>(e));
+        reinterpret_cast<float*>(&dv)[t] =
+            empty ? __int_as_float(0x7f800000) : __uint_as_float(static_cast<uint32_t>(e >> 32));
+      }
+      *reinterpret_cast<float4*>(dout + j) = dv;
+      if constexpr (sizeof(IdxT) == 4) {
+        *reinterpret_cast<int4*>(io + j) = make_int4(iv[0], iv[1], iv[2], iv[3]);
+      } else {
+        *reinterpret_cast<longlong2*>(io + j) = make_longlong2(iv[0], iv[1]);
+        *reinterpret_cast<longlong2*>(io + j + 2) = make_longlong2(iv[2], iv[3]);
+      }
+    }
+  } else {
+#pragma unroll
+    for (int j = 0; j < KCAP; ++j) {
+      if (j < k) {
+        const uint64_t e = L[j];
+        const bool empty = e == kEmpty;
+        io[j] = empty ? static_cast<IdxT>(pad) : static_cast<IdxT>(static_cast<int32_t>(e));
+        dout[j] = empty ? __int_as_float(0x7f800000) : __uint_as_float(static_cast<uint32_t>(e >> 32));
+      }
+    }
+  }
+}
+
+__device__ __forceinline__ int2 load_run(const QueryLaunch& a, int row, int lane) {
+  int2 run = make_int2(0, 0);
+  if (lane < kNeighbours) run = a.runs[static_cast<int64_t>(row) * kNeighbours + lane];
+  if (run.y < 0 || run.x < 0 || static_cast<int64_t>(run.x) + run.y > a.n_support) {
+    raise_status(&a.meta->status, kStatusTable);
+    run.y = 0;
+  }
+  return run;
+}
+
 template <int KCAP, bool EXACT, typename IdxT>
-__global__ void __launch_bounds__(256) k_query(QueryLaunch a, int tile_records,
-                                               int min_cands_per_lane) {
+__global__ void __launch_bounds__(256) k_query(QueryLaunch a, int T, int min_cands_per_lane) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw) + warp;
-  float4* tile = reinterpret_cast<float4*>(smem_raw + 128) +
-                 static_cast<size_t>(warp) * tile_records;
+  unsigned char* wb = smem_raw + 128 + static_cast<size_t>(warp) * warp_smem_bytes(T);
+  float4* tile = reinterpret_cast<float4*>(wb);
+  uint16_t* tmp16 = reinterpret_cast<uint16_t*>(wb + static_cast<size_t>(T) * 16);
+  uint16_t* srt16 = tmp16 + T;
+  GroupSlot* slots =
+      reinterpret_cast<GroupSlot*>(wb + ((static_cast<size_t>(T) * 20 + 15) & ~size_t{15}));
+  uint16_t* bstart = reinterpret_cast<uint16_t*>(slots + kMaxGroupsPerItem);
+  uint8_t* qgroup = reinterpret_cast<uint8_t*>(bstart + kMaxGroupsPerItem * (kBuckets + 1));
+  uint32_t* hist = reinterpret_cast<uint32_t*>(qgroup + 32);
   Meta* meta = a.meta;
   if (lane == 0) {
     mbar_init(bar, 1);
@@ -102,6 +259,7 @@ __global__ void __launch_bounds__(256) k_query(QueryLaunch a, int tile_records,
   __syncwarp();
   uint32_t phase = 0;
   const int n_items = meta->n_items;
+  const int n_groups = *a.group_count_ptr;
   const int k = a.k;
 
   for (;;) {
@@ -110,134 +268,240 @@ __global__ void __launch_bounds__(256) k_query(QueryLaunch a, int tile_records,
     item = __shfl_sync(kFull, item, 0);
     if (item >= n_items) break;
     const int4 it = a.items[item];
-    const int q_start = it.y;
-    int q_count = it.z;
-    if (q_start < 0 || q_count < 0 || q_count > 32 ||
-        static_cast<int64_t>(q_start) + q_count > a.n_qrec) {
+    const int q0 = it.x, qn = it.y, g0 = it.z, gn = it.w & 0xffff;
+    const bool chunked = (it.w & kItemChunked) != 0;
+    if (q0 < 0 || qn < 1 || qn > 32 || static_cast<int64_t>(q0) + qn > a.n_qrec || g0 < 0 ||
+        gn < 1 || gn > kMaxGroupsPerItem || g0 + gn > n_groups || (chunked && gn != 1)) {
       if (lane == 0) raise_status(&meta->status, kStatusTable);
       continue;
     }
 
-    // Candidate runs, validated against the support array.
-    int2 run = make_int2(0, 0);
-    if (lane < kNeighbours) run = a.runs[static_cast<int64_t>(it.x) * kNeighbours + lane];
-    if (run.y < 0 || run.x < 0 || static_cast<int64_t>(run.x) + run.y > a.n_support) {
-      raise_status(&meta->status, kStatusTable);
-      run.y = 0;
-    }
-    const int incl = warp_inclusive_scan(run.y);
-    const int total = __shfl_sync(kFull, incl, 31);
-    const int run_off = incl - run.y;
-
-    // Lanes per query: as many as the queries leave free, but each lane
-    // should see at least min_cands_per_lane candidates.
-    int lg = 5 - ceil_log2(q_count > 0 ? q_count : 1);
-    while (lg > 0 && (total >> lg) < min_cands_per_lane) --lg;
-    const int G = 1 << lg;
-    const int qi = lane >> lg, sub = lane & (G - 1);
-    const bool active = qi < q_count;
-    float4 q = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (active) q = a.qrec[q_start + qi];
-
-    uint64_t L[KCAP];
+    if (chunked) {
+      // ------------------------------------------------ chunked item
+      const int row = a.group_row ? a.group_row[g0] : g0;
+      const int2 run = load_run(a, row, lane);
+      const int incl = warp_inclusive_scan(run.y);
+      const int total = __shfl_sync(kFull, incl, 31);
+      const int run_off = incl - run.y;
+      int lg = 5 - ceil_log2(qn);
+      while (lg > 0 && (total >> lg) < min_cands_per_lane) --lg;
+      const int G = 1 << lg;
+      const int qi = lane >> lg, sub = lane & (G - 1);
+      const bool active = qi < qn;
+      float4 q = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (active) q = a.qrec[q0 + qi];
+      uint64_t L[KCAP];
 #pragma unroll
-    for (int j = 0; j < KCAP; ++j) L[j] = kEmpty;
-    uint32_t thr = 0xffffffffu;
-
-    bool timed_out = false;
-    for (int c0 = 0; c0 < total; c0 += tile_records) {
-      const int c1 = min(total, c0 + tile_records);
-      __syncwarp();
-      fence_proxy_async_smem();  // earlier generic reads of the tile precede the copies
-      if (lane == 0) mbar_arrive_expect_tx(bar, static_cast<uint32_t>(c1 - c0) * 16u);
-      __syncwarp();
-      const int lo = max(run_off, c0), hi = min(run_off + run.y, c1);
-      if (hi > lo)
-        bulk_copy_g2s(tile + (lo - c0), a.srec + run.x + (lo - run_off),
-                      static_cast<uint32_t>(hi - lo) * 16u, bar);
-      if (!mbar_wait_bounded(bar, phase, kWaitLimit)) {
-        timed_out = true;
-        break;
-      }
-      phase ^= 1u;
-      const int cnt = c1 - c0;
-      for (int i0 = 0; i0 < cnt; i0 += G) {
-        const int i = i0 + sub;
-        const bool ok = active && i < cnt;
-        const float4 c = ok ? tile[i] : q;
-        const float d = sq_dist(c.x, c.y, c.z, q.x, q.y, q.z);
-        const uint32_t db = __float_as_uint(d);
-        const bool acc = ok && (d < a.cut_r2) && (db <= thr);
-        if (__any_sync(kFull, acc)) {
-          const uint64_t x =
-              acc ? ((static_cast<uint64_t>(db) << 32) | static_cast<uint32_t>(__float_as_int(c.w)))
-                  : kEmpty;
-          list_insert<KCAP>(L, x);
-          // The list holds the exact KCAP best, so its last entry is a valid
-          // (if K < KCAP, slightly loose) acceptance bound for the K best.
-          thr = static_cast<uint32_t>(L[KCAP - 1] >> 32);
+      for (int j = 0; j < KCAP; ++j) L[j] = kEmpty;
+      uint32_t thr = 0xffffffffu;
+      bool timed_out = false;
+      for (int c0 = 0; c0 < total; c0 += T) {
+        const int c1 = min(total, c0 + T);
+        __syncwarp();
+        fence_proxy_async_smem();  // earlier generic reads of the tile precede the copies
+        if (lane == 0) mbar_arrive_expect_tx(bar, static_cast<uint32_t>(c1 - c0) * 16u);
+        __syncwarp();
+        const int lo = max(run_off, c0), hi = min(run_off + run.y, c1);
+        if (hi > lo)
+          bulk_copy_g2s(tile + (lo - c0), a.srec + run.x + (lo - run_off),
+                        static_cast<uint32_t>(hi - lo) * 16u, bar);
+        if (!mbar_wait_bounded(bar, phase, kWaitLimit)) {
+          timed_out = true;
+          break;
+        }
+        phase ^= 1u;
+        const int cnt = c1 - c0;
+        for (int i0 = 0; i0 < cnt; i0 += G) {
+          const int i = i0 + sub;
+          const bool ok = active && i < cnt;
+          const float4 c = ok ? tile[i] : q;
+          const float d = sq_dist(c.x, c.y, c.z, q.x, q.y, q.z);
+          const uint32_t db = __float_as_uint(d);
+          const bool acc = ok && (d < a.cut_r2) && (db <= thr);
+          if (__any_sync(kFull, acc)) {
+            list_insert<KCAP>(L, acc ? make_key(d, c.w) : kEmpty);
+            thr = static_cast<uint32_t>(L[KCAP - 1] >> 32);
+          }
         }
       }
+      if (timed_out) {
+        if (lane == 0) raise_status(&meta->status, kStatusTimeout);
+        mbar_wait_bounded(bar, phase, kWaitLimit);  // let this warp's copies land
+        return;
+      }
+      for (int m = 1; m < G; m <<= 1) merge_with_lane<KCAP>(L, m);
+      if (active && sub == 0) write_row<IdxT, KCAP, EXACT>(a, L, __float_as_int(q.w), k);
+      continue;
     }
-    if (timed_out) {
+
+    // -------------------------------------------------- packed item
+    int ga = 0, gb = 0, grow = 0;
+    if (lane < gn) {
+      const int g = g0 + lane;
+      const int gs = a.group_start[g], ge = a.group_start[g + 1];
+      ga = max(gs, q0);
+      gb = max(ga, min(ge, q0 + qn));
+      grow = a.group_row ? a.group_row[g] : g;
+    }
+    __syncwarp();
+    fence_proxy_async_smem();  // earlier generic accesses of the tile precede the copies
+    __syncwarp();
+    int seg = 0;
+    bool overflow = false;
+    for (int gi = 0; gi < gn; ++gi) {
+      const int ga_ = __shfl_sync(kFull, ga, gi), gb_ = __shfl_sync(kFull, gb, gi);
+      const int row = __shfl_sync(kFull, grow, gi);
+      int len = 0;
+      if (gb_ > ga_ && !overflow) {
+        const int2 run = load_run(a, row, lane);
+        const int incl = warp_inclusive_scan(run.y);
+        len = __shfl_sync(kFull, incl, 31);
+        if (seg + len > T) {
+          overflow = true;
+          len = 0;
+        } else if (len > 0) {
+          if (lane == 0) mbar_expect_tx(bar, static_cast<uint32_t>(len) * 16u);
+          __syncwarp();
+          if (run.y > 0)
+            bulk_copy_g2s(tile + seg + (incl - run.y), a.srec + run.x,
+                          static_cast<uint32_t>(run.y) * 16u, bar);
+        }
+      }
+      if (lane == 0) {
+        GroupSlot s{};
+        s.seg = seg;
+        s.len = len;
+        s.a = ga_;
+        s.b = overflow ? ga_ : gb_;
+        slots[gi] = s;
+      }
+      seg += len;
+    }
+    if (lane == 0) mbar_arrive(bar);
+    if (!mbar_wait_bounded(bar, phase, kWaitLimit)) {
       if (lane == 0) raise_status(&meta->status, kStatusTimeout);
-      // Let this warp's copies land before the CTA may exit.
       mbar_wait_bounded(bar, phase, kWaitLimit);
       return;
     }
+    phase ^= 1u;
+    if (overflow) {  // the packer bounds every item by the tile; report a broken item
+      if (lane == 0) raise_status(&meta->status, kStatusTable);
+      continue;
+    }
+    // query -> group map (0xff: a query no group of the item covers)
+    qgroup[lane] = 0xffu;
+    __syncwarp();
+    if (lane < gn)
+      for (int p = ga; p < gb; ++p) qgroup[p - q0] = static_cast<uint8_t>(lane);
+    __syncwarp();
 
-    for (int m = 1; m < G; m <<= 1) merge_with_lane<KCAP>(L, m);
+    // Per group: centroid of its queries, distance buckets, counting sort.
+    for (int gi = 0; gi < gn; ++gi) {
+      const GroupSlot s = slots[gi];
+      if (s.b <= s.a) continue;
+      const int nq = s.b - s.a;
+      float4 qv = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (lane < nq) qv = a.qrec[s.a + lane];
+      const float inv_nq = 1.f / static_cast<float>(nq);
+      const float cx = warp_sum(qv.x) * inv_nq;
+      const float cy = warp_sum(qv.y) * inv_nq;
+      const float cz = warp_sum(qv.z) * inv_nq;
+      float dmax = 0.f;
+      for (int t = lane; t < s.len; t += 32) {
+        const float4 c = tile[s.seg + t];
+        const float dx = c.x - cx, dy = c.y - cy, dz = c.z - cz;
+        dmax = fmaxf(dmax, sqrtf(dx * dx + dy * dy + dz * dz));
+      }
+      dmax = warp_max(dmax);
+      const float w = dmax > 0.f ? dmax * (1.0f / kBuckets) * 1.0001f : 1.f;
+      const float inv_w = 1.f / w;
+      hist[lane] = 0u;  // kBuckets == 32: one bucket per lane
+      __syncwarp();
+      for (int t = lane; t < s.len; t += 32) {
+        const float4 c = tile[s.seg + t];
+        const float dx = c.x - cx, dy = c.y - cy, dz = c.z - cz;
+        const float dc = sqrtf(dx * dx + dy * dy + dz * dz);
+        const int bkt = min(static_cast<int>(dc * inv_w), kBuckets - 1);
+        const uint32_t r = atomicAdd(&hist[bkt], 1u);
+        tmp16[s.seg + t] = static_cast<uint16_t>((bkt << 10) | r);
+      }
+      __syncwarp();
+      const uint32_t h = hist[lane];
+      const uint32_t hi = static_cast<uint32_t>(warp_inclusive_scan(static_cast<int>(h)));
+      uint16_t* bs = bstart + gi * (kBuckets + 1);
+      bs[lane] = static_cast<uint16_t>(hi - h);
+      if (lane == 31) bs[kBuckets] = static_cast<uint16_t>(hi);
+      __syncwarp();
+      hist[lane] = hi - h;
+      __syncwarp();
+      for (int t = lane; t < s.len; t += 32) {
+        const uint16_t v = tmp16[s.seg + t];
+        const int bkt = v >> 10;
+        srt16[s.seg + hist[bkt] + (v & 1023)] = static_cast<uint16_t>((bkt << 10) | t);
+      }
+      if (lane == 0) {
+        const float mag = fmaxf(fabsf(cx), fmaxf(fabsf(cy), fabsf(cz))) + dmax;
+        slots[gi].cx = cx;
+        slots[gi].cy = cy;
+        slots[gi].cz = cz;
+        slots[gi].inv_w = inv_w;
+        slots[gi].eps = mag * 4e-6f + 1e-30f;
+      }
+      __syncwarp();
+    }
 
-    if (active && sub == 0) {
-      const int row = __float_as_int(q.w);
-      if (row < 0 || row >= a.n_rows) {
-        raise_status(&meta->status, kStatusTable);
-      } else {
-        int64_t pad;
-        switch (a.pad_mode) {
-          case kPadArray64: pad = static_cast<const int64_t*>(a.pad)[row]; break;
-          case kPadArray32: pad = static_cast<const int32_t*>(a.pad)[row]; break;
-          case kPadMinusOne: pad = -1; break;
-          default: pad = row; break;
-        }
-        IdxT* io = static_cast<IdxT*>(a.idx_out) + static_cast<int64_t>(row) * k;
-        float* dout = a.dist_out + static_cast<int64_t>(row) * k;
-        if (EXACT && (KCAP % 4) == 0 && a.vec_ok) {
+    // One query per lane.
+    const int mapped = lane < qn ? qgroup[lane] : 0;
+    if (lane < qn && mapped >= gn) raise_status(&meta->status, kStatusTable);
+    const bool active = lane < qn && mapped < gn;
+    const int gi = active ? mapped : 0;
+    const GroupSlot s = slots[gi];
+    const uint16_t* bs = bstart + gi * (kBuckets + 1);
+    float4 q = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (active) q = a.qrec[q0 + lane];
+    const float rdx = q.x - s.cx, rdy = q.y - s.cy, rdz = q.z - s.cz;
+    const float rq = sqrtf(rdx * rdx + rdy * rdy + rdz * rdz);
+    const int len = active ? s.len : 0;
+
+    uint64_t L[KCAP];
 #pragma unroll
-          for (int j = 0; j < KCAP; j += 4) {
-            float4 dv;
-            IdxT iv[4];
-#pragma unroll
-            for (int t = 0; t < 4; ++t) {
-              const uint64_t e = L[j + t];
-              const bool empty = e == kEmpty;
-              iv[t] = empty ? static_cast<IdxT>(pad) : static_cast<IdxT>(static_cast<int32_t>(e));
-              reinterpret_cast<float*>(&dv)[t] =
-                  empty ? __int_as_float(0x7f800000) : __uint_as_float(static_cast<uint32_t>(e >> 32));
-            }
-            *reinterpret_cast<float4*>(dout + j) = dv;
-            if constexpr (sizeof(IdxT) == 4) {
-              *reinterpret_cast<int4*>(io + j) = make_int4(iv[0], iv[1], iv[2], iv[3]);
-            } else {
-              *reinterpret_cast<longlong2*>(io + j) = make_longlong2(iv[0], iv[1]);
-              *reinterpret_cast<longlong2*>(io + j + 2) = make_longlong2(iv[2], iv[3]);
-            }
-          }
-        } else {
-#pragma unroll
-          for (int j = 0; j < KCAP; ++j) {
-            if (j < k) {
-              const uint64_t e = L[j];
-              const bool empty = e == kEmpty;
-              io[j] = empty ? static_cast<IdxT>(pad) : static_cast<IdxT>(static_cast<int32_t>(e));
-              dout[j] = empty ? __int_as_float(0x7f800000) : __uint_as_float(static_cast<uint32_t>(e >> 32));
-            }
-          }
+    for (int j = 0; j < KCAP; ++j) {
+      uint64_t key = kEmpty;
+      if (j < len) {
+        const uint16_t e = srt16[s.seg + j];
+        const float4 c = tile[s.seg + (e & 1023)];
+        const float d = sq_dist(c.x, c.y, c.z, q.x, q.y, q.z);
+        if (d < a.cut_r2) key = make_key(d, c.w);
+      }
+      L[j] = key;
+    }
+    bitonic_sort<KCAP>(L);
+    uint32_t thr = static_cast<uint32_t>(L[KCAP - 1] >> 32);
+    int stop = active ? stop_position<KCAP>(L, s, rq, bs) : 0;
+    for (int t = KCAP;; ++t) {
+      const bool live = t < stop;
+      if (!__any_sync(kFull, live)) break;
+      bool acc = false;
+      uint64_t x = kEmpty;
+      if (live) {
+        const uint16_t e = srt16[s.seg + t];
+        const float4 c = tile[s.seg + (e & 1023)];
+        const float d = sq_dist(c.x, c.y, c.z, q.x, q.y, q.z);
+        const uint32_t db = __float_as_uint(d);
+        acc = (d < a.cut_r2) && (db <= thr);
+        if (acc) x = make_key(d, c.w);
+      }
+      if (__any_sync(kFull, acc)) {
+        list_insert<KCAP>(L, x);
+        if (acc) {
+          thr = static_cast<uint32_t>(L[KCAP - 1] >> 32);
+          stop = min(stop, stop_position<KCAP>(L, s, rq, bs));
         }
       }
     }
+    if (active) write_row<IdxT, KCAP, EXACT>(a, L, __float_as_int(q.w), k);
+    __syncwarp();
   }
-  // Leave the barrier idle before the CTA exits.
   __syncwarp();
 }
 
@@ -257,10 +521,11 @@ QueryShape resolve_shape(const fknn_config* cfg) {
 bool shape_valid(const QueryShape& s) {
   const bool warps_ok = s.warps_per_cta == 1 || s.warps_per_cta == 2 ||
                         s.warps_per_cta == 4 || s.warps_per_cta == 8;
-  return warps_ok && s.tile_records >= 64 && s.tile_records <= 4096 &&
+  return warps_ok && s.tile_records >= 64 && s.tile_records <= 1024 &&
          s.tile_records % 32 == 0 && s.min_candidates_per_lane >= 1 &&
          s.ctas_per_sm >= 0 && s.ctas_per_sm <= 32 &&
-         128 + static_cast<size_t>(s.warps_per_cta) * s.tile_records * 16 <= 227 * 1024;
+         128 + static_cast<size_t>(s.warps_per_cta) * warp_smem_bytes(s.tile_records) <=
+             227 * 1024;
 }
 
 namespace {
@@ -269,7 +534,8 @@ template <int KCAP, bool EXACT, typename IdxT>
 int launch_t(const QueryLaunch& q, const QueryShape& shape, cudaStream_t s) {
   auto kern = k_query<KCAP, EXACT, IdxT>;
   const int threads = shape.warps_per_cta * 32;
-  const size_t smem = 128 + static_cast<size_t>(shape.warps_per_cta) * shape.tile_records * 16;
+  const size_t smem =
+      128 + static_cast<size_t>(shape.warps_per_cta) * warp_smem_bytes(shape.tile_records);
   // Device properties and occupancy are resolved once per (device, shape) and
   // cached, so a launch inside a CUDA graph capture issues nothing but the
   // kernel itself.

@@ -92,10 +92,6 @@ __global__ void k_tab_qrec(const float* __restrict__ xyz, int64_t n, const int32
                         __int_as_float(static_cast<int>(r)));
 }
 
-// Declared in fknn_grid.cu.
-__global__ void k_items(const int32_t* __restrict__ group_start, const int32_t* __restrict__ group_row,
-                        const int* group_count_ptr, Meta* meta, int4* __restrict__ items);
-
 namespace {
 
 inline int blocks_for(int64_t n, int per_block) {
@@ -108,6 +104,8 @@ struct TabBufs {
   float4* qrec;
   int2* runs;
   int4* items;
+  int32_t* cands;
+  uint32_t* seg_counts;
 };
 
 TabBufs tab_layout(void* ws, int64_t n, int64_t m, int64_t p, size_t* bytes) {
@@ -117,7 +115,9 @@ TabBufs tab_layout(void* ws, int64_t n, int64_t m, int64_t p, size_t* bytes) {
   b.srec = a.take<float4>(n);
   b.qrec = a.take<float4>(m);
   b.runs = a.take<int2>(static_cast<size_t>(p) * 27);
-  b.items = a.take<int4>(static_cast<size_t>(m + m / 32 + p + 32));
+  b.items = a.take<int4>(items_capacity(p, m));
+  b.cands = a.take<int32_t>(p);
+  b.seg_counts = a.take<uint32_t>(pack_segments(p));
   if (bytes) *bytes = a.used + 256;
   return b;
 }
@@ -153,11 +153,9 @@ int run_tables(const TablesArgs& t, void* ws, size_t ws_bytes, const QueryShape&
     k_tab_qrec<<<blocks_for(m, 256), 256, 0, s>>>(t.xyz_sorted, t.n, t.qindex, m, b.meta, b.qrec);
     ++nl;
   }
-  if (t.p > 0) {
-    k_items<<<blocks_for(t.p, 256), 256, 0, s>>>(selected ? t.steps_query : t.steps, nullptr,
-                                                 &b.meta->n_groups, b.meta, b.items);
-    ++nl;
-  }
+  if (t.p > 0)
+    nl += launch_items(b.runs, selected ? t.steps_query : t.steps, nullptr, &b.meta->n_groups, t.p,
+                       shape.tile_records, b.cands, b.seg_counts, &b.meta->n_items, b.items, s);
   e = cudaGetLastError();
   if (e != cudaSuccess) {
     note_cuda_error(e);
@@ -170,6 +168,9 @@ int run_tables(const TablesArgs& t, void* ws, size_t ws_bytes, const QueryShape&
     q.qrec = selected ? b.qrec : b.srec;
     q.n_qrec = static_cast<int>(m);
     q.runs = b.runs;
+    q.group_start = selected ? t.steps_query : t.steps;
+    q.group_row = nullptr;
+    q.group_count_ptr = &b.meta->n_groups;
     q.items = b.items;
     q.meta = b.meta;
     q.k = t.k;

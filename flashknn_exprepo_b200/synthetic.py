@@ -11,7 +11,8 @@ scans keep several returns per voxel in the near field.
   room           C2  ~80k points on a 6x8x3 m room + 10 boxes, sigma 5 mm, 4 cm voxels
   lidar          C3  64 rings x 2048 azimuths, ground + cylinders + boxes to 50 m,
                      10% dropped, 5 cm voxels
-  uneven_batch   C4  16 clouds, counts log-uniform in [20k, 200k], room / lidar mixed
+  uneven_batch   C4  16 clouds, counts log-uniform in [20k, 200k], room / lidar mixed,
+                     every cloud voxel-first deduplicated at the 5 cm grid voxel
   backward_weights C5 w ~ N(0,1) for the loss sum(w * d)
 """
 from __future__ import annotations
@@ -213,8 +214,30 @@ def draw_counts(n_clouds=16, lo=20000, hi=200000, seed=SEED, total=1_500_000, to
 
 
 def uneven_batch(n_clouds: int = 16, lo: int = 20000, hi: int = 200000, seed: int = SEED,
-                 voxel: float = 0.05, total: int = 1_500_000) -> Batch:
-    """C4: clouds with log-uniform sizes, alternating room-like / LiDAR-like."""
+                 voxel: float = 0.05, total: int = 1_500_000, cache: bool = True) -> Batch:
+    """C4: clouds with log-uniform sizes, alternating room-like / LiDAR-like.
+
+    Cached in the temp directory (keyed by the arguments), since generating
+    the ray-cast scans takes several seconds."""
+    import hashlib
+    import os
+    import tempfile
+    tag = hashlib.sha1(repr(("v2", n_clouds, lo, hi, seed, voxel, total)).encode()).hexdigest()[:12]
+    path = os.path.join(tempfile.gettempdir(), f"fknn_uneven_batch_{tag}.npz")
+    if cache and os.path.exists(path):
+        z = np.load(path, allow_pickle=False)
+        return Batch(xyz=z["xyz"], offsets=z["offsets"], counts=z["counts"],
+                     kinds=[str(k) for k in z["kinds"]], voxel=float(z["voxel"]))
+    batch = _uneven_batch(n_clouds, lo, hi, seed, voxel, total)
+    if cache:
+        tmp = path + f".{os.getpid()}.npz"
+        np.savez(tmp, xyz=batch.xyz, offsets=batch.offsets, counts=batch.counts,
+                 kinds=np.array(batch.kinds), voxel=np.float64(batch.voxel))
+        os.replace(tmp, path)
+    return batch
+
+
+def _uneven_batch(n_clouds, lo, hi, seed, voxel, total) -> Batch:
     counts, seed = draw_counts(n_clouds, lo, hi, seed, total)
     rng = np.random.default_rng(seed)
     clouds, kinds = [], []
@@ -226,14 +249,27 @@ def uneven_batch(n_clouds: int = 16, lo: int = 20000, hi: int = 200000, seed: in
                        dims=(6.0 * scale, 8.0 * scale, 3.0))
             kinds.append("room")
         else:
-            rings = 64 if target <= 100000 else 128
-            pts = lidar(seed=seed + 101 * i, rings=rings, voxel=voxel)
+            # voxel-first at the grid voxel, as the reference prepares its
+            # LiDAR frames (scripts/prepare_semantickitti_pack.py:39-43,84);
+            # enough rays that the deduplicated scan reaches the target size
+            rings, az = next(((r, a) for r, a, cap in ((64, 2048, 70000), (128, 2048, 110000),
+                                                       (128, 4096, 150000)) if target <= cap),
+                             (256, 4096))
+            pts = lidar(seed=seed + 101 * i, rings=rings, azimuths=az, voxel=voxel, dedup=True)
             kinds.append("lidar")
         pts = crop(pts, int(target), rng)
         clouds.append(pts.astype(np.float32))
     counts = np.array([len(c) for c in clouds], np.int64)
     return Batch(xyz=np.ascontiguousarray(np.concatenate(clouds)), offsets=np.cumsum(counts),
                  counts=counts, kinds=kinds, voxel=voxel)
+
+
+def first_clouds(batch: Batch, count: int) -> Batch:
+    """The first `count` clouds of a batch (smaller cases for profiling)."""
+    end = int(batch.offsets[count - 1])
+    return Batch(xyz=np.ascontiguousarray(batch.xyz[:end]), offsets=batch.offsets[:count].copy(),
+                 counts=batch.counts[:count].copy(), kinds=batch.kinds[:count],
+                 voxel=batch.voxel)
 
 
 def backward_weights(n: int, k: int, seed: int = SEED) -> np.ndarray:
