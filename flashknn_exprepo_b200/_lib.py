@@ -21,6 +21,7 @@ FKNN_ERR_WORKSPACE = -3
 FKNN_ERR_CUDA = -4
 FKNN_ERR_SIZE = -5
 FKNN_ERR_NUM_DOWN = -6
+FKNN_ERR_SCRATCH_LIMIT = -7
 
 DEVICE_COORD_RANGE = 1
 DEVICE_BAD_TABLE = 2
@@ -74,6 +75,8 @@ _SIGNATURES = {
     "fknn_tables_workspace_bytes": (_SZ, [_I64, _I64, _I64]),
     "fknn_query_tables": (ctypes.c_int, [_P, _I64, _P, _P, _P, _I64, _I32, _F32, _P, _P, _P, _SZ,
                                          _P, _P]),
+    "fknn_query_tables_noalloc": (ctypes.c_int, [_P, _I64, _P, _P, _P, _I64, _I32, _F32, _P, _P,
+                                                 _P]),
     "fknn_selected_query_tables": (ctypes.c_int, [_P, _I64, _P, _I64, _P, _P, _P, _P, _I64, _I32,
                                                   _F32, _P, _P, _P, _SZ, _P, _P]),
     "fknn_morton_encode": (ctypes.c_int, [_P, _P, _I64, _P, _P]),

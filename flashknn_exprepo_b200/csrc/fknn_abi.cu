@@ -107,6 +107,9 @@ const char* fknn_error_string(int code) {
     case FKNN_ERR_CUDA: return "CUDA launch failed";
     case FKNN_ERR_SIZE: return "too many points for 32-bit indexing";
     case FKNN_ERR_NUM_DOWN: return "num_down must lie in [0, 8]";
+    case FKNN_ERR_SCRATCH_LIMIT:
+      return "problem exceeds the built-in scratch of fknn_query_tables_noalloc "
+             "(at most 32768 points and 32768 parent cells)";
     default: return "unknown error";
   }
 }

@@ -44,6 +44,7 @@ extern "C" {
 #define FKNN_ERR_CUDA (-4)      /* a launch failed: see fknn_last_cuda_error() */
 #define FKNN_ERR_SIZE (-5)      /* more points than 32-bit indexing allows */
 #define FKNN_ERR_NUM_DOWN (-6)  /* num_down outside [0, 8] */
+#define FKNN_ERR_SCRATCH_LIMIT (-7) /* larger than the built-in scratch of fknn_query_tables_noalloc */
 
 /* --------------------------------------------------- device status bits */
 #define FKNN_DEVICE_COORD_RANGE 1 /* grid coordinate outside [-2^15, 2^15) */
@@ -126,6 +127,21 @@ FKNN_API int fknn_query_tables(const float* xyz_sorted, int64_t n, const int32_t
                       const int32_t* neigh, const int32_t* cnt, int64_t p, int32_t k,
                       float cut_r2, int32_t* idx_out, float* dist_out, void* workspace,
                       size_t workspace_bytes, const fknn_config* config, void* stream);
+
+/* No counterpart in the reference.  Same inputs, outputs and results as
+ * fknn_query_tables, for callers that cannot give the library device memory
+ * (a plugin whose host framework owns all device allocations, a real-time
+ * loop that must not allocate after start-up, a binding that only forwards
+ * tensors): the scratch is a fixed array inside the library (about 10 MiB on
+ * every GPU that loads it, kept until exit), so n and p are limited to 32768
+ * each; larger problems return FKNN_ERR_SCRATCH_LIMIT.  All calls on a device
+ * share that array: calls that overlap on the GPU race, so order them on one
+ * stream.  The first call on a device looks up the array's address with that
+ * device current; make it before any stream capture. */
+FKNN_API int fknn_query_tables_noalloc(const float* xyz_sorted, int64_t n, const int32_t* steps,
+                                       const int32_t* neigh, const int32_t* cnt, int64_t p,
+                                       int32_t k, float cut_r2, int32_t* idx_out,
+                                       float* dist_out, void* stream);
 
 /* Replaces FlashKNN_Selected_Query_DL (FlashKNN/csrc/flash_knn_query.h:206-218):
  * qindex int32 [m] (sorted support index of each query, grouped by parent
