@@ -17,6 +17,7 @@
 //                   heads per 2048-point tile
 //   k_scan_tiles    tile offsets -> number of cells
 //   k_cells         cell keys and starts (cells stay in key order)
+//   k_hash_*        open-addressing table of the cell keys
 //   k_runs          27 (start, count) candidate runs per cell / query group,
 //                   centre first, (0,-1,+1)^3 in ij order like the reference
 //                   neighbour table (flash_knn_construction.cu:42-63)
@@ -322,13 +323,64 @@ __device__ __forceinline__ int axis_offset(int position) {
   return position == 0 ? 0 : (position == 1 ? -1 : 1);
 }
 
-__device__ __forceinline__ int64_t find_key(const uint64_t* keys, int n, uint64_t key) {
-  int lo = 0, hi = n;
-  while (lo < hi) {
-    const int mid = (lo + hi) >> 1;
-    if (keys[mid] < key) lo = mid + 1; else hi = mid;
+// ------------------------------------------------------- cell hash table
+// Open addressing over the cell keys (linear probing, load <= 1/2): the
+// 27-neighbour lookup costs one or two L2 probes instead of a binary search
+// over all cells.  The table is sized from the device-side cell count, so
+// only the used prefix is cleared on every call.
+constexpr uint64_t kHashEmpty = ~0ull;
+
+__device__ __forceinline__ uint32_t hash_capacity(int cells) {
+  uint32_t cap = 16;
+  while (cap < 2u * static_cast<uint32_t>(cells)) cap <<= 1;
+  return cap;
+}
+
+__device__ __forceinline__ uint32_t hash_slot(uint64_t key, uint32_t mask) {
+  key ^= key >> 33;
+  key *= 0xff51afd7ed558ccdULL;
+  key ^= key >> 33;
+  key *= 0xc4ceb9fe1a85ec53ULL;
+  key ^= key >> 33;
+  return static_cast<uint32_t>(key) & mask;
+}
+
+__global__ void k_hash_clear(const int* cell_count_ptr, uint64_t* __restrict__ hkeys) {
+  const uint32_t cap = hash_capacity(*cell_count_ptr);
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < cap; i += gridDim.x * blockDim.x)
+    hkeys[i] = kHashEmpty;
+}
+
+__global__ void k_hash_insert(const uint64_t* __restrict__ cell_key, const int* cell_count_ptr,
+                              uint64_t* __restrict__ hkeys, int32_t* __restrict__ hvals) {
+  const int cells = *cell_count_ptr;
+  const uint32_t mask = hash_capacity(cells) - 1;
+  for (int64_t c = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; c < cells;
+       c += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const uint64_t key = cell_key[c];
+    uint32_t h = hash_slot(key, mask);
+    for (uint32_t probe = 0; probe <= mask; ++probe) {
+      const unsigned long long prev = atomicCAS(
+          reinterpret_cast<unsigned long long*>(hkeys + h), kHashEmpty, key);
+      if (prev == kHashEmpty || prev == key) {
+        hvals[h] = static_cast<int32_t>(c);
+        break;
+      }
+      h = (h + 1) & mask;
+    }
   }
-  return (lo < n && keys[lo] == key) ? lo : -1;
+}
+
+__device__ __forceinline__ int32_t hash_find(const uint64_t* hkeys, const int32_t* hvals,
+                                             uint32_t mask, uint64_t key) {
+  uint32_t h = hash_slot(key, mask);
+  for (uint32_t probe = 0; probe <= mask; ++probe) {
+    const uint64_t k = hkeys[h];
+    if (k == key) return hvals[h];
+    if (k == kHashEmpty) return -1;
+    h = (h + 1) & mask;
+  }
+  return -1;
 }
 
 // One thread per (group, neighbour position).  group_key[g] is a key in the
@@ -336,30 +388,34 @@ __device__ __forceinline__ int64_t find_key(const uint64_t* keys, int n, uint64_
 // offset j, or (0, 0) when that cell is empty.
 __global__ void __launch_bounds__(256)
     k_runs(const uint64_t* __restrict__ group_key, const int* group_count_ptr,
-           const uint64_t* __restrict__ cell_key, const int32_t* __restrict__ cell_start,
-           const int* cell_count_ptr, const Meta* meta, int2* __restrict__ runs) {
-  const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-  const int n_groups = *group_count_ptr;
-  if (t >= static_cast<int64_t>(n_groups) * kNeighbours) return;
-  const int g = static_cast<int>(t / kNeighbours), j = static_cast<int>(t % kNeighbours);
+           const uint64_t* __restrict__ hkeys, const int32_t* __restrict__ hvals,
+           const int32_t* __restrict__ cell_start, const int* cell_count_ptr, const Meta* meta,
+           int2* __restrict__ runs) {
+  const int64_t total = static_cast<int64_t>(*group_count_ptr) * kNeighbours;
   const int bpa = meta->bpa;
-  const uint64_t key = group_key[g];
+  const int cells = *cell_count_ptr;
+  const uint32_t hmask = hash_capacity(cells) - 1;
   const uint64_t mask = bpa ? ((1ull << (3 * bpa)) - 1) : 0ull;
-  const uint64_t cloud = key >> (3 * bpa);
-  const uint64_t m = key & mask;
-  const int x = static_cast<int>(compact3(m >> 2)) + axis_offset(j / 9);
-  const int y = static_cast<int>(compact3(m >> 1)) + axis_offset((j / 3) % 3);
-  const int z = static_cast<int>(compact3(m)) + axis_offset(j % 3);
   const int lim = 1 << bpa;
-  int2 run = make_int2(0, 0);
-  if (x >= 0 && y >= 0 && z >= 0 && x < lim && y < lim && z < lim) {
-    const uint64_t nk = (cloud << (3 * bpa)) |
-                        morton3(static_cast<uint32_t>(x), static_cast<uint32_t>(y),
-                                static_cast<uint32_t>(z));
-    const int64_t hit = find_key(cell_key, *cell_count_ptr, nk);
-    if (hit >= 0) run = make_int2(cell_start[hit], cell_start[hit + 1] - cell_start[hit]);
+  for (int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; t < total;
+       t += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int g = static_cast<int>(t / kNeighbours), j = static_cast<int>(t % kNeighbours);
+    const uint64_t key = group_key[g];
+    const uint64_t cloud = key >> (3 * bpa);
+    const uint64_t m = key & mask;
+    const int x = static_cast<int>(compact3(m >> 2)) + axis_offset(j / 9);
+    const int y = static_cast<int>(compact3(m >> 1)) + axis_offset((j / 3) % 3);
+    const int z = static_cast<int>(compact3(m)) + axis_offset(j % 3);
+    int2 run = make_int2(0, 0);
+    if (cells > 0 && x >= 0 && y >= 0 && z >= 0 && x < lim && y < lim && z < lim) {
+      const uint64_t nk = (cloud << (3 * bpa)) |
+                          morton3(static_cast<uint32_t>(x), static_cast<uint32_t>(y),
+                                  static_cast<uint32_t>(z));
+      const int32_t hit = hash_find(hkeys, hvals, hmask, nk);
+      if (hit >= 0) run = make_int2(cell_start[hit], cell_start[hit + 1] - cell_start[hit]);
+    }
+    runs[t] = run;
   }
-  runs[t] = run;
 }
 
 // ------------------------------------------------------ selected queries
@@ -450,6 +506,9 @@ struct Bufs {
   int4* items;
   int32_t* cands;
   uint32_t* seg_counts;
+  uint64_t* hkeys;
+  int32_t* hvals;
+  int64_t hash_cap;
 };
 
 Bufs layout(void* ws, int64_t n, int64_t m, int64_t n_clouds, int kind, size_t* bytes) {
@@ -474,6 +533,10 @@ Bufs layout(void* ws, int64_t n, int64_t m, int64_t n_clouds, int kind, size_t* 
   b.srec = a.take<float4>(n);
   b.cell_key = a.take<uint64_t>(n);
   b.cell_start = a.take<int32_t>(n + 1);
+  b.hash_cap = 16;
+  while (b.hash_cap < 2 * n) b.hash_cap <<= 1;
+  b.hkeys = a.take<uint64_t>(b.hash_cap);
+  b.hvals = a.take<int32_t>(b.hash_cap);
   if (kind == FKNN_QUERY_SELECTED) {
     b.pos_of = a.take<int32_t>(n);
     b.cell_of = a.take<int32_t>(n);
@@ -500,6 +563,14 @@ Bufs layout(void* ws, int64_t n, int64_t m, int64_t n_clouds, int kind, size_t* 
 
 inline int blocks_for(int64_t n, int per_block) {
   return static_cast<int>(ceil_div(n > 0 ? n : 1, per_block));
+}
+
+// Grid for kernels whose real extent is only known on the device: enough
+// blocks to fill the GPU, a grid-stride loop covers the rest.
+inline int capped_blocks(int64_t upper_threads) {
+  return static_cast<int>(ceil_div(upper_threads > 0 ? upper_threads : 1, 256) < 2048
+                              ? ceil_div(upper_threads > 0 ? upper_threads : 1, 256)
+                              : 2048);
 }
 
 }  // namespace
@@ -556,7 +627,11 @@ int run_fused(const FusedArgs& f, void* ws, size_t ws_bytes, const QueryShape& s
     k_scan_tiles<<<1, 1024, 0, s>>>(b.tile_counts, tiles, &b.meta->n_cells);
     k_cells<uint64_t><<<tiles, 256, 0, s>>>(n, sp64, key_bits, b.tile_counts,
                                             &b.meta->n_cells, b.cell_key, b.cell_start, b.cell_of);
-    nl += 3;
+    k_hash_clear<<<static_cast<int>(b.hash_cap < 1024 * 256 ? ceil_div(b.hash_cap, 256) : 1024), 256, 0,
+                   s>>>(&b.meta->n_cells, b.hkeys);
+    k_hash_insert<<<capped_blocks(n), 256, 0, s>>>(b.cell_key, &b.meta->n_cells, b.hkeys,
+                                                     b.hvals);
+    nl += 5;
   }
 
   const float4* qrec = b.srec;
@@ -570,8 +645,9 @@ int run_fused(const FusedArgs& f, void* ws, size_t ws_bytes, const QueryShape& s
 
   if (kind == FKNN_QUERY_SELF) {
     if (n > 0) {
-      k_runs<<<blocks_for(n * kNeighbours, 256), 256, 0, s>>>(
-          b.cell_key, &b.meta->n_cells, b.cell_key, b.cell_start, &b.meta->n_cells, b.meta, b.runs);
+      k_runs<<<capped_blocks(n * kNeighbours), 256, 0, s>>>(
+          b.cell_key, &b.meta->n_cells, b.hkeys, b.hvals, b.cell_start, &b.meta->n_cells, b.meta,
+          b.runs);
       ++nl;
       nl += launch_items(b.runs, b.cell_start, nullptr, &b.meta->n_cells, n, shape.tile_records,
                          b.cands, b.seg_counts, &b.meta->n_items, b.items, s);
@@ -585,8 +661,9 @@ int run_fused(const FusedArgs& f, void* ws, size_t ws_bytes, const QueryShape& s
     group_row = b.group_row;
     group_count_ptr = &b.meta->n_groups;
     if (n > 0) {
-      k_runs<<<blocks_for(n * kNeighbours, 256), 256, 0, s>>>(
-          b.cell_key, &b.meta->n_cells, b.cell_key, b.cell_start, &b.meta->n_cells, b.meta, b.runs);
+      k_runs<<<capped_blocks(n * kNeighbours), 256, 0, s>>>(
+          b.cell_key, &b.meta->n_cells, b.hkeys, b.hvals, b.cell_start, &b.meta->n_cells, b.meta,
+          b.runs);
       ++nl;
     }
     if (m > 0 && n > 0) {
@@ -629,9 +706,9 @@ int run_fused(const FusedArgs& f, void* ws, size_t ws_bytes, const QueryShape& s
       k_cells<uint64_t><<<tiles, 256, 0, s>>>(m, sp64, key_bits, b.tile_counts,
                                               &b.meta->n_groups, b.group_key, b.group_start,
                                               nullptr);
-      k_runs<<<blocks_for(m * kNeighbours, 256), 256, 0, s>>>(
-          b.group_key, &b.meta->n_groups, b.cell_key, b.cell_start, &b.meta->n_cells, b.meta,
-          b.runs);
+      k_runs<<<capped_blocks(m * kNeighbours), 256, 0, s>>>(
+          b.group_key, &b.meta->n_groups, b.hkeys, b.hvals, b.cell_start, &b.meta->n_cells,
+          b.meta, b.runs);
       nl += 4;
       nl += launch_items(b.runs, b.group_start, nullptr, &b.meta->n_groups, m, shape.tile_records,
                          b.cands, b.seg_counts, &b.meta->n_items, b.items, s);

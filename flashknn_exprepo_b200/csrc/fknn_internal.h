@@ -31,7 +31,7 @@ static_assert(sizeof(Meta) == 64, "Meta layout");
 // belong to the groups [g_first, g_first + g_count).  A chunked item has one
 // group whose candidates exceed a tile; they are streamed tile by tile.
 constexpr int kItemChunked = 1 << 30;
-constexpr int kMaxGroupsPerItem = 32;
+constexpr int kMaxGroupsPerItem = 16;
 
 // Resolved launch shape of the query kernel.
 struct QueryShape {
@@ -77,7 +77,10 @@ int launch_items(const int2* runs, const int32_t* group_start, const int32_t* gr
                  const int* group_count_ptr, int64_t max_groups, int tile, int32_t* cands,
                  uint32_t* seg_counts, int* n_items_ptr, int4* items, cudaStream_t s);
 size_t items_capacity(int64_t max_groups, int64_t n_queries);
-inline int64_t pack_segments(int64_t max_groups) { return (max_groups + 63) / 64; }
+constexpr int kPackSegment = 16;
+inline int64_t pack_segments(int64_t max_groups) {
+  return (max_groups + kPackSegment - 1) / kPackSegment;
+}
 
 // Bump allocator over a caller-provided workspace (256-byte aligned slices).
 struct Arena {

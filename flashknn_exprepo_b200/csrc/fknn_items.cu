@@ -9,29 +9,29 @@
 // stream their candidates tile by tile.
 //
 // Packing is a sequential greedy pass over the groups in key order; it runs
-// in parallel over segments of 64 groups (one thread each): a count pass,
-// a scan of the per-segment counts, and a write pass.  Items therefore keep
-// the spatial order of the groups.
+// in parallel over segments of kPackSegment groups (one thread each): a
+// count pass, a scan of the per-segment counts, and a write pass.  Items
+// therefore keep the spatial order of the groups.
 #include "fknn_common.cuh"
 #include "fknn_internal.h"
 #include "fknn_sort.cuh"
 
 namespace fknn {
 
-constexpr int kPackSegment = 64;
-
 // cands[g] = number of candidate records of group g (sum of its 27 runs).
 __global__ void __launch_bounds__(256)
     k_group_cands(const int2* __restrict__ runs, const int32_t* __restrict__ group_row,
                   const int* group_count_ptr, int32_t* __restrict__ cands) {
-  const int64_t g = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (g >= *group_count_ptr) return;
-  const int64_t row = group_row ? group_row[g] : g;
-  const int2* r = runs + row * kNeighbours;
-  int total = 0;
+  const int n_groups = *group_count_ptr;
+  for (int64_t g = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; g < n_groups;
+       g += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t row = group_row ? group_row[g] : g;
+    const int2* r = runs + row * kNeighbours;
+    int total = 0;
 #pragma unroll
-  for (int j = 0; j < kNeighbours; ++j) total += max(r[j].y, 0);
-  cands[g] = total;
+    for (int j = 0; j < kNeighbours; ++j) total += max(r[j].y, 0);
+    cands[g] = total;
+  }
 }
 
 // One thread per segment of kPackSegment groups.  With items == nullptr it
@@ -39,73 +39,92 @@ __global__ void __launch_bounds__(256)
 // seg_offsets[seg].  Item = (q_start, q_count, g_first, g_count | flags).
 __global__ void __launch_bounds__(256)
     k_pack(const int32_t* __restrict__ group_start, const int32_t* __restrict__ cands,
-           const int* group_count_ptr, int64_t n_segs, int tile, uint32_t* __restrict__ seg_counts,
+           const int* group_count_ptr, int tile, uint32_t* __restrict__ seg_counts,
            const uint32_t* __restrict__ seg_offsets, int4* __restrict__ items) {
-  const int64_t seg = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (seg >= n_segs) return;
   const int n_groups = *group_count_ptr;
-  const int64_t g_begin = seg * kPackSegment;
-  if (g_begin >= n_groups) {  // segments past the device-side group count hold nothing
-    if (!items) seg_counts[seg] = 0u;
-    return;
-  }
-  const int64_t g_lim = g_begin + kPackSegment;
-  const int g_end = static_cast<int>(g_lim < n_groups ? g_lim : n_groups);
-  uint32_t out = items ? seg_offsets[seg] : 0u;
-  uint32_t count = 0;
-  int cur_q0 = 0, cur_qn = 0, cur_g0 = 0, cur_gn = 0, cur_c = 0;
-  auto emit = [&](int q0, int qn, int g0, int gn, int flags) {
-    if (items) items[out + count] = make_int4(q0, qn, g0, gn | flags);
-    ++count;
-  };
-  auto flush = [&]() {
-    if (cur_gn > 0) emit(cur_q0, cur_qn, cur_g0, cur_gn, 0);
-    cur_qn = cur_gn = cur_c = 0;
-  };
-  for (int g = static_cast<int>(g_begin); g < g_end; ++g) {
-    const int gs = group_start[g], ge = group_start[g + 1];
-    const int c = cands[g];
-    if (ge <= gs) continue;
-    if (c > tile) {  // streams its candidates: items of its own
-      flush();
-      for (int s = gs; s < ge; s += 32) emit(s, min(32, ge - s), g, 1, kItemChunked);
-      continue;
-    }
-    int pos = gs;
-    while (pos < ge) {
-      // An item spans the groups [cur_g0, g]: groups without queries inside
-      // that span still count, because the kernel walks the span.
-      if (cur_gn > 0 && (cur_c + c > tile || cur_qn == 32 ||
-                         g - cur_g0 + 1 > kMaxGroupsPerItem))
+  const int64_t n_segs = (n_groups + kPackSegment - 1) / kPackSegment;
+  for (int64_t seg = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; seg < n_segs;
+       seg += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t g_begin = seg * kPackSegment;
+    const int64_t g_lim = g_begin + kPackSegment;
+    const int g_end = static_cast<int>(g_lim < n_groups ? g_lim : n_groups);
+    uint32_t out = items ? seg_offsets[seg] : 0u;
+    uint32_t count = 0;
+    int cur_q0 = 0, cur_qn = 0, cur_g0 = 0, cur_gn = 0, cur_c = 0;
+    auto emit = [&](int q0, int qn, int g0, int gn, int flags) {
+      if (items) items[out + count] = make_int4(q0, qn, g0, gn | flags);
+      ++count;
+    };
+    auto flush = [&]() {
+      if (cur_gn > 0) emit(cur_q0, cur_qn, cur_g0, cur_gn, 0);
+      cur_qn = cur_gn = cur_c = 0;
+    };
+    for (int g = static_cast<int>(g_begin); g < g_end; ++g) {
+      const int gs = group_start[g], ge = group_start[g + 1];
+      const int c = cands[g];
+      if (ge <= gs) continue;
+      if (c > tile) {  // streams its candidates: items of its own
         flush();
-      if (cur_gn == 0) {
-        cur_q0 = pos;
-        cur_g0 = g;
+        for (int q = gs; q < ge; q += 32) emit(q, min(32, ge - q), g, 1, kItemChunked);
+        continue;
       }
-      const int take = min(ge - pos, 32 - cur_qn);
-      cur_qn += take;
-      cur_gn = g - cur_g0 + 1;
-      cur_c += c;
-      pos += take;
+      int pos = gs;
+      while (pos < ge) {
+        // An item spans the groups [cur_g0, g]: groups without queries inside
+        // that span still count, because the kernel walks the span.
+        if (cur_gn > 0 && (cur_c + c > tile || cur_qn == 32 ||
+                           g - cur_g0 + 1 > kMaxGroupsPerItem))
+          flush();
+        if (cur_gn == 0) {
+          cur_q0 = pos;
+          cur_g0 = g;
+        }
+        const int take = min(ge - pos, 32 - cur_qn);
+        cur_qn += take;
+        cur_gn = g - cur_g0 + 1;
+        cur_c += c;
+        pos += take;
+      }
     }
+    flush();
+    if (!items) seg_counts[seg] = count;
   }
-  flush();
-  if (!items) seg_counts[seg] = count;
+}
+
+// Exclusive scan of the per-segment item counts over the segments that hold
+// groups (the device-side group count bounds the work).
+__global__ void __launch_bounds__(1024)
+    k_scan_segments(uint32_t* __restrict__ seg_counts, const int* group_count_ptr,
+                    int* __restrict__ total_out) {
+  __shared__ uint32_t warp_sums[32];
+  __shared__ uint32_t s_total;
+  const int n_segs = (*group_count_ptr + kPackSegment - 1) / kPackSegment;
+  uint32_t carry = 0;
+  for (int t0 = 0; t0 < n_segs; t0 += blockDim.x) {
+    const int t = t0 + threadIdx.x;
+    const uint32_t x = t < n_segs ? seg_counts[t] : 0u;
+    const uint32_t incl = block_inclusive_scan(x, warp_sums, &s_total);
+    if (t < n_segs) seg_counts[t] = carry + incl - x;
+    carry += s_total;
+  }
+  if (threadIdx.x == 0) *total_out = static_cast<int>(carry);
 }
 
 int launch_items(const int2* runs, const int32_t* group_start, const int32_t* group_row,
                  const int* group_count_ptr, int64_t max_groups, int tile, int32_t* cands,
                  uint32_t* seg_counts, int* n_items_ptr, int4* items, cudaStream_t s) {
   if (max_groups <= 0) return 0;
-  const int gblocks = static_cast<int>(ceil_div(max_groups, 256));
-  const int64_t n_segs = ceil_div(max_groups, kPackSegment);
-  const int sblocks = static_cast<int>(ceil_div(n_segs, 256));
+  // grids for the host-side bound, capped: the device count drives the loops
+  const int64_t gb = ceil_div(max_groups, 256);
+  const int gblocks = static_cast<int>(gb < 2048 ? gb : 2048);
+  const int64_t sb = ceil_div(ceil_div(max_groups, kPackSegment), 256);
+  const int sblocks = static_cast<int>(sb < 1024 ? sb : 1024);
   k_group_cands<<<gblocks, 256, 0, s>>>(runs, group_row, group_count_ptr, cands);
-  k_pack<<<sblocks, 256, 0, s>>>(group_start, cands, group_count_ptr, n_segs, tile, seg_counts,
-                                 nullptr, nullptr);
-  k_scan_tiles<<<1, 1024, 0, s>>>(seg_counts, static_cast<int>(n_segs), n_items_ptr);
-  k_pack<<<sblocks, 256, 0, s>>>(group_start, cands, group_count_ptr, n_segs, tile, nullptr,
-                                 seg_counts, items);
+  k_pack<<<sblocks, 256, 0, s>>>(group_start, cands, group_count_ptr, tile, seg_counts, nullptr,
+                                 nullptr);
+  k_scan_segments<<<1, 1024, 0, s>>>(seg_counts, group_count_ptr, n_items_ptr);
+  k_pack<<<sblocks, 256, 0, s>>>(group_start, cands, group_count_ptr, tile, nullptr, seg_counts,
+                                 items);
   return 4;
 }
 

@@ -14,9 +14,9 @@
 //     groups, one query per lane.  Each group's 27 runs are staged into the
 //     warp's shared-memory tile by non-multicast cp.async.bulk copies that
 //     complete on the warp's mbarrier.  Each group's candidates are then
-//     counting-sorted (32 buckets) by distance to the centroid of the
+//     counting-sorted (32 buckets of squared distance) by distance to the centroid of the
 //     group's queries, so every lane fills its list with near candidates
-//     first: the first KCAP candidates are sorted by a bitonic network, the
+//     first: the first KCAP candidates are sorted by a sorting network, the
 //     rest go through a branch-free insertion network only when some lane
 //     improves (warp vote), and a lane stops at the first bucket whose lower
 //     distance bound exceeds its current K-th distance (triangle
@@ -42,7 +42,7 @@ struct GroupSlot {
   int len;    // number of candidates
   int a, b;   // the group's query range inside the item (query-record positions)
   float cx, cy, cz;  // centroid of those queries
-  float inv_w;       // 1 / bucket width
+  float inv_w2;      // 1 / bucket width in squared distance
   float eps;         // absolute margin of the early-exit bound
   int pad0, pad1, pad2;
 };
@@ -77,6 +77,18 @@ __device__ __forceinline__ void list_insert(uint64_t (&L)[KCAP], uint64_t x) {
   L[0] = x < L[0] ? x : L[0];
 }
 
+// The same network over the upper half only: valid when x does not belong
+// in the lower half (x >= L[KCAP/2 - 1]), which leaves that half unchanged.
+template <int KCAP>
+__device__ __forceinline__ void list_insert_upper(uint64_t (&L)[KCAP], uint64_t x) {
+#pragma unroll
+  for (int j = KCAP - 1; j >= KCAP / 2; --j) {
+    const bool cj = x < L[j];
+    const bool cm = x < L[j - 1];
+    L[j] = cj ? (cm ? L[j - 1] : x) : L[j];
+  }
+}
+
 template <int KCAP>
 __device__ __forceinline__ void cas(uint64_t (&L)[KCAP], int i, int j, bool ascending) {
   const uint64_t a = L[i], b = L[j];
@@ -85,19 +97,76 @@ __device__ __forceinline__ void cas(uint64_t (&L)[KCAP], int i, int j, bool asce
   L[j] = sw ? a : b;
 }
 
-// Full ascending bitonic sort of the register list.
+// Ascending sorting networks for the fill (comparator counts 1, 5, 19, 60,
+// 185, 531 for 2..64 keys).  8 and 16 keys use published minimum-size
+// networks; larger sizes sort both halves and join them with Batcher's
+// odd-even merge.  Each network was checked with the 0-1 principle (all
+// 2^n binary inputs for n <= 16, all pairs of sorted binary halves for the
+// merges).
+// Inserts x (kEmpty = none).  Late improvements mostly belong in the upper
+// half of the list: when that holds for every lane, only that half is
+// updated.
 template <int KCAP>
-__device__ __forceinline__ void bitonic_sort(uint64_t (&L)[KCAP]) {
-#pragma unroll
-  for (int size = 2; size <= KCAP; size <<= 1) {
-#pragma unroll
-    for (int stride = size >> 1; stride > 0; stride >>= 1) {
-#pragma unroll
-      for (int j = 0; j < KCAP; ++j) {
-        const int p = j ^ stride;
-        if (p > j) cas<KCAP>(L, j, p, (j & size) == 0);
-      }
+__device__ __forceinline__ void insert_one(uint64_t (&L)[KCAP], uint64_t x) {
+  if constexpr (KCAP >= 8) {
+    if (__all_sync(kFull, x >= L[KCAP / 2 - 1])) {
+      list_insert_upper<KCAP>(L, x);
+      return;
     }
+  }
+  list_insert<KCAP>(L, x);
+}
+
+template <int KCAP>
+__device__ __forceinline__ void cas_up(uint64_t (&L)[KCAP], int i, int j) {
+  const uint64_t a = L[i], b = L[j];
+  const bool sw = b < a;
+  L[i] = sw ? b : a;
+  L[j] = sw ? a : b;
+}
+
+template <int KCAP, int LO, int N, int R>
+__device__ __forceinline__ void odd_even_merge(uint64_t (&L)[KCAP]) {
+  constexpr int M = R * 2;
+  if constexpr (M < N) {
+    odd_even_merge<KCAP, LO, N, M>(L);
+    odd_even_merge<KCAP, LO + R, N, M>(L);
+#pragma unroll
+    for (int i = LO + R; i + R < LO + N; i += M) cas_up<KCAP>(L, i, i + R);
+  } else {
+    cas_up<KCAP>(L, LO, LO + R);
+  }
+}
+
+template <int KCAP, int OFF, int N>
+__device__ __forceinline__ void sort_network(uint64_t (&L)[KCAP]) {
+  if constexpr (N == 2) {
+    cas_up<KCAP>(L, OFF, OFF + 1);
+  } else if constexpr (N == 4) {
+    constexpr int net[5][2] = {{0, 1}, {2, 3}, {0, 2}, {1, 3}, {1, 2}};
+#pragma unroll
+    for (int c = 0; c < 5; ++c) cas_up<KCAP>(L, OFF + net[c][0], OFF + net[c][1]);
+  } else if constexpr (N == 8) {
+    constexpr int net[19][2] = {{0, 2}, {1, 3}, {4, 6}, {5, 7}, {0, 4}, {1, 5}, {2, 6},
+                                {3, 7}, {0, 1}, {2, 3}, {4, 5}, {6, 7}, {2, 4}, {3, 5},
+                                {1, 4}, {3, 6}, {1, 2}, {3, 4}, {5, 6}};
+#pragma unroll
+    for (int c = 0; c < 19; ++c) cas_up<KCAP>(L, OFF + net[c][0], OFF + net[c][1]);
+  } else if constexpr (N == 16) {
+    constexpr int net[60][2] = {
+        {0, 13}, {1, 12}, {2, 15}, {3, 14}, {4, 8},  {5, 6},   {7, 11},  {9, 10},  {0, 5},
+        {1, 7},  {2, 9},  {3, 4},  {6, 13}, {8, 14}, {10, 15}, {11, 12}, {0, 1},   {2, 3},
+        {4, 5},  {6, 8},  {7, 9},  {10, 11}, {12, 13}, {14, 15}, {0, 2},  {1, 3},   {4, 10},
+        {5, 11}, {6, 7},  {8, 9},  {12, 14}, {13, 15}, {1, 2},  {3, 12},  {4, 6},   {5, 7},
+        {8, 10}, {9, 11}, {13, 14}, {1, 4}, {2, 6},   {5, 8},   {7, 10},  {9, 13},  {11, 14},
+        {2, 4},  {3, 6},  {9, 12}, {11, 13}, {3, 5},  {6, 8},   {7, 9},   {10, 12}, {3, 4},
+        {5, 6},  {7, 8},  {9, 10}, {11, 12}, {6, 7},  {8, 9}};
+#pragma unroll
+    for (int c = 0; c < 60; ++c) cas_up<KCAP>(L, OFF + net[c][0], OFF + net[c][1]);
+  } else if constexpr (N > 16) {
+    sort_network<KCAP, OFF, N / 2>(L);
+    sort_network<KCAP, OFF + N / 2, N / 2>(L);
+    odd_even_merge<KCAP, OFF, N, 1>(L);
   }
 }
 
@@ -162,17 +231,18 @@ __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
 }
 
 // First sorted position whose bucket cannot hold a candidate closer than the
-// lane's current KCAP-th distance.  A candidate in bucket b lies at least
-// b*w from the centroid, hence at least b*w - rq from the query; buckets
-// with b*w > rq + sqrt(thr) (plus margins) are skipped.
+// lane's current KCAP-th distance.  Buckets are uniform in the squared
+// distance to the centroid: a candidate in bucket b lies at least
+// sqrt(b*w2) from the centroid, hence at least sqrt(b*w2) - rq from the
+// query; buckets with b*w2 > (rq + sqrt(thr))^2 (plus margins) are skipped.
 template <int KCAP>
 __device__ __forceinline__ int stop_position(const uint64_t (&L)[KCAP], const GroupSlot& s,
                                              float rq, const uint16_t* bstart) {
   const uint64_t last = L[KCAP - 1];
   if (last == kEmpty) return s.len;
   const float thr = __uint_as_float(static_cast<uint32_t>(last >> 32));
-  const float bnd = sqrtf(thr) * 1.0001f + s.eps;
-  const float lim = (rq + bnd) * s.inv_w;
+  const float reach = rq + sqrtf(thr) * 1.0001f + s.eps;
+  const float lim = reach * reach * s.inv_w2;
   if (!(lim < static_cast<float>(kBuckets - 1))) return s.len;
   return bstart[static_cast<int>(lim) + 1];
 }
@@ -406,22 +476,22 @@ __global__ void __launch_bounds__(256) k_query(QueryLaunch a, int T, int min_can
       const float cx = warp_sum(qv.x) * inv_nq;
       const float cy = warp_sum(qv.y) * inv_nq;
       const float cz = warp_sum(qv.z) * inv_nq;
-      float dmax = 0.f;
+      float d2max = 0.f;
       for (int t = lane; t < s.len; t += 32) {
         const float4 c = tile[s.seg + t];
         const float dx = c.x - cx, dy = c.y - cy, dz = c.z - cz;
-        dmax = fmaxf(dmax, sqrtf(dx * dx + dy * dy + dz * dz));
+        d2max = fmaxf(d2max, dx * dx + dy * dy + dz * dz);
       }
-      dmax = warp_max(dmax);
-      const float w = dmax > 0.f ? dmax * (1.0f / kBuckets) * 1.0001f : 1.f;
-      const float inv_w = 1.f / w;
+      d2max = warp_max(d2max);
+      const float w2 = d2max > 0.f ? d2max * (1.0f / kBuckets) * 1.0001f : 1.f;
+      const float inv_w2 = 1.f / w2;
       hist[lane] = 0u;  // kBuckets == 32: one bucket per lane
       __syncwarp();
+      // Bucket of every candidate and its rank inside the bucket.
       for (int t = lane; t < s.len; t += 32) {
         const float4 c = tile[s.seg + t];
         const float dx = c.x - cx, dy = c.y - cy, dz = c.z - cz;
-        const float dc = sqrtf(dx * dx + dy * dy + dz * dz);
-        const int bkt = min(static_cast<int>(dc * inv_w), kBuckets - 1);
+        const int bkt = min(static_cast<int>((dx * dx + dy * dy + dz * dz) * inv_w2), kBuckets - 1);
         const uint32_t r = atomicAdd(&hist[bkt], 1u);
         tmp16[s.seg + t] = static_cast<uint16_t>((bkt << 10) | r);
       }
@@ -440,11 +510,11 @@ __global__ void __launch_bounds__(256) k_query(QueryLaunch a, int T, int min_can
         srt16[s.seg + hist[bkt] + (v & 1023)] = static_cast<uint16_t>((bkt << 10) | t);
       }
       if (lane == 0) {
-        const float mag = fmaxf(fabsf(cx), fmaxf(fabsf(cy), fabsf(cz))) + dmax;
+        const float mag = fmaxf(fabsf(cx), fmaxf(fabsf(cy), fabsf(cz))) + sqrtf(d2max);
         slots[gi].cx = cx;
         slots[gi].cy = cy;
         slots[gi].cz = cz;
-        slots[gi].inv_w = inv_w;
+        slots[gi].inv_w2 = inv_w2;
         slots[gi].eps = mag * 4e-6f + 1e-30f;
       }
       __syncwarp();
@@ -475,7 +545,7 @@ __global__ void __launch_bounds__(256) k_query(QueryLaunch a, int T, int min_can
       }
       L[j] = key;
     }
-    bitonic_sort<KCAP>(L);
+    sort_network<KCAP, 0, KCAP>(L);
     uint32_t thr = static_cast<uint32_t>(L[KCAP - 1] >> 32);
     int stop = active ? stop_position<KCAP>(L, s, rq, bs) : 0;
     for (int t = KCAP;; ++t) {
@@ -492,7 +562,7 @@ __global__ void __launch_bounds__(256) k_query(QueryLaunch a, int T, int min_can
         if (acc) x = make_key(d, c.w);
       }
       if (__any_sync(kFull, acc)) {
-        list_insert<KCAP>(L, x);
+        insert_one<KCAP>(L, x);
         if (acc) {
           thr = static_cast<uint32_t>(L[KCAP - 1] >> 32);
           stop = min(stop, stop_position<KCAP>(L, s, rq, bs));
@@ -508,7 +578,7 @@ __global__ void __launch_bounds__(256) k_query(QueryLaunch a, int T, int min_can
 // ------------------------------------------------------------------ host
 
 QueryShape resolve_shape(const fknn_config* cfg) {
-  QueryShape s{4, 512, 8, 0};
+  QueryShape s{4, 448, 8, 0};
   if (cfg) {
     if (cfg->warps_per_cta) s.warps_per_cta = cfg->warps_per_cta;
     if (cfg->tile_records) s.tile_records = cfg->tile_records;
