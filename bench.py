@@ -11,8 +11,9 @@ before every timed step, outside its events.
 
 Also reported on the same line: ``e2e`` (the public ``knn_query`` call with
 host buffers, H2D and D2H inside the timed region), the loop of plain
-per-cloud calls, forward+backward time, the query kernel's roofline and the
-CPU oracle timed on the host cores.
+per-cloud calls, forward+backward and backward-only time, the query
+kernel's roofline, recall@K against an FP64 brute force (timed), and the
+reference's CPU kNN (nanoflann) timed on the host cores.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--k 16]
 Under torchrun every rank takes a share of the clouds (whole clouds, largest
@@ -142,6 +143,18 @@ def measured_peak_hbm():
     return 6650.0, "fallback"
 
 
+def profiled_traffic(k):
+    """DRAM bytes (read + write) of one query-kernel launch on this workload,
+    from the committed ncu summary of that kernel; None when absent."""
+    path = os.path.join(ROOT, "profiles", f"k_query_uneven_batch_k{k}.txt")
+    if not os.path.exists(path):
+        return None
+    import re
+    with open(path) as f:
+        m = re.search(r"dram_bytes_per_launch\s*=\s*([0-9]+)", f.read())
+    return int(m.group(1)) if m else None
+
+
 def cpu_cores():
     try:
         return len(os.sched_getaffinity(0))
@@ -171,6 +184,25 @@ def cpu_oracle_rate(xyz, offsets, k, voxel, budget_s=20.0):
     return {"value": n / dt, "unit": "queries/s", "cores": cores, "kind": "port",
             "sample": f"first {take} of {len(offsets)} clouds ({n} points, construction + "
                       f"query), one pass, OpenMP x{cores}", "seconds": dt}
+
+
+def nanoflann_rate(batch, k, steps, warmup):
+    """The reference's CPU kNN (nanoflann, built from the reference's header
+    into oracle/_ref) over the whole batch on every host core: queries/s of
+    KD-tree construction + exact top-K, one pass over the batch per step."""
+    from oracle import ref_nanoflann
+    cores = cpu_cores()
+    n = int(len(batch.xyz))
+    for _ in range(warmup):
+        ref_nanoflann.knn(batch.xyz, batch.offsets, k, nthreads=cores)
+    secs = []
+    for _ in range(steps):
+        _, _, tb, tq = ref_nanoflann.knn(batch.xyz, batch.offsets, k, nthreads=cores)
+        secs.append(tb + tq)
+    return {"value": n * len(secs) / sum(secs), "unit": "queries/s", "cores": cores,
+            "kind": "reference",
+            "sample": f"whole batch ({n} points, {len(batch.offsets)} clouds) x {steps} passes: "
+                      f"nanoflann KD-tree build (leaf 20) + exact K={k} query, OpenMP x{cores}"}
 
 
 # --------------------------------------------------------------- our arm
@@ -362,37 +394,103 @@ def extras_single_gpu(args, fk, torch, dev, batch, voxel, flush):
         e1.synchronize()
         ms.append(e0.elapsed_time(e1))
     res["fwd_bwd_ms"] = sum(ms) / reps
+
+    # the backward kernels alone, on the forward's outputs
+    x = xyz.detach()
+    idx, d = fk.ops.knn_offsets(x, off, k, voxel, 2)
+    g = w * torch.isfinite(d).to(w.dtype)
+    grad = torch.empty_like(x)
+    for _ in range(2):
+        fk.ops.backward(x, x, idx, d, g, grad_q=grad, grad_p=grad, accumulate=True)
+    torch.cuda.synchronize(dev)
+    ms = []
+    for _ in range(reps):
+        flush.zero_()
+        grad.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        fk.ops.backward(x, x, idx, d, g, grad_q=grad, grad_p=grad, accumulate=True)
+        e1.record()
+        e1.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    res["backward_ms"] = sum(ms) / reps
+    res["recall"] = fp64_recall(batch, idx.cpu().numpy(), k)
     return res
+
+
+def fp64_recall(batch, idx, k, per_cloud=256):
+    """recall@K of the grid kNN against an exact FP64 brute force over whole
+    clouds, on a seeded sample of queries per cloud; the brute force runs on
+    every host core and is timed."""
+    from oracle import oracle as O
+    rng = np.random.default_rng(47)
+    starts = np.concatenate([[0], batch.offsets[:-1]])
+    rows = np.concatenate([np.sort(rng.choice(np.arange(s, e), min(per_cloud, e - s),
+                                              replace=False))
+                           for s, e in zip(starts, batch.offsets)])
+    q_off = np.cumsum([min(per_cloud, e - s) for s, e in zip(starts, batch.offsets)])
+    cores = cpu_cores()
+    t0 = time.perf_counter()
+    exact, _ = O.brute_knn_f64(batch.xyz, batch.offsets, k, batch.xyz[rows], q_off,
+                               nthreads=cores)
+    dt = time.perf_counter() - t0
+    rec = O.set_recall(idx[rows], exact)
+    return {"recall_at_k": float(rec.mean()), "rows": int(len(rows)),
+            "fp64_brute_force": {"value": len(rows) / dt, "unit": "queries/s", "cores": cores,
+                                 "sample": f"{per_cloud} seeded queries per cloud against "
+                                           f"the whole cloud"}}
 
 
 # ---------------------------------------------------------- reference arm
 
 def run_reference(args):
-    """CPU arm: the oracle port of the reference path on every host core,
-    plus (when a GPU and the sm_100a reference build are present) the
-    reference's own per-cloud GPU pipeline for context."""
+    """The reference's CPU kNN path, timed on every host core: nanoflann
+    (KD-tree, leaf 20, exact FP32 top-K, the reference's own nanoflann.hpp
+    built into oracle/_ref) over every cloud of the batch, construction and
+    query, one step = one pass over the 16 clouds.  Falls back to the oracle
+    port of the grid path when the nanoflann build is missing.  Also reported:
+    nanoflann on one thread (as the reference runs it), the oracle port, and
+    the reference's own per-cloud GPU pipeline for context."""
     from flashknn_exprepo_b200 import synthetic
+    from oracle import ref_nanoflann
     batch = synthetic.uneven_batch()
     k = args.k
     voxel = synthetic.C4_VOXEL
-    rates = []
-    cpu = None
-    for _ in range(max(1, args.steps)):
-        cpu = cpu_oracle_rate(batch.xyz, batch.offsets, k, voxel,
-                              budget_s=max(2.0, 60.0 / max(1, args.steps)))
-        rates.append(cpu["value"])
-    value = statistics.median(rates)
+    cores = cpu_cores()
+    n = int(len(batch.xyz))
+    extra = {}
+    if ref_nanoflann.available():
+        cpu = nanoflann_rate(batch, k, max(1, args.steps), max(0, args.warmup))
+        value = cpu["value"]
+        sub = synthetic.first_clouds(batch, 2)
+        _, _, tb, tq = ref_nanoflann.knn(sub.xyz, sub.offsets, k, nthreads=1)
+        extra["nanoflann_single_thread"] = {
+            "value": len(sub.xyz) / (tb + tq), "unit": "queries/s", "cores": 1,
+            "sample": f"first 2 clouds ({len(sub.xyz)} points), build + query"}
+        port = cpu_oracle_rate(batch.xyz, batch.offsets, k, voxel, budget_s=10.0)
+        port.pop("seconds", None)
+        extra["grid_port"] = port
+    else:
+        rates = []
+        for _ in range(max(1, args.steps)):
+            cpu = cpu_oracle_rate(batch.xyz, batch.offsets, k, voxel,
+                                  budget_s=max(2.0, 60.0 / max(1, args.steps)))
+            rates.append(cpu["value"])
+        cpu.pop("seconds", None)
+        value = statistics.median(rates)
+        cpu["value"] = value
     line = {"impl": "reference", "metric": "kNN queries/s at K=16 (batched uneven 16-cloud, "
                                            "construction + query)",
             "value": value, "unit": "queries/s", "higher_is_better": True,
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "dtype": "f32", "data": "synthetic (seeded, stands in for S3DIS/SemanticKITTI)",
-            "config": {"workload": "uneven_batch_16clouds_k16", "n_points": int(len(batch.xyz)),
+            "config": {"workload": "uneven_batch_16clouds_k16", "n_points": n,
                        "k": k, "voxel_m": voxel, "num_down": 2},
-            "cpu_baseline": {"value": value, "unit": "queries/s", "cores": cpu["cores"],
-                             "kind": cpu["kind"], "sample": cpu["sample"]},
+            "cpu_baseline": cpu,
             "e2e": {"value": value, "unit": "queries/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
+    line.update(extra)
     try:
         line["reference_gpu_per_cloud"] = reference_gpu_per_cloud(batch, k, voxel)
     except Exception as exc:  # context only: never fails the CPU arm
@@ -472,7 +570,7 @@ def main():
         avg = sum(kern) / len(kern)
         achieved = algo_bytes / (avg * 1e-3) / 1e9
         roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                    "frac": achieved / peak, "traffic": None,
+                    "frac": achieved / peak, "traffic": profiled_traffic(k),
                     "kernel": "fknn::k_query<16>", "kernel_ms": avg,
                     "algorithmic_bytes_per_launch": algo_bytes,
                     "peak_source": f"{peak_kind} hbm_gbs"}
@@ -496,11 +594,23 @@ def main():
         line["batched_vs_per_cloud"] = out["value"] / out["per_cloud"]["value"]
     if "fwd_bwd_ms" in out:
         line["fwd_bwd_ms"] = out["fwd_bwd_ms"]
+    if kern:
+        line["phases_ms"] = {"construction": out["ms_per_step"] - roofline["kernel_ms"],
+                             "query": roofline["kernel_ms"],
+                             "backward": out.get("backward_ms")}
+    if "recall" in out:
+        line["recall"] = out["recall"]
     if world == 1 and not args.no_extras:
         from flashknn_exprepo_b200 import synthetic
         b = synthetic.uneven_batch()
-        line["cpu_baseline"] = cpu_oracle_rate(b.xyz, b.offsets, k, synthetic.C4_VOXEL)
-        line["cpu_baseline"].pop("seconds", None)
+        from oracle import ref_nanoflann
+        port = cpu_oracle_rate(b.xyz, b.offsets, k, synthetic.C4_VOXEL, budget_s=10.0)
+        port.pop("seconds", None)
+        if ref_nanoflann.available():
+            line["cpu_baseline"] = nanoflann_rate(b, k, 3, 1)
+            line["grid_port_cpu"] = port
+        else:
+            line["cpu_baseline"] = port
     print(json.dumps(line))
     if dist is not None:
         dist.destroy_process_group()

@@ -11,10 +11,17 @@ flash_knn_construction.cu -- with the reference's own nvcc flags (-O2
 oracle/ref_bindings.cpp.  The reference's setup.py is not used.
 
 Load the result with ``oracle.ref_kernels.load()``.
+
+``build_nanoflann`` compiles the reference's CPU kNN baseline -- nanoflann
+over Query/ThirdParty/nanoflannkdtree/csrcs/nanoflann.hpp, with the
+reference's flags (-O3 -mavx2 -funroll-loops) -- through the C binding
+oracle/ref_nanoflann.cpp into oracle/_ref/libref_nanoflann.so (load it with
+``oracle.ref_nanoflann``).
 """
 from __future__ import annotations
 
 import os
+import subprocess
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -46,5 +53,19 @@ def build(reference: str | None = None, verbose: bool = False) -> str:
     return mod.__file__
 
 
+def build_nanoflann(reference: str | None = None) -> str:
+    reference = reference or os.environ.get("FKNN_REFERENCE", "/root/reference")
+    inc = os.path.join(reference, "Query", "ThirdParty", "nanoflannkdtree", "csrcs")
+    if not os.path.isfile(os.path.join(inc, "nanoflann.hpp")):
+        raise FileNotFoundError(f"nanoflann.hpp not found under {inc}")
+    os.makedirs(OUT, exist_ok=True)
+    out = os.path.join(OUT, "libref_nanoflann.so")
+    subprocess.run(["g++", "-O3", "-mavx2", "-funroll-loops", "-fopenmp", "-fPIC", "-shared",
+                    "-std=c++17", "-I", inc, os.path.join(HERE, "ref_nanoflann.cpp"), "-o", out],
+                   check=True)
+    return out
+
+
 if __name__ == "__main__":
     print(build(verbose="--verbose" in sys.argv))
+    print(build_nanoflann())

@@ -177,3 +177,20 @@ def test_backward_f64_matches_finite_differences():
                 fd = (loss(ap if arr is q else q, p if arr is q else ap)
                       - loss(am if arr is q else q, p if arr is q else am)) / (2 * h)
                 assert abs(fd - grad[i, a]) <= 1e-6 * max(1.0, abs(fd))
+
+
+def test_reference_nanoflann_baseline_is_exact_knn():
+    """The reference's CPU kNN (nanoflann, built into oracle/_ref) returns the
+    exact neighbours; it is the CPU baseline the bench times."""
+    from oracle import ref_nanoflann
+    if not ref_nanoflann.available():
+        pytest.skip("oracle/_ref/libref_nanoflann.so not built")
+    rng = np.random.default_rng(9)
+    xyz = rng.random((3000, 3), dtype=np.float32)
+    offs = np.array([1200, 3000])
+    idx, dist, _, _ = ref_nanoflann.knn(xyz, offs, 8, ordered=True, nthreads=2)
+    bi, bd = O.brute_knn_f64(xyz, offs, 8)
+    assert np.allclose(dist, bd, rtol=1e-5, atol=1e-9)
+    start = np.repeat([0, 1200], [1200, 1800])[:, None]
+    hit = (idx.astype(np.int64) + start == bi)
+    assert hit.mean() > 0.999  # equal-distance order aside
