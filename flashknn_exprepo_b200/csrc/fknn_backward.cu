@@ -4,25 +4,40 @@
 //   grad_q[i] = sum_j 2 g_ij (q_i - p[idx_ij])          (one thread per query,
 //                                                        j in ascending order)
 //   grad_p[n] = sum_{idx_ij = n} -2 g_ij (q_i - p_n)     (segmented reduction)
-// The reference-side sum runs over the (i, j) entries grouped by neighbour
-// index with a stable radix sort of (idx, i*K+j); each segment is summed in
-// ascending i*K+j order, so the result does not depend on scheduling and is
-// bitwise reproducible.  No floating-point atomics are used.
+// The reference-side sum is a segmented reduction over the entries sorted by
+// neighbour index: a counting sort by idx (integer atomics count each
+// segment, a scan places the segments, a scatter fills them), then one
+// thread per support point orders its segment by entry number e = i*K+j
+// (a register sorting network; a warp-cooperative selection for segments
+// longer than 32) and sums it sequentially in ascending e.  Every FP32
+// operation therefore happens in an order fixed by the inputs alone: the
+// gradients are bitwise reproducible, and no floating-point atomics are used.
 #include "fknn_common.cuh"
 #include "fknn_internal.h"
+#include "fknn_networks.cuh"
 #include "fknn_sort.cuh"
 #include "fknn_backward.h"
 
 namespace fknn {
 
-// One thread per query: grad_q, and the (neighbour index, entry) pairs.
-// Padding entries (dist == +inf or idx outside [0, n)) get the key n, which
-// sorts after every real index and is never summed.
+namespace {
+
+constexpr int kScanTile = 1024;
+constexpr uint64_t kNoPair = ~0ull;
+
+__device__ __forceinline__ bool entry_valid(int32_t t, int64_t n, float d) {
+  return t >= 0 && t < n && !isinf(d);
+}
+
+}  // namespace
+
+// One thread per query: grad_q over j in ascending order, and the size of
+// every neighbour's segment (count[t], integer atomics).
 __global__ void __launch_bounds__(256)
     k_bwd_query(const float* __restrict__ q_xyz, int64_t m, const float* __restrict__ p_xyz,
                 int64_t n, const int32_t* __restrict__ idx, const float* __restrict__ dist,
                 const float* __restrict__ grad, int k, float* __restrict__ grad_q, int accumulate,
-                uint32_t* __restrict__ keys, uint32_t* __restrict__ vals) {
+                uint32_t* __restrict__ count) {
   const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (i >= m) return;
   const float qx = q_xyz[3 * i], qy = q_xyz[3 * i + 1], qz = q_xyz[3 * i + 2];
@@ -30,12 +45,9 @@ __global__ void __launch_bounds__(256)
   for (int j = 0; j < k; ++j) {
     const int64_t e = i * k + j;
     const int32_t t = idx[e];
-    const bool valid = t >= 0 && t < n && !isinf(dist[e]);
-    if (keys) {
-      keys[e] = valid ? static_cast<uint32_t>(t) : static_cast<uint32_t>(n);
-      vals[e] = static_cast<uint32_t>(e);
-    }
-    if (!valid) continue;
+    if (!entry_valid(t, n, dist[e])) continue;
+    if (count) atomicAdd(&count[t], 1u);
+    if (!grad_q) continue;
     const float g2 = 2.f * grad[e];
     gx = __fmaf_rn(g2, __fsub_rn(qx, p_xyz[3 * static_cast<int64_t>(t)]), gx);
     gy = __fmaf_rn(g2, __fsub_rn(qy, p_xyz[3 * static_cast<int64_t>(t) + 1]), gy);
@@ -53,49 +65,157 @@ __global__ void __launch_bounds__(256)
   }
 }
 
-// Segment bounds in the sorted pairs: first[key] / last[key] (exclusive);
-// both arrays are zeroed beforehand, so indices without entries stay empty.
-__global__ void k_bwd_bounds(int64_t total, SortPair<uint32_t> sp, const int* bits_ptr,
-                             uint32_t n, uint32_t* __restrict__ first, uint32_t* __restrict__ last) {
-  const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (t >= total) return;
-  const uint32_t* keys = sp.keys[sort_passes_for_bits(*bits_ptr) & 1];
-  const uint32_t key = keys[t];
-  if (key >= n) return;
-  if (t == 0 || keys[t - 1] != key) first[key] = static_cast<uint32_t>(t);
-  if (t == total - 1 || keys[t + 1] != key) last[key] = static_cast<uint32_t>(t + 1);
+// Segment sizes summed per tile of kScanTile support points.
+__global__ void __launch_bounds__(kScanTile)
+    k_bwd_tile_sums(const uint32_t* __restrict__ count, int64_t n,
+                    uint32_t* __restrict__ tile_sums) {
+  __shared__ uint32_t warp_sums[32];
+  __shared__ uint32_t s_total;
+  const int64_t p = static_cast<int64_t>(blockIdx.x) * kScanTile + threadIdx.x;
+  block_inclusive_scan(p < n ? count[p] : 0u, warp_sums, &s_total);
+  if (threadIdx.x == 0) tile_sums[blockIdx.x] = s_total;
 }
 
-// One thread per support point: ordered sum over its segment.
+// start[p] = first slot of p's segment, cursor[p] = one past its last slot
+// (the scatter counts it down); start[n] = number of valid entries.
+__global__ void __launch_bounds__(kScanTile)
+    k_bwd_starts(const uint32_t* __restrict__ count, int64_t n,
+                 const uint32_t* __restrict__ tile_offsets, uint32_t* __restrict__ start,
+                 uint32_t* __restrict__ cursor) {
+  __shared__ uint32_t warp_sums[32];
+  const int64_t p = static_cast<int64_t>(blockIdx.x) * kScanTile + threadIdx.x;
+  const uint32_t c = p < n ? count[p] : 0u;
+  const uint32_t incl = block_inclusive_scan(c, warp_sums, nullptr) + tile_offsets[blockIdx.x];
+  if (p < n) {
+    start[p] = incl - c;
+    cursor[p] = incl;
+    if (p == n - 1) start[n] = incl;
+  }
+}
+
+// One thread per entry: scatter (e << 32 | bits of -2 g_e) into the
+// segment of its neighbour.  The slot order inside a segment depends on the
+// scheduling; the reduction below orders each segment by e.
 __global__ void __launch_bounds__(256)
-    k_bwd_support(const float* __restrict__ q_xyz, const float* __restrict__ p_xyz, int64_t n,
-                  const float* __restrict__ grad, int k, SortPair<uint32_t> sp,
-                  const int* bits_ptr, const uint32_t* __restrict__ first,
-                  const uint32_t* __restrict__ last, float* __restrict__ grad_p, int accumulate) {
-  const int64_t p = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (p >= n) return;
-  const uint32_t* vals = sp.vals[sort_passes_for_bits(*bits_ptr) & 1];
-  const float px = p_xyz[3 * p], py = p_xyz[3 * p + 1], pz = p_xyz[3 * p + 2];
-  float gx = 0.f, gy = 0.f, gz = 0.f;
-  for (uint32_t t = first[p]; t < last[p]; ++t) {
-    const uint32_t e = vals[t];
-    const int64_t i = e / static_cast<uint32_t>(k);
+    k_bwd_scatter(int64_t total, int64_t n, const int32_t* __restrict__ idx,
+                  const float* __restrict__ dist, const float* __restrict__ grad,
+                  uint32_t* __restrict__ cursor, uint64_t* __restrict__ pairs) {
+  for (int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; e < total;
+       e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int32_t t = idx[e];
+    if (!entry_valid(t, n, dist[e])) continue;
+    const uint32_t slot = atomicSub(&cursor[t], 1u) - 1u;
     const float g2 = -2.f * grad[e];
-    gx = __fmaf_rn(g2, __fsub_rn(q_xyz[3 * i], px), gx);
-    gy = __fmaf_rn(g2, __fsub_rn(q_xyz[3 * i + 1], py), gy);
-    gz = __fmaf_rn(g2, __fsub_rn(q_xyz[3 * i + 2], pz), gz);
+    pairs[slot] = (static_cast<uint64_t>(e) << 32) | __float_as_uint(g2);
   }
-  if (accumulate) {
-    gx = __fadd_rn(grad_p[3 * p], gx);
-    gy = __fadd_rn(grad_p[3 * p + 1], gy);
-    gz = __fadd_rn(grad_p[3 * p + 2], gz);
-  }
-  grad_p[3 * p] = gx;
-  grad_p[3 * p + 1] = gy;
-  grad_p[3 * p + 2] = gz;
 }
 
-__global__ void k_bwd_bits(Meta* meta, int bits) { meta->key_bits = bits; }
+namespace {
+
+struct Acc {
+  float x = 0.f, y = 0.f, z = 0.f;
+};
+
+// One term of the reference-side sum, in the order the caller fixes.
+__device__ __forceinline__ void add_pair(Acc& a, uint64_t pr, const float* __restrict__ q_xyz,
+                                         int k, float px, float py, float pz) {
+  const int64_t i = static_cast<int64_t>(pr >> 32) / k;
+  const float g2 = __uint_as_float(static_cast<uint32_t>(pr));
+  a.x = __fmaf_rn(g2, __fsub_rn(q_xyz[3 * i], px), a.x);
+  a.y = __fmaf_rn(g2, __fsub_rn(q_xyz[3 * i + 1], py), a.y);
+  a.z = __fmaf_rn(g2, __fsub_rn(q_xyz[3 * i + 2], pz), a.z);
+}
+
+// Sorts a segment of at most CAP pairs in registers and sums it.
+template <int CAP>
+__device__ __forceinline__ void sum_short(Acc& a, const uint64_t* __restrict__ seg, uint32_t len,
+                                          const float* __restrict__ q_xyz, int k, float px,
+                                          float py, float pz) {
+  uint64_t L[CAP];
+#pragma unroll
+  for (int c = 0; c < CAP; ++c) L[c] = c < static_cast<int>(len) ? seg[c] : kNoPair;
+  sort_network<CAP, 0, CAP>(L);
+#pragma unroll
+  for (int c = 0; c < CAP; ++c)
+    if (c < static_cast<int>(len)) add_pair(a, L[c], q_xyz, k, px, py, pz);
+}
+
+__device__ __forceinline__ uint64_t warp_min_u64(uint64_t v) {
+#pragma unroll
+  for (int s = 16; s > 0; s >>= 1) {
+    const uint64_t o = (static_cast<uint64_t>(__shfl_xor_sync(kFull, static_cast<uint32_t>(v >> 32), s))
+                        << 32) |
+                       __shfl_xor_sync(kFull, static_cast<uint32_t>(v), s);
+    v = o < v ? o : v;
+  }
+  return v;
+}
+
+}  // namespace
+
+// One thread per support point: its segment in ascending e, summed in that
+// order.  Segments of more than 32 entries (hub points: many queries share
+// them as a neighbour) are taken by the whole warp, one at a time: every
+// round the warp selects the smallest remaining e (entries are distinct),
+// so the order and the arithmetic are those of the short path.
+__global__ void __launch_bounds__(128)
+    k_bwd_support(const float* __restrict__ q_xyz, const float* __restrict__ p_xyz, int64_t n,
+                  int k, const uint32_t* __restrict__ start, const uint64_t* __restrict__ pairs,
+                  float* __restrict__ grad_p, int accumulate) {
+  const int64_t p0 = static_cast<int64_t>(blockIdx.x) * blockDim.x;
+  if (p0 >= n) return;  // whole warps leave together: n is the same for all
+  const int64_t p = p0 + threadIdx.x;
+  const int lane = threadIdx.x & 31;
+  const bool live = p < n;
+  uint32_t s = 0, len = 0;
+  float px = 0.f, py = 0.f, pz = 0.f;
+  if (live) {
+    s = start[p];
+    len = start[p + 1] - s;
+    px = p_xyz[3 * p];
+    py = p_xyz[3 * p + 1];
+    pz = p_xyz[3 * p + 2];
+  }
+  Acc a;
+  const bool long_seg = len > 32;
+  if (__any_sync(kFull, !long_seg && len > 16)) {
+    if (!long_seg) sum_short<32>(a, pairs + s, len, q_xyz, k, px, py, pz);
+  } else if (!long_seg && len > 0) {
+    sum_short<16>(a, pairs + s, len, q_xyz, k, px, py, pz);
+  }
+  uint32_t todo = __ballot_sync(kFull, long_seg);
+  while (todo) {
+    const int leader = __ffs(todo) - 1;
+    todo &= todo - 1;
+    const uint32_t ls = __shfl_sync(kFull, s, leader);
+    const uint32_t ll = __shfl_sync(kFull, len, leader);
+    const float lx = __shfl_sync(kFull, px, leader);
+    const float ly = __shfl_sync(kFull, py, leader);
+    const float lz = __shfl_sync(kFull, pz, leader);
+    Acc b;
+    uint64_t last = 0;
+    for (uint32_t r = 0; r < ll; ++r) {
+      uint64_t best = kNoPair;
+      for (uint32_t t = lane; t < ll; t += 32) {
+        const uint64_t v = pairs[ls + t];
+        if ((r == 0 || v > last) && v < best) best = v;
+      }
+      best = warp_min_u64(best);
+      add_pair(b, best, q_xyz, k, lx, ly, lz);
+      last = best;
+    }
+    if (lane == leader) a = b;
+  }
+  if (!live) return;
+  if (accumulate) {
+    a.x = __fadd_rn(grad_p[3 * p], a.x);
+    a.y = __fadd_rn(grad_p[3 * p + 1], a.y);
+    a.z = __fadd_rn(grad_p[3 * p + 2], a.z);
+  }
+  grad_p[3 * p] = a.x;
+  grad_p[3 * p + 1] = a.y;
+  grad_p[3 * p + 2] = a.z;
+}
 
 namespace {
 
@@ -104,35 +224,24 @@ inline int blocks_for(int64_t n, int per_block) {
 }
 
 struct BwdBufs {
-  Meta* meta;
-  uint32_t* keys[2];
-  uint32_t* vals[2];
-  uint32_t* hist;
-  uint32_t* totals;
-  uint32_t* first;
-  uint32_t* last;
+  uint32_t* count;    // [n]
+  uint32_t* start;    // [n + 1]
+  uint32_t* cursor;   // [n]
+  uint32_t* tiles;    // [n_tiles]
+  uint64_t* pairs;    // [m * k]
+  int* total;         // valid entries (written by the tile scan)
 };
 
 BwdBufs bwd_layout(void* ws, int64_t m, int64_t n, int k, size_t* bytes) {
   Arena a(ws);
   BwdBufs b{};
-  const int64_t total = m * k;
-  b.meta = a.take<Meta>(1);
-  b.keys[0] = a.take<uint32_t>(total);
-  b.keys[1] = a.take<uint32_t>(total);
-  b.vals[0] = a.take<uint32_t>(total);
-  b.vals[1] = a.take<uint32_t>(total);
-  b.hist = a.take<uint32_t>(sort_hist_elems(total));
-  b.totals = a.take<uint32_t>(kSortMaxPasses * 256);
-  b.first = a.take<uint32_t>(n);
-  b.last = a.take<uint32_t>(n);
+  b.total = a.take<int>(1);
+  b.count = a.take<uint32_t>(n);
+  b.start = a.take<uint32_t>(n + 1);
+  b.cursor = a.take<uint32_t>(n);
+  b.tiles = a.take<uint32_t>(ceil_div(n > 0 ? n : 1, kScanTile));
+  b.pairs = a.take<uint64_t>(m * k);
   if (bytes) *bytes = a.used + 256;
-  return b;
-}
-
-int bits_for(int64_t count) {
-  int b = 0;
-  while ((1ll << b) < count) ++b;
   return b;
 }
 
@@ -151,39 +260,33 @@ int run_backward(const BackwardArgs& a, void* ws, size_t ws_bytes, cudaStream_t 
   if (ws_bytes < need) return FKNN_ERR_WORKSPACE;
   const int64_t total = a.m * a.k;
   const bool want_p = a.grad_p != nullptr && a.n > 0;
-  cudaError_t e = cudaMemsetAsync(b.meta, 0, sizeof(Meta), s);
-  if (e == cudaSuccess && want_p) {
-    e = cudaMemsetAsync(b.totals, 0, kSortMaxPasses * 256 * sizeof(uint32_t), s);
-    if (e == cudaSuccess) e = cudaMemsetAsync(b.first, 0, sizeof(uint32_t) * a.n, s);
-    if (e == cudaSuccess) e = cudaMemsetAsync(b.last, 0, sizeof(uint32_t) * a.n, s);
-  }
+  int nl = 0;
+  cudaError_t e = cudaSuccess;
+  if (want_p) e = cudaMemsetAsync(b.count, 0, sizeof(uint32_t) * a.n, s);
   if (e != cudaSuccess) {
     note_cuda_error(e);
     return FKNN_ERR_CUDA;
   }
-  int nl = 0;
-  if (a.m > 0) {
-    k_bwd_query<<<blocks_for(a.m, 256), 256, 0, s>>>(
-        a.q_xyz, a.m, a.p_xyz, a.n, a.idx, a.dist, a.grad, a.k, a.grad_q, a.accumulate,
-        want_p ? b.keys[0] : nullptr, want_p ? b.vals[0] : nullptr);
+  if (a.m > 0 && (a.grad_q || want_p)) {
+    k_bwd_query<<<blocks_for(a.m, 256), 256, 0, s>>>(a.q_xyz, a.m, a.p_xyz, a.n, a.idx, a.dist,
+                                                     a.grad, a.k, a.grad_q, a.accumulate,
+                                                     want_p ? b.count : nullptr);
     ++nl;
   }
   if (want_p) {
-    const int bits = bits_for(a.n + 1);
+    const int tiles = blocks_for(a.n, kScanTile);
+    k_bwd_tile_sums<<<tiles, kScanTile, 0, s>>>(b.count, a.n, b.tiles);
+    k_scan_tiles<<<1, 1024, 0, s>>>(b.tiles, tiles, b.total);
+    k_bwd_starts<<<tiles, kScanTile, 0, s>>>(b.count, a.n, b.tiles, b.start, b.cursor);
+    nl += 3;
     if (total > 0) {
-      k_bwd_bits<<<1, 1, 0, s>>>(b.meta, bits);
-      SortBuffers<uint32_t> sb{{b.keys[0], b.keys[1]}, {b.vals[0], b.vals[1]}, b.hist, b.totals};
-      nl += 1 + launch_radix_sort(sb, total, &b.meta->key_bits, sort_passes_for_bits(bits), s);
-      const SortPair<uint32_t> sp{{b.keys[0], b.keys[1]}, {b.vals[0], b.vals[1]}};
-      k_bwd_bounds<<<blocks_for(total, 256), 256, 0, s>>>(total, sp, &b.meta->key_bits,
-                                                         static_cast<uint32_t>(a.n), b.first,
-                                                         b.last);
+      const int64_t sb = ceil_div(total, 256);
+      k_bwd_scatter<<<static_cast<int>(sb < 8192 ? sb : 8192), 256, 0, s>>>(
+          total, a.n, a.idx, a.dist, a.grad, b.cursor, b.pairs);
       ++nl;
     }
-    const SortPair<uint32_t> sp{{b.keys[0], b.keys[1]}, {b.vals[0], b.vals[1]}};
-    k_bwd_support<<<blocks_for(a.n, 256), 256, 0, s>>>(a.q_xyz, a.p_xyz, a.n, a.grad, a.k, sp,
-                                                       &b.meta->key_bits, b.first, b.last,
-                                                       a.grad_p, a.accumulate);
+    k_bwd_support<<<blocks_for(a.n, 128), 128, 0, s>>>(a.q_xyz, a.p_xyz, a.n, a.k, b.start,
+                                                       b.pairs, a.grad_p, a.accumulate);
     ++nl;
   }
   e = cudaGetLastError();

@@ -179,8 +179,9 @@ FKNN_API int fknn_build_tables(const int64_t* grid_coord, const int64_t* batch_i
  * FlashKnnWrapper.py:165).  For d_ij = |p[idx_ij] - q_i|^2:
  *   grad_q[i] (+)= sum_j 2 g_ij (q_i - p[idx_ij])
  *   grad_p[n] (+)= sum_{idx_ij = n} -2 g_ij (q_i - p_n)
- * summed in a fixed order (grad_p through a stable sort of the neighbour
- * index and a segmented reduction), so results are bitwise reproducible.
+ * summed in a fixed order (grad_p: a counting sort of the entries by
+ * neighbour index, each segment summed in ascending entry order i*K+j), so
+ * results are bitwise reproducible.  Requires m*k < 2^31.
  * Entries with dist == +inf or idx < 0 (padding) carry no gradient.
  * accumulate != 0 adds into grad_q / grad_p instead of overwriting them
  * (grad_q may alias grad_p for a self query only with accumulate != 0). */

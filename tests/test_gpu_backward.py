@@ -219,3 +219,33 @@ def test_backward_ignores_padding_entries(fk):
     # the pair (1, 2): d = |x1 - x2|^2 counted twice (1->2 and 2->1)
     want = 4 * (xyz[1] - xyz[2]).astype(np.float64)
     assert np.allclose(g[1], want, rtol=1e-5) and np.allclose(g[2], -want, rtol=1e-5)
+
+
+def test_hub_points_with_long_segments(fk):
+    """Exact duplicates make the lowest-index copies the neighbours of every
+    copy (ties break by lower index), so a few support points collect
+    hundreds of entries: the warp-cooperative path of the segmented sum."""
+    rng = np.random.default_rng(12)
+    base = rng.random((2000, 3), dtype=np.float32)
+    hub = np.repeat(base[:3], 150, axis=0)          # three clusters of 150 copies
+    xyz = np.concatenate([base[3:], hub])
+    rng.shuffle(xyz)
+    n, k = len(xyz), 16
+    x = torch.from_numpy(xyz).to(DEV)
+    offs = torch.tensor([n], device=DEV)
+    idx, dist = fk.ops.knn_offsets(x, offs, k, 0.03, 2)
+    counts = np.bincount(idx.cpu().numpy().ravel(), minlength=n)
+    assert counts.max() > 100
+    g = torch.from_numpy(np.random.default_rng(3).standard_normal((n, k)).astype(np.float32))
+    g = _masked(g.to(DEV), dist)
+    outs = []
+    for _ in range(2):
+        gq = torch.empty_like(x)
+        gp = torch.empty_like(x)
+        fk.ops.backward(x, x, idx, dist, g, grad_q=gq, grad_p=gp)
+        outs.append((gq.cpu().numpy(), gp.cpu().numpy()))
+    assert np.array_equal(outs[0][1].view(np.uint32), outs[1][1].view(np.uint32))
+    wq, wp = O.backward_f64(xyz, xyz, idx.cpu().numpy(), dist.cpu().numpy(),
+                            g.cpu().numpy().astype(np.float64))
+    assert _rel_max(outs[0][0], wq) <= 1e-5
+    assert _rel_max(outs[0][1], wp) <= 1e-5
