@@ -482,3 +482,172 @@ void orc_backward_f64(const float* qxyz, int64_t m, const float* pxyz,
       }
     }
 }
+
+/* ------------------------------------------------- adaptive neighbourhood */
+
+/* Morton interleave of non-negative coordinates below 2^21. */
+static uint64_t morton21(uint64_t x, uint64_t y, uint64_t z) {
+  uint64_t key = 0;
+  for (int bit = 0; bit < 21; ++bit) {
+    key |= ((x >> bit) & 1u) << (3 * bit + 2);
+    key |= ((y >> bit) & 1u) << (3 * bit + 1);
+    key |= ((z >> bit) & 1u) << (3 * bit);
+  }
+  return key;
+}
+
+/*
+ * Adaptive-neighbourhood self query
+ * (FlashKNN/functions/adaptive_octree.py:211-351 and :531-575):
+ *   - grid coordinates are translated per batch to their minimum
+ *     (:129-147); every translated coordinate must be below 2^16;
+ *   - the octree levels s = 0..S group the points by (batch, spatial key
+ *     >> 3s) (:256-274), S = max_shift, or the bit length of the largest
+ *     translated coordinate when max_shift < 0 (:249-252);
+ *   - a node's candidate count is the number of points in the 27 nodes of
+ *     its level at integer offsets (0,-1,+1)^3 (:150-205, :287-302); offsets
+ *     that leave [0, 2^(16-s)) name no node;
+ *   - level selection (:312-351): start at S, active = count > max_f*K; for
+ *     s = S-1..0 a still-active point moves to level s when its level-s
+ *     count is >= min_f*K, and stays active while that count is > max_f*K;
+ *   - the query is the exact top-K over the points of the 27 nodes around
+ *     the point's node at its selected level (the compatible-table kernel
+ *     launch, :369-488 and :555-575), FP32 distances, d < cut_r2, padding
+ *     (own index, +inf), ties by the lower original index.
+ * Positions are xyz, or the translated grid coordinates when xyz is NULL
+ * (:545-549).  Outputs in input order: level_out[n] (may be NULL),
+ * idx_out[n*k], dist_out[n*k].
+ * Returns 0; -1 bad K or n < K or n == 0; -2 batch outside [0, 32768);
+ * -3 a batch spans 2^16 or more; -4 max_shift > 16.
+ */
+int orc_adaptive_query(const int64_t* grid, const int64_t* batch, int64_t n,
+                       const float* xyz, int k, int min_f, int max_f,
+                       int max_shift, float cut_r2, int variant,
+                       int32_t* level_out, int64_t* idx_out, float* dist_out,
+                       int nthreads) {
+  if (k < 1 || k > ORC_MAXK || n <= 0 || n < k) return -1;
+  enum { NB = 32768 };
+  int64_t* bmin = (int64_t*)malloc(sizeof(int64_t) * 3 * NB);
+  for (int64_t i = 0; i < 3 * NB; ++i) bmin[i] = INT64_MAX;
+  for (int64_t i = 0; i < n; ++i) {
+    if (batch[i] < 0 || batch[i] >= NB) { free(bmin); return -2; }
+    for (int a = 0; a < 3; ++a)
+      if (grid[3 * i + a] < bmin[3 * batch[i] + a]) bmin[3 * batch[i] + a] = grid[3 * i + a];
+  }
+  int64_t* norm = (int64_t*)malloc(sizeof(int64_t) * 3 * (size_t)n);
+  int64_t maxc = 0;
+  for (int64_t i = 0; i < n; ++i)
+    for (int a = 0; a < 3; ++a) {
+      int64_t v = grid[3 * i + a] - bmin[3 * batch[i] + a];
+      if (v >= 65536) { free(norm); free(bmin); return -3; }
+      norm[3 * i + a] = v;
+      if (v > maxc) maxc = v;
+    }
+  free(bmin);
+  int auto_s = 0;
+  while ((1ll << auto_s) <= maxc) ++auto_s;  /* bit length of maxc */
+  int S = max_shift >= 0 ? max_shift : auto_s;
+  if (S > 16) { free(norm); return -4; }
+  int L = S + 1;
+
+  int64_t* key = (int64_t*)malloc(sizeof(int64_t) * (size_t)n);
+  for (int64_t i = 0; i < n; ++i)
+    key[i] = (int64_t)(((uint64_t)batch[i] << 48) |
+                       morton21((uint64_t)norm[3 * i], (uint64_t)norm[3 * i + 1],
+                                (uint64_t)norm[3 * i + 2]));
+  int64_t* order = (int64_t*)malloc(sizeof(int64_t) * (size_t)n);
+  orc_argsort_i64(key, n, order);
+
+  /* per level: node of every sorted position, node keys / starts, counts */
+  int64_t* node_of = (int64_t*)malloc(sizeof(int64_t) * (size_t)n * L);
+  int64_t** nkey = (int64_t**)malloc(sizeof(int64_t*) * L);
+  int64_t** nstart = (int64_t**)malloc(sizeof(int64_t*) * L);
+  int64_t** ncand = (int64_t**)malloc(sizeof(int64_t*) * L);
+  int64_t* ncount = (int64_t*)malloc(sizeof(int64_t) * L);
+  const uint64_t spatial_mask = (1ull << 48) - 1;
+  for (int s = 0; s < L; ++s) {
+    nkey[s] = (int64_t*)malloc(sizeof(int64_t) * (size_t)n);
+    nstart[s] = (int64_t*)malloc(sizeof(int64_t) * (size_t)(n + 1));
+    int64_t p = 0;
+    for (int64_t q = 0; q < n; ++q) {
+      uint64_t kk = (uint64_t)key[order[q]];
+      int64_t nk = (int64_t)(((kk >> 48) << 48) | ((kk & spatial_mask) >> (3 * s)));
+      if (q == 0 || nk != nkey[s][p - 1]) { nkey[s][p] = nk; nstart[s][p] = q; ++p; }
+      node_of[(size_t)s * n + q] = p - 1;
+    }
+    nstart[s][p] = n;
+    ncount[s] = p;
+    ncand[s] = (int64_t*)malloc(sizeof(int64_t) * (size_t)(p ? p : 1));
+    const int64_t lim = 1ll << (16 - s);
+    for (int64_t c = 0; c < p; ++c) {
+      int64_t f = order[nstart[s][c]];
+      int64_t cx = norm[3 * f] >> s, cy = norm[3 * f + 1] >> s, cz = norm[3 * f + 2] >> s;
+      int64_t b = batch[f], total = 0;
+      for (int j = 0; j < 27; ++j) {
+        int64_t x = cx + axis_offset(j / 9), y = cy + axis_offset((j / 3) % 3),
+                z = cz + axis_offset(j % 3);
+        if (x < 0 || y < 0 || z < 0 || x >= lim || y >= lim || z >= lim) continue;
+        int64_t nk = (int64_t)(((uint64_t)b << 48) | morton21((uint64_t)x, (uint64_t)y, (uint64_t)z));
+        int64_t hit = search_sorted(nkey[s], p, nk);
+        if (hit >= 0) total += nstart[s][hit + 1] - nstart[s][hit];
+      }
+      ncand[s][c] = total;
+    }
+  }
+
+  /* level selection, sorted order */
+  int* sel = (int*)malloc(sizeof(int) * (size_t)n);
+  for (int64_t q = 0; q < n; ++q) {
+    int level = S;
+    int active = ncand[S][node_of[(size_t)S * n + q]] > (int64_t)max_f * k;
+    for (int s = S - 1; s >= 0; --s) {
+      int64_t child = ncand[s][node_of[(size_t)s * n + q]];
+      int use = active && child >= (int64_t)min_f * k;
+      if (use) level = s;
+      active = use && child > (int64_t)max_f * k;
+    }
+    sel[q] = level;
+  }
+
+#ifdef _OPENMP
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+#pragma omp parallel for schedule(dynamic, 64)
+#endif
+  for (int64_t q = 0; q < n; ++q) {
+    float dl[ORC_MAXK];
+    int64_t il[ORC_MAXK];
+    for (int j = 0; j < k; ++j) { dl[j] = INFINITY; il[j] = INT64_MAX; }
+    const int64_t i = order[q];
+    const int s = sel[q];
+    const int64_t lim = 1ll << (16 - s);
+    float qp[3], cp[3];
+    for (int a = 0; a < 3; ++a) qp[a] = xyz ? xyz[3 * i + a] : (float)norm[3 * i + a];
+    int64_t cx = norm[3 * i] >> s, cy = norm[3 * i + 1] >> s, cz = norm[3 * i + 2] >> s;
+    for (int j = 0; j < 27; ++j) {
+      int64_t x = cx + axis_offset(j / 9), y = cy + axis_offset((j / 3) % 3),
+              z = cz + axis_offset(j % 3);
+      if (x < 0 || y < 0 || z < 0 || x >= lim || y >= lim || z >= lim) continue;
+      int64_t nk = (int64_t)(((uint64_t)batch[i] << 48) | morton21((uint64_t)x, (uint64_t)y, (uint64_t)z));
+      int64_t hit = search_sorted(nkey[s], ncount[s], nk);
+      if (hit < 0) continue;
+      for (int64_t r = nstart[s][hit]; r < nstart[s][hit + 1]; ++r) {
+        int64_t t = order[r];
+        for (int a = 0; a < 3; ++a) cp[a] = xyz ? xyz[3 * t + a] : (float)norm[3 * t + a];
+        float d = sqdist(cp, qp, variant);
+        if (!(d < cut_r2)) continue;
+        topk_insert(d, t, dl, il, k);
+      }
+    }
+    for (int j = 0; j < k; ++j) {
+      idx_out[i * k + j] = il[j] == INT64_MAX ? i : il[j];
+      dist_out[i * k + j] = dl[j];
+    }
+    if (level_out) level_out[i] = s;
+  }
+
+  free(sel);
+  for (int s = 0; s < L; ++s) { free(nkey[s]); free(nstart[s]); free(ncand[s]); }
+  free(ncount); free(ncand); free(nstart); free(nkey); free(node_of);
+  free(order); free(key); free(norm);
+  return 0;
+}

@@ -67,6 +67,8 @@ def _declare(L):
     L.orc_brute_knn_f64.argtypes = [P, P, I64, P, P, I32, P, P, I32]
     L.orc_backward_f64.restype = None
     L.orc_backward_f64.argtypes = [P, I64, P, I64, P, P, P, I32, P, P]
+    L.orc_adaptive_query.restype = I32
+    L.orc_adaptive_query.argtypes = [P, P, I64, P, I32, I32, I32, I32, F32, I32, P, P, P, I32]
 
 
 def _ptr(a):
@@ -254,3 +256,22 @@ def set_recall(pred, exact):
     for r in range(exact.shape[0]):
         hits[r] = np.isin(exact[r], pred[r]).sum() / k
     return hits
+
+
+def adaptive_query(grid, batch, k, xyz=None, min_factor=2, max_factor=8, max_shift=-1,
+                   cut_r2=np.inf, variant=DEFAULT_VARIANT, nthreads=0):
+    """Adaptive-neighbourhood self query (AdaptiveNeighborhoodFlashKNN):
+    (levels int32 [n], idx int64 [n,K], dist f32 [n,K]) in input order."""
+    grid = _c(grid, np.int64)
+    batch = _c(batch, np.int64)
+    xyz = _c(xyz, np.float32)
+    n = grid.shape[0]
+    levels = np.empty(n, np.int32)
+    idx = np.empty((n, k), np.int64)
+    dist = np.empty((n, k), np.float32)
+    rc = lib().orc_adaptive_query(_ptr(grid), _ptr(batch), n, _ptr(xyz), k, min_factor,
+                                  max_factor, max_shift, float(cut_r2), variant, _ptr(levels),
+                                  _ptr(idx), _ptr(dist), nthreads)
+    if rc != 0:
+        raise ValueError(f"orc_adaptive_query failed with {rc}")
+    return levels, idx, dist

@@ -194,3 +194,42 @@ def test_reference_nanoflann_baseline_is_exact_knn():
     start = np.repeat([0, 1200], [1200, 1800])[:, None]
     hit = (idx.astype(np.int64) + start == bi)
     assert hit.mean() > 0.999  # equal-distance order aside
+
+
+def adaptive_cases():
+    return sorted(f[len("adaptive_"):-4] for f in os.listdir(GOLDEN)
+                  if f.startswith("adaptive_") and f.endswith(".npz"))
+
+
+def adaptive_args(z):
+    cut = float(z["cut_radius"])
+    r2 = np.float32(cut) * np.float32(cut) if np.isfinite(cut) else np.inf
+    xyz = None if bool(z["grid_positions"]) else z["xyz"]
+    return dict(k=int(z["k"]), xyz=xyz, min_factor=int(z["min_factor"]),
+                max_factor=int(z["max_factor"]), max_shift=int(z["max_shift"]), cut_r2=r2)
+
+
+def same_up_to_kth_ties(idx_a, dist_a, idx_b, dist_b):
+    """Identical distance rows; indices identical for every distance below
+    the row's K-th (equal distances at the K-th may be kept in any order)."""
+    if not np.array_equal(dist_a.view(np.uint32), dist_b.view(np.uint32)):
+        return False
+    for r in np.nonzero((idx_a != idx_b).any(1))[0]:
+        kth = dist_a[r, -1]
+        for d in np.unique(dist_a[r]):
+            if d != kth and set(idx_a[r][dist_a[r] == d]) != set(idx_b[r][dist_b[r] == d]):
+                return False
+    return True
+
+
+@pytest.mark.parametrize("case", adaptive_cases())
+def test_oracle_adaptive_matches_reference_pipeline(case):
+    """The adaptive octree restatement against the reference's own
+    AdaptiveNeighborhoodFlashKNN run (tests/golden/make_golden_adaptive.py):
+    the same level for every point, bit-identical distances, the same
+    neighbours (ties at the K-th distance aside: the reference orders them by
+    Morton position, the restatement by input index)."""
+    z = np.load(os.path.join(GOLDEN, f"adaptive_{case}.npz"))
+    levels, idx, dist = O.adaptive_query(z["grid"], z["batch"], **adaptive_args(z))
+    assert np.array_equal(levels, z["ref_levels"])
+    assert same_up_to_kth_ties(idx, dist, z["ref_idx"], z["ref_dist"])
