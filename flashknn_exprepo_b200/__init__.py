@@ -4,8 +4,9 @@ Public entry points (mirroring the reference's ``FlashKNN/functions``):
   FlashKNN              -- query / selected_query drop-in (wrapper.py)
   knn_query, KNNQuery   -- Pointcept-style offset batching with a
                            differentiable squared distance (pointops.py)
+  AdaptiveNeighborhoodFlashKNN
+                        -- per-point octree level (adaptive.py)
   xyz2key               -- Morton keys (z_order.py)
-  BatchedKNNPlan        -- CUDA-graph captured batched query (plan.py)
   ops                   -- tensor-level C-ABI calls, incl. the reference
                            table ABI (query_tables, build_tables, ...)
 The CUDA library is libfknn.so next to this file (``python -m
@@ -13,8 +14,10 @@ flashknn_exprepo_b200.build``); nothing falls back to the CPU.
 """
 from . import ops
 from ._lib import FknnError
+from .adaptive import AdaptiveNeighborhoodFlashKNN
 from .pointops import KNNQuery, knn_query
 from .wrapper import FlashKNN
 from .z_order import xyz2key
 
-__all__ = ["FlashKNN", "KNNQuery", "knn_query", "xyz2key", "ops", "FknnError"]
+__all__ = ["FlashKNN", "AdaptiveNeighborhoodFlashKNN", "KNNQuery", "knn_query", "xyz2key",
+           "ops", "FknnError"]

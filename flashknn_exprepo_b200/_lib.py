@@ -86,6 +86,9 @@ _SIGNATURES = {
     "fknn_backward_workspace_bytes": (_SZ, [_I64, _I64, _I32]),
     "fknn_backward": (ctypes.c_int, [_P, _I64, _P, _I64, _P, _P, _P, _I32, _P, _P, _I32, _P, _SZ,
                                      _P]),
+    "fknn_adaptive_workspace_bytes": (_SZ, [_I64]),
+    "fknn_adaptive_query": (ctypes.c_int, [_P, _P, _I64, _P, _I32, _I32, _I32, _I32, _F32, _I32,
+                                           _P, _P, _P, _P, _SZ, _P, _P]),
 }
 
 EXPORTED = tuple(_SIGNATURES)

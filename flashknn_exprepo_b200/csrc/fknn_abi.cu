@@ -8,6 +8,7 @@
 
 #include "../../include/fknn.h"
 #include "fknn_backward.h"
+#include "fknn_adaptive.h"
 #include "fknn_grid.h"
 #include "fknn_internal.h"
 #include "fknn_tables.h"
@@ -341,6 +342,39 @@ int fknn_build_tables(const int64_t* grid_coord, const int64_t* batch_idx, int64
   fknn::BuildTablesArgs t{grid_coord, batch_idx, n, num_down, order, steps, neigh, cnt, n_parents};
   int launches = 0;
   const int rc = fknn::run_build_tables(t, workspace, workspace_bytes, as_stream(stream), &launches);
+  return finish(rc, launches);
+}
+
+size_t fknn_adaptive_workspace_bytes(int64_t n) {
+  if (n < 0) return 0;
+  return fknn::adaptive_workspace_bytes(n);
+}
+
+int fknn_adaptive_query(const int64_t* grid_coord, const int64_t* batch_idx, int64_t n,
+                        const float* xyz, int32_t k, int32_t min_candidates_factor,
+                        int32_t max_candidates_factor, int32_t max_shift, float cut_r2,
+                        int32_t idx_bits, void* idx_out, float* dist_out, int8_t* level_out,
+                        void* workspace, size_t workspace_bytes, const fknn_config* config,
+                        void* stream) {
+  int rc = check_k(k);
+  if (rc) return rc;
+  if (n < 0) return FKNN_ERR_ARG;
+  if (n > kMaxPoints) return FKNN_ERR_SIZE;
+  if (n > 0 && n < k) return FKNN_ERR_ARG;
+  if (min_candidates_factor < 1 || max_candidates_factor < min_candidates_factor ||
+      static_cast<int64_t>(max_candidates_factor) * k > (1ll << 30))
+    return FKNN_ERR_ARG;
+  if (max_shift > 16) return FKNN_ERR_ARG;
+  if (idx_bits != 32 && idx_bits != 64) return FKNN_ERR_ARG;
+  if (!workspace || (n > 0 && (!grid_coord || !idx_out || !dist_out))) return FKNN_ERR_ARG;
+  if (!aligned(workspace, 256)) return FKNN_ERR_ARG;
+  QueryShape shape;
+  if ((rc = shape_from(config, &shape))) return rc;
+  const fknn::AdaptiveArgs a{grid_coord, batch_idx, xyz, n, k, min_candidates_factor,
+                             max_candidates_factor, max_shift < 0 ? -1 : max_shift, cut_r2,
+                             idx_bits, idx_out, dist_out, level_out};
+  int launches = 0;
+  rc = fknn::run_adaptive(a, workspace, workspace_bytes, shape, as_stream(stream), &launches);
   return finish(rc, launches);
 }
 

@@ -111,6 +111,42 @@ def knn_grid(xyz, grid_coord, batch_idx, k, num_down=2, cut_r2=math.inf, query_i
     return idx, dist
 
 
+def adaptive_query(grid_coord, batch_idx, k, xyz=None, min_factor=2, max_factor=8,
+                   max_shift=None, cut_r2=math.inf, idx_dtype=torch.int64, config=None,
+                   want_levels=False, validate=False):
+    """AdaptiveNeighborhoodFlashKNN.query: per-point octree level, exact top-K
+    over the 27 same-level nodes.  Returns (idx [n,k] of ``idx_dtype`` in
+    input numbering, dist2 f32 [n,k], levels int8 [n] or None)."""
+    lib = _lib.load()
+    grid_coord = _require(grid_coord, "grid_coord", torch.int64, 2, 3)
+    dev = grid_coord.device
+    n = grid_coord.shape[0]
+    if batch_idx is not None:
+        batch_idx = _require(batch_idx, "batch_idx", torch.int64, 1)
+        if batch_idx.numel() != n:
+            raise ValueError("batch_idx must have one entry per point")
+    if xyz is not None:
+        xyz = _require(xyz, "xyz", torch.float32, 2, 3)
+        if xyz.shape[0] != n:
+            raise ValueError("xyz and grid_coord must have the same number of points")
+    if idx_dtype not in (torch.int32, torch.int64):
+        raise ValueError("idx_dtype must be torch.int32 or torch.int64")
+    idx = torch.empty((n, k), dtype=idx_dtype, device=dev)
+    dist = torch.empty((n, k), dtype=torch.float32, device=dev)
+    levels = torch.empty(n, dtype=torch.int8, device=dev) if want_levels else None
+    ws = _lib.WORKSPACE.get(lib.fknn_adaptive_workspace_bytes(n), dev)
+    _, cfg = _config_ptr(config)
+    rc = lib.fknn_adaptive_query(ptr(grid_coord), ptr(batch_idx), n, ptr(xyz), k, int(min_factor),
+                                 int(max_factor), -1 if max_shift is None else int(max_shift),
+                                 float(cut_r2), 64 if idx_dtype == torch.int64 else 32, ptr(idx),
+                                 ptr(dist), ptr(levels), ptr(ws), ws.numel(), cfg,
+                                 stream_handle(dev))
+    check(rc, "fknn_adaptive_query")
+    if validate:
+        _lib.raise_on_status(ws, "adaptive_query")
+    return idx, dist, levels
+
+
 def query_tables(xyz_sorted, steps, neigh, cnt, k, cut_r2=math.inf, config=None,
                  validate=False):
     """Reference table ABI (FlashKNN_Query_Dynamic_Load): sorted-space (idx, dist)."""

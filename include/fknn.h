@@ -116,6 +116,28 @@ FKNN_API int fknn_knn_grid(const float* xyz, const int64_t* grid_coord, const in
                   float* dist_out, void* workspace, size_t workspace_bytes,
                   const fknn_config* config, void* stream);
 
+/* AdaptiveNeighborhoodFlashKNN.query (FlashKNN/functions/adaptive_octree.py
+ * :505-612): every point takes its exact top-K over the 27 same-level nodes
+ * of the octree level picked by coarse-to-fine candidate counting (descend
+ * while the count exceeds max_candidates_factor*K, provided the finer count
+ * is at least min_candidates_factor*K).  grid_coord int64 [n,3], batch_idx
+ * int64 [n] in [0, 32768) (NULL = one batch), xyz f32 [n,3] or NULL (then
+ * the positions are the grid coordinates translated to each batch's
+ * minimum, as in the reference).  max_shift < 0 builds levels up to the bit
+ * length of the largest translated coordinate; otherwise 0..max_shift (<=
+ * 16).  Requires n >= k.  idx_out [n,k] (idx_bits 64: int64, 32: int32) in
+ * input index space, dist_out f32 [n,k], padding (own index, +inf);
+ * level_out int8 [n] (NULL = not wanted) receives the selected level.
+ * Device status: FKNN_DEVICE_BATCH_RANGE for a batch id outside the range,
+ * FKNN_DEVICE_COORD_RANGE for a batch spanning 2^16 grid cells or more. */
+FKNN_API size_t fknn_adaptive_workspace_bytes(int64_t n);
+FKNN_API int fknn_adaptive_query(const int64_t* grid_coord, const int64_t* batch_idx, int64_t n,
+                        const float* xyz, int32_t k, int32_t min_candidates_factor,
+                        int32_t max_candidates_factor, int32_t max_shift, float cut_r2,
+                        int32_t idx_bits, void* idx_out, float* dist_out, int8_t* level_out,
+                        void* workspace, size_t workspace_bytes, const fknn_config* config,
+                        void* stream);
+
 /* ------------------------------------------ reference table ABI (a8, a10)
  * Replaces FlashKNN_Query_Dynamic_Load (FlashKNN/csrc/flash_knn_query.h:144-154):
  * xyz_sorted f32 [n,3], steps int32 [p+1], neigh int32 [p,27] (-1 = empty),
