@@ -27,6 +27,7 @@ DEVICE_COORD_RANGE = 1
 DEVICE_BAD_TABLE = 2
 DEVICE_TIMEOUT = 4
 DEVICE_BATCH_RANGE = 8
+DEVICE_NO_CANDIDATES = 16  # informational: general / back queries pad such rows
 
 QUERY_SELF = 0
 QUERY_SELECTED = 1
@@ -37,6 +38,7 @@ _STATUS_TEXT = {
     DEVICE_BAD_TABLE: "a table or index names rows outside the point array",
     DEVICE_TIMEOUT: "a bounded wait on a shared-memory bulk copy gave up",
     DEVICE_BATCH_RANGE: "a batch id lies outside [0, number of clouds)",
+    DEVICE_NO_CANDIDATES: "a query has no candidate in its 27-cell neighbourhood",
 }
 
 
@@ -86,6 +88,9 @@ _SIGNATURES = {
     "fknn_backward_workspace_bytes": (_SZ, [_I64, _I64, _I32]),
     "fknn_backward": (ctypes.c_int, [_P, _I64, _P, _I64, _P, _P, _P, _I32, _P, _P, _I32, _P, _SZ,
                                      _P]),
+    "fknn_back_query_workspace_bytes": (_SZ, [_I64, _I64]),
+    "fknn_back_query": (ctypes.c_int, [_P, _I64, _P, _I64, _P, _F32, _I32, _I32, _P, _P, _P, _SZ,
+                                       _P, _P]),
     "fknn_adaptive_workspace_bytes": (_SZ, [_I64]),
     "fknn_adaptive_query": (ctypes.c_int, [_P, _P, _I64, _P, _I32, _I32, _I32, _I32, _F32, _I32,
                                            _P, _P, _P, _P, _SZ, _P, _P]),
@@ -176,7 +181,9 @@ def read_status(ws: torch.Tensor) -> int:
     return out.value
 
 
-def raise_on_status(ws: torch.Tensor, what: str) -> None:
-    bits = read_status(ws)
+def raise_on_status(ws: torch.Tensor, what: str, ignore: int = DEVICE_NO_CANDIDATES) -> None:
+    """Raise FknnError for device status bits other than `ignore` (queries
+    without candidates are valid for general queries: they are padded)."""
+    bits = read_status(ws) & ~ignore
     if bits:
         raise FknnError(f"{what}: device reported {status_text(bits)} (status {bits})")

@@ -1,6 +1,7 @@
 // extern "C" entry points of libfknn.so (declared in include/fknn.h).
 // Host-side checks only: argument errors return before any launch.
 #include <atomic>
+#include <cmath>
 #include <cstdint>
 #include <mutex>
 #include <vector>
@@ -342,6 +343,49 @@ int fknn_build_tables(const int64_t* grid_coord, const int64_t* batch_idx, int64
   fknn::BuildTablesArgs t{grid_coord, batch_idx, n, num_down, order, steps, neigh, cnt, n_parents};
   int launches = 0;
   const int rc = fknn::run_build_tables(t, workspace, workspace_bytes, as_stream(stream), &launches);
+  return finish(rc, launches);
+}
+
+size_t fknn_back_query_workspace_bytes(int64_t n, int64_t m) {
+  if (n < 0 || m < 0) return 0;
+  return fknn::fused_workspace_bytes(m, n, 32768, FKNN_QUERY_GENERAL);
+}
+
+int fknn_back_query(const float* xyz, int64_t n, const int64_t* sel_indices, int64_t m,
+                    const int64_t* batch_idx, float query_grid_size, int32_t k,
+                    int32_t idx_bits, void* idx_out, float* dist_out, void* workspace,
+                    size_t workspace_bytes, const fknn_config* config, void* stream) {
+  int rc = check_k(k);
+  if (rc) return rc;
+  if (n < 0 || m < 0) return FKNN_ERR_ARG;
+  if (n > kMaxPoints || m > kMaxPoints) return FKNN_ERR_SIZE;
+  if (!(query_grid_size > 0.f) || (idx_bits != 32 && idx_bits != 64)) return FKNN_ERR_ARG;
+  if (!workspace || (n > 0 && (!xyz || !idx_out || !dist_out)) || (m > 0 && !sel_indices))
+    return FKNN_ERR_ARG;
+  if (!aligned(workspace, 256)) return FKNN_ERR_ARG;
+  QueryShape shape;
+  if ((rc = shape_from(config, &shape))) return rc;
+  fknn::FusedArgs f{};
+  f.kind = FKNN_QUERY_GENERAL;
+  f.xyz = xyz;                 // support = the rows sel_indices of xyz
+  f.sindex = sel_indices;
+  f.n = m;
+  f.n_src = n;
+  f.batch = batch_idx;
+  f.n_clouds = batch_idx ? 32768 : 1;
+  f.qxyz = xyz;                // queries = every point
+  f.qbatch = batch_idx;
+  f.m = n;
+  f.voxel = query_grid_size;
+  f.num_down = 0;
+  f.trunc_grid = 1;            // the reference voxelises with (xyz / size).long()
+  f.k = k;
+  f.cut_r2 = INFINITY;
+  f.idx_bits = idx_bits;
+  f.idx_out = idx_out;
+  f.dist_out = dist_out;
+  int launches = 0;
+  rc = fknn::run_fused(f, workspace, workspace_bytes, shape, as_stream(stream), &launches);
   return finish(rc, launches);
 }
 

@@ -17,6 +17,7 @@ constexpr int kStatusRange = FKNN_DEVICE_COORD_RANGE;
 constexpr int kStatusTable = FKNN_DEVICE_BAD_TABLE;
 constexpr int kStatusTimeout = FKNN_DEVICE_TIMEOUT;
 constexpr int kStatusBatch = FKNN_DEVICE_BATCH_RANGE;
+constexpr int kStatusNoCandidates = FKNN_DEVICE_NO_CANDIDATES;
 
 __host__ __device__ inline int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
 

@@ -42,22 +42,42 @@ namespace fknn {
 // ---------------------------------------------------------------- sources
 
 struct PointSrc {
-  const float* xyz;        // f32 [n,3]
-  const int64_t* grid;     // int64 [n,3] or null: floor(xyz / voxel)
-  const int64_t* batch;    // int64 [n] or null
+  const float* xyz;        // f32 [n_src,3]
+  const int64_t* grid;     // int64 [n_src,3] or null: floor(xyz / voxel)
+  const int64_t* batch;    // int64 [n_src] or null
   const int64_t* offsets;  // cumulative cloud ends or null
   int64_t n_clouds;        // clouds addressable by this source
-  int64_t n;
-  float voxel;
+  int64_t n;               // points of this source
+  float inv_voxel;         // FP32 reciprocal of the voxel edge
   int num_down;
+  const int64_t* index;    // point i is row index[i] of xyz / grid / batch, or null
+  int64_t n_src;           // rows of xyz / grid / batch when index is given
+  int trunc;               // voxelise with trunc(xyz / voxel) instead of floor
 };
+
+// Row of point i in the source arrays; an index outside the rows is
+// reported (kStatusTable) and read as row 0.
+__device__ __forceinline__ int64_t row_of(const PointSrc& p, int64_t i, int* status) {
+  if (!p.index) return i;
+  const int64_t r = p.index[i];
+  if (r < 0 || r >= p.n_src) {
+    raise_status(status, kStatusTable);
+    return 0;
+  }
+  return r;
+}
 
 __device__ __forceinline__ int grid_axis(const PointSrc& p, int64_t i, int a, int* status) {
   int64_t g;
+  const int64_t row = row_of(p, i, status);
   if (p.grid) {
-    g = p.grid[3 * i + a];
+    g = p.grid[3 * row + a];
   } else {
-    const float f = floorf(__fdiv_rn(p.xyz[3 * i + a], p.voxel));
+    // x * (1 / voxel): the rounding of PyTorch's CUDA tensor / scalar
+    // division, which the reference's callers voxelise with
+    // (Query/benchmark_s3dis.py:159, Networks/hierarchy.py:30)
+    const float q = __fmul_rn(p.xyz[3 * row + a], p.inv_voxel);
+    const float f = p.trunc ? truncf(q) : floorf(q);
     if (!(f >= -32768.f && f <= 32767.f)) {
       raise_status(status, kStatusRange);
       return 0;
@@ -74,7 +94,7 @@ __device__ __forceinline__ int grid_axis(const PointSrc& p, int64_t i, int a, in
 __device__ __forceinline__ int cloud_of(const PointSrc& p, int64_t i, int* status) {
   int64_t b = 0;
   if (p.batch) {
-    b = p.batch[i];
+    b = p.batch[row_of(p, i, status)];
   } else if (p.offsets) {
     int64_t lo = 0, hi = p.n_clouds;  // first cloud whose end exceeds i
     while (lo < hi) {
@@ -256,9 +276,9 @@ __device__ __forceinline__ bool is_head(const KeyT* keys, int64_t s) {
 // tile_counts[tile] = number of cell heads in the tile.
 template <typename KeyT>
 __global__ void __launch_bounds__(256)
-    k_gather(const float* __restrict__ xyz, int64_t n, SortPair<KeyT> sp, const int* bits_ptr,
-             float4* __restrict__ rec, int32_t* __restrict__ pos_of,
-             uint32_t* __restrict__ tile_counts) {
+    k_gather(const float* __restrict__ xyz, const int64_t* __restrict__ index, int64_t n_src,
+             int64_t n, SortPair<KeyT> sp, const int* bits_ptr, float4* __restrict__ rec,
+             int32_t* __restrict__ pos_of, uint32_t* __restrict__ tile_counts) {
   __shared__ uint32_t warp_sums[32];
   __shared__ uint32_t s_total;
   const int buf = sorted_buffer(*bits_ptr);
@@ -271,8 +291,13 @@ __global__ void __launch_bounds__(256)
     const int64_t s = base + r;
     if (s >= n) break;
     const uint32_t id = vals[s];
-    rec[s] = make_float4(xyz[3 * static_cast<int64_t>(id)], xyz[3 * static_cast<int64_t>(id) + 1],
-                         xyz[3 * static_cast<int64_t>(id) + 2], __int_as_float(static_cast<int>(id)));
+    int64_t row = id;
+    if (index) {
+      row = index[id];
+      if (row < 0 || row >= n_src) row = 0;  // reported by k_bbox
+    }
+    rec[s] = make_float4(xyz[3 * row], xyz[3 * row + 1], xyz[3 * row + 2],
+                         __int_as_float(static_cast<int>(id)));
     if (pos_of) pos_of[id] = static_cast<int32_t>(s);
     heads += is_head(keys, s) ? 1u : 0u;
   }
@@ -598,12 +623,15 @@ int run_fused(const FusedArgs& f, void* ws, size_t ws_bytes, const QueryShape& s
   k_init<<<64, 256, 0, s>>>(b.meta, b.bbox, n_clouds, b.totals, 3 * kSortMaxPasses * 256);
   ++nl;
 
-  PointSrc ps{f.xyz, f.grid, f.batch, f.offsets, n_clouds, n, f.voxel, f.num_down};
+  const float inv_voxel = 1.0f / f.voxel;  // host FP32 division, correctly rounded
+  PointSrc ps{f.xyz, f.grid, f.batch, f.offsets, n_clouds, n, inv_voxel, f.num_down,
+              f.sindex, f.n_src, f.trunc_grid};
   if (n > 0) {
     k_bbox<<<blocks_for(n, 2048), 256, 0, s>>>(ps, b.pc_s, b.bbox, b.meta);
     ++nl;
   }
-  PointSrc pq{f.qxyz, nullptr, nullptr, f.qoffsets, n_clouds, m, f.voxel, f.num_down};
+  PointSrc pq{f.qxyz, nullptr, f.qbatch, f.qbatch ? nullptr : f.qoffsets, n_clouds, m, inv_voxel,
+              f.num_down, nullptr, m, f.trunc_grid};
   if (kind == FKNN_QUERY_GENERAL && m > 0) {
     k_bbox<<<blocks_for(m, 2048), 256, 0, s>>>(pq, b.pc_q, b.bbox, b.meta);
     ++nl;
@@ -622,7 +650,7 @@ int run_fused(const FusedArgs& f, void* ws, size_t ws_bytes, const QueryShape& s
     SortBuffers<uint64_t> sb{{b.keys64[0], b.keys64[1]}, {b.vals[0], b.vals[1]}, b.hist, b.totals};
     nl += launch_radix_sort(sb, n, key_bits, max_passes, s);
     const int tiles = blocks_for(n, 2048);
-    k_gather<uint64_t><<<tiles, 256, 0, s>>>(f.xyz, n, sp64, key_bits, b.srec,
+    k_gather<uint64_t><<<tiles, 256, 0, s>>>(f.xyz, f.sindex, f.n_src, n, sp64, key_bits, b.srec,
                                              b.pos_of, b.tile_counts);
     k_scan_tiles<<<1, 1024, 0, s>>>(b.tile_counts, tiles, &b.meta->n_cells);
     k_cells<uint64_t><<<tiles, 256, 0, s>>>(n, sp64, key_bits, b.tile_counts,
@@ -700,8 +728,8 @@ int run_fused(const FusedArgs& f, void* ws, size_t ws_bytes, const QueryShape& s
                                b.totals + kSortMaxPasses * 256};
       nl += launch_radix_sort(qb, m, key_bits, max_passes, s);
       const int tiles = blocks_for(m, 2048);
-      k_gather<uint64_t><<<tiles, 256, 0, s>>>(f.qxyz, m, sp64, key_bits, b.qrec, nullptr,
-                                               b.tile_counts);
+      k_gather<uint64_t><<<tiles, 256, 0, s>>>(f.qxyz, nullptr, m, m, sp64, key_bits, b.qrec,
+                                               nullptr, b.tile_counts);
       k_scan_tiles<<<1, 1024, 0, s>>>(b.tile_counts, tiles, &b.meta->n_groups);
       k_cells<uint64_t><<<tiles, 256, 0, s>>>(m, sp64, key_bits, b.tile_counts,
                                               &b.meta->n_groups, b.group_key, b.group_start,
@@ -711,7 +739,7 @@ int run_fused(const FusedArgs& f, void* ws, size_t ws_bytes, const QueryShape& s
           b.meta, b.runs);
       nl += 4;
       nl += launch_items(b.runs, b.group_start, nullptr, &b.meta->n_groups, m, shape.tile_records,
-                         b.cands, b.seg_counts, &b.meta->n_items, b.items, s);
+                         b.cands, b.seg_counts, &b.meta->n_items, b.items, s, &b.meta->status);
     }
   }
 

@@ -17,8 +17,12 @@ struct FusedArgs {
   const int64_t* offsets;        // cumulative cloud ends or null
   int64_t n;
   int64_t n_clouds;              // batch ids must lie in [0, n_clouds)
+  const int64_t* sindex;         // support point i is row sindex[i] of xyz/grid/batch, or null
+  int64_t n_src;                 // rows of xyz/grid/batch when sindex is given
+  int trunc_grid;                // voxelise with trunc(xyz / voxel) instead of floor
   const float* qxyz;             // general queries f32 [m,3]
   const int64_t* qoffsets;       // general queries' cloud ends
+  const int64_t* qbatch;         // general queries' batch ids (instead of qoffsets), or null
   const int64_t* query_indices;  // selected queries int64 [m]
   int64_t m;
   float voxel;

@@ -75,7 +75,8 @@ int launch_query(const QueryLaunch& q, const QueryShape& shape, cudaStream_t s);
 // greedy packing; *n_items_ptr receives the item count.  Returns launches.
 int launch_items(const int2* runs, const int32_t* group_start, const int32_t* group_row,
                  const int* group_count_ptr, int64_t max_groups, int tile, int32_t* cands,
-                 uint32_t* seg_counts, int* n_items_ptr, int4* items, cudaStream_t s);
+                 uint32_t* seg_counts, int* n_items_ptr, int4* items, cudaStream_t s,
+                 int* status = nullptr);
 size_t items_capacity(int64_t max_groups, int64_t n_queries);
 constexpr int kPackSegment = 16;
 inline int64_t pack_segments(int64_t max_groups) {

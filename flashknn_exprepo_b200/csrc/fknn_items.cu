@@ -18,10 +18,11 @@
 
 namespace fknn {
 
-// cands[g] = number of candidate records of group g (sum of its 27 runs).
+// cands[g] = number of candidate records of group g (sum of its 27 runs);
+// a group without candidates sets kStatusNoCandidates when status is given.
 __global__ void __launch_bounds__(256)
     k_group_cands(const int2* __restrict__ runs, const int32_t* __restrict__ group_row,
-                  const int* group_count_ptr, int32_t* __restrict__ cands) {
+                  const int* group_count_ptr, int32_t* __restrict__ cands, int* status) {
   const int n_groups = *group_count_ptr;
   for (int64_t g = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; g < n_groups;
        g += static_cast<int64_t>(gridDim.x) * blockDim.x) {
@@ -31,6 +32,7 @@ __global__ void __launch_bounds__(256)
 #pragma unroll
     for (int j = 0; j < kNeighbours; ++j) total += max(r[j].y, 0);
     cands[g] = total;
+    if (total == 0) raise_status(status, kStatusNoCandidates);
   }
 }
 
@@ -112,14 +114,15 @@ __global__ void __launch_bounds__(1024)
 
 int launch_items(const int2* runs, const int32_t* group_start, const int32_t* group_row,
                  const int* group_count_ptr, int64_t max_groups, int tile, int32_t* cands,
-                 uint32_t* seg_counts, int* n_items_ptr, int4* items, cudaStream_t s) {
+                 uint32_t* seg_counts, int* n_items_ptr, int4* items, cudaStream_t s,
+                 int* status) {
   if (max_groups <= 0) return 0;
   // grids for the host-side bound, capped: the device count drives the loops
   const int64_t gb = ceil_div(max_groups, 256);
   const int gblocks = static_cast<int>(gb < 2048 ? gb : 2048);
   const int64_t sb = ceil_div(ceil_div(max_groups, kPackSegment), 256);
   const int sblocks = static_cast<int>(sb < 1024 ? sb : 1024);
-  k_group_cands<<<gblocks, 256, 0, s>>>(runs, group_row, group_count_ptr, cands);
+  k_group_cands<<<gblocks, 256, 0, s>>>(runs, group_row, group_count_ptr, cands, status);
   k_pack<<<sblocks, 256, 0, s>>>(group_start, cands, group_count_ptr, tile, seg_counts, nullptr,
                                  nullptr);
   k_scan_segments<<<1, 1024, 0, s>>>(seg_counts, group_count_ptr, n_items_ptr);

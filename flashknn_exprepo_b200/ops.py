@@ -111,6 +111,40 @@ def knn_grid(xyz, grid_coord, batch_idx, k, num_down=2, cut_r2=math.inf, query_i
     return idx, dist
 
 
+def back_query(xyz, sel_indices, query_grid_size, k, batch_idx=None, idx_dtype=torch.int64,
+               config=None, validate=False):
+    """FlashKNN.back_query kernels: for every point of ``xyz`` the k nearest
+    points of the subset ``sel_indices`` in the 27 cells around its cell
+    (cells = trunc(xyz / query_grid_size)).  Returns (idx [n,k] positions in
+    ``sel_indices``, dist2 f32 [n,k], empty) where ``empty`` is True when some
+    point had no subset point around it (its row is (-1, +inf))."""
+    lib = _lib.load()
+    xyz = _require(xyz, "xyz", torch.float32, 2, 3)
+    dev = xyz.device
+    n = xyz.shape[0]
+    sel_indices = _require(sel_indices, "sel_indices", torch.int64, 1)
+    m = sel_indices.numel()
+    if batch_idx is not None:
+        batch_idx = _require(batch_idx, "batch_idx", torch.int64, 1)
+        if batch_idx.numel() != n:
+            raise ValueError("batch_idx must have one entry per point")
+    if idx_dtype not in (torch.int32, torch.int64):
+        raise ValueError("idx_dtype must be torch.int32 or torch.int64")
+    idx = torch.empty((n, k), dtype=idx_dtype, device=dev)
+    dist = torch.empty((n, k), dtype=torch.float32, device=dev)
+    ws = _lib.WORKSPACE.get(lib.fknn_back_query_workspace_bytes(n, m), dev)
+    _, cfg = _config_ptr(config)
+    rc = lib.fknn_back_query(ptr(xyz), n, ptr(sel_indices), m, ptr(batch_idx),
+                             float(query_grid_size), k, 64 if idx_dtype == torch.int64 else 32,
+                             ptr(idx), ptr(dist), ptr(ws), ws.numel(), cfg, stream_handle(dev))
+    check(rc, "fknn_back_query")
+    empty = None
+    if validate:
+        _lib.raise_on_status(ws, "back_query")
+        empty = bool(_lib.read_status(ws) & _lib.DEVICE_NO_CANDIDATES)
+    return idx, dist, empty
+
+
 def adaptive_query(grid_coord, batch_idx, k, xyz=None, min_factor=2, max_factor=8,
                    max_shift=None, cut_r2=math.inf, idx_dtype=torch.int64, config=None,
                    want_levels=False, validate=False):

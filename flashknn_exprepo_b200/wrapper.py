@@ -125,6 +125,34 @@ class FlashKNN:
         self._record("selected_query", t0, {"memory_mode": memory_mode})
         return (idx, dist) if return_distances else idx
 
+    @torch.no_grad()
+    def back_query(self, xyz, sel_indices, query_grid_size, down_grid_size, batch_idx,
+                   dynamic_load=True, memory_mode="SM"):
+        """Dense-to-subset map (FlashKnnWrapper.py:459-644): for every point of
+        ``xyz`` its ``num_nbr`` nearest points of the subset ``sel_indices``
+        among the subset points in the 27 cells around its cell, cells =
+        trunc(xyz / query_grid_size).  Returns positions in ``sel_indices``:
+        K == 1: int64 [N] (memory_mode "SM") or [N, 1] ("GM"); K > 1:
+        (int64 [N, K], f32 squared distances [N, K]), rows ascending (the
+        reference leaves them in heap order).  Like the reference, raises
+        AssertionError when some point has no subset point around it.
+        ``down_grid_size`` and ``dynamic_load`` are accepted and unused, as
+        in the reference."""
+        del down_grid_size, dynamic_load
+        if memory_mode not in {"SM", "GM"}:
+            raise ValueError(f"memory_mode must be 'SM' or 'GM', got {memory_mode!r}")
+        t0 = time.perf_counter() if self.debug else 0.0
+        idx, dist, empty = ops.back_query(xyz.float(), sel_indices, query_grid_size,
+                                          self.num_nbr, batch_idx, config=self.config,
+                                          validate=True)
+        if empty:
+            raise AssertionError("some query points have no support point in their "
+                                 "neighbourhood; consider a larger query_grid_size")
+        self._record("back_query", t0, {"memory_mode": memory_mode})
+        if self.num_nbr == 1:
+            return idx.flatten() if memory_mode == "SM" else idx
+        return idx, dist
+
     def rng_grid(self, rng, device="cuda"):
         """The 27 offsets (0,-1,+1)^3 in the reference's ij order, centre first."""
         if isinstance(rng, list):

@@ -51,6 +51,8 @@ extern "C" {
 #define FKNN_DEVICE_BAD_TABLE 2   /* a table names rows outside the point array */
 #define FKNN_DEVICE_TIMEOUT 4     /* a bounded wait on a bulk copy gave up */
 #define FKNN_DEVICE_BATCH_RANGE 8 /* batch id outside [0, 2^15) */
+#define FKNN_DEVICE_NO_CANDIDATES 16 /* informational: a query saw no candidate
+                                        (general / back queries pad it with -1) */
 
 /* Optional launch shape of the query kernel; NULL selects the defaults.
  * warps_per_cta in {1,2,4,8}; tile_records (candidate records staged per
@@ -115,6 +117,23 @@ FKNN_API int fknn_knn_grid(const float* xyz, const int64_t* grid_coord, const in
                   int32_t num_down, float cut_r2, int32_t idx_bits, void* idx_out,
                   float* dist_out, void* workspace, size_t workspace_bytes,
                   const fknn_config* config, void* stream);
+
+/* FlashKNN.back_query (FlashKNN/functions/FlashKnnWrapper.py:459-644, kernels
+ * FlashKNN_Nearest_Back_Query_DL / FlashKNN_Back_Query_DL,
+ * flash_knn_query_dynamic_load.cu:949-1208): for every point of xyz [n,3]
+ * the k nearest points of the subset sel_indices [m] (rows of xyz) among the
+ * subset points in the 27 cells around the point's cell, cells =
+ * trunc(xyz / query_grid_size) per batch (batch_idx int64 [n] or NULL).
+ * idx_out [n,k] (idx_bits 64: int64, 32: int32) holds positions in
+ * sel_indices (0..m-1), ascending by (distance, position); dist_out f32
+ * [n,k].  A point with no subset point around it gets (-1, +inf) and sets
+ * FKNN_DEVICE_NO_CANDIDATES (the reference asserts that this never
+ * happens). */
+FKNN_API size_t fknn_back_query_workspace_bytes(int64_t n, int64_t m);
+FKNN_API int fknn_back_query(const float* xyz, int64_t n, const int64_t* sel_indices, int64_t m,
+                    const int64_t* batch_idx, float query_grid_size, int32_t k,
+                    int32_t idx_bits, void* idx_out, float* dist_out, void* workspace,
+                    size_t workspace_bytes, const fknn_config* config, void* stream);
 
 /* AdaptiveNeighborhoodFlashKNN.query (FlashKNN/functions/adaptive_octree.py
  * :505-612): every point takes its exact top-K over the 27 same-level nodes

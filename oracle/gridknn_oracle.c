@@ -370,8 +370,12 @@ int orc_knn_general(const float* sxyz, const int64_t* sgrid,
 
 /*
  * Pointcept-style offset batching on top of orc_knn_general: offsets are
- * cumulative cloud ends, grid = floor(xyz / voxel) in FP32 (the reference
- * callers' voxelisation, Query/benchmark_s3dis.py:159), batch = cloud id.
+ * cumulative cloud ends, grid = floor(xyz * (1 / voxel)) in FP32, batch =
+ * cloud id.  The reference's callers voxelise with torch.floor(coord /
+ * voxel_size) on CUDA tensors (Query/benchmark_s3dis.py:159,
+ * Networks/hierarchy.py:30): PyTorch evaluates a CUDA tensor divided by a
+ * Python scalar as a product with the scalar's FP32 reciprocal, so that is
+ * the rounding restated here.
  * qxyz == NULL means a self query (pad = own index); otherwise pad = -1.
  */
 int orc_knn_offsets(const float* xyz, const int64_t* offsets, int64_t b,
@@ -379,6 +383,7 @@ int orc_knn_offsets(const float* xyz, const int64_t* offsets, int64_t b,
                     int num_down, int k, float cut_r2, int variant,
                     int32_t* idx_out, float* dist_out, int nthreads) {
   int64_t n = b ? offsets[b - 1] : 0;
+  const float inv = 1.0f / voxel;
   int self = qxyz == NULL;
   if (self) { qxyz = xyz; qoffsets = offsets; }
   int64_t m = b ? qoffsets[b - 1] : 0;
@@ -391,13 +396,13 @@ int orc_knn_offsets(const float* xyz, const int64_t* offsets, int64_t b,
   for (int64_t i = 0; i < n; ++i) {
     while (c < b && i >= offsets[c]) ++c;
     sb[i] = c;
-    for (int a = 0; a < 3; ++a) sg[3 * i + a] = (int64_t)floorf(xyz[3 * i + a] / voxel);
+    for (int a = 0; a < 3; ++a) sg[3 * i + a] = (int64_t)floorf(xyz[3 * i + a] * inv);
   }
   c = 0;
   for (int64_t i = 0; i < m; ++i) {
     while (c < b && i >= qoffsets[c]) ++c;
     qb[i] = c;
-    for (int a = 0; a < 3; ++a) qg[3 * i + a] = (int64_t)floorf(qxyz[3 * i + a] / voxel);
+    for (int a = 0; a < 3; ++a) qg[3 * i + a] = (int64_t)floorf(qxyz[3 * i + a] * inv);
     if (pad) pad[i] = i;
   }
   int rc = orc_knn_general(xyz, sg, sb, n, qxyz, qg, qb, m, num_down, k, cut_r2,
@@ -649,5 +654,114 @@ int orc_adaptive_query(const int64_t* grid, const int64_t* batch, int64_t n,
   for (int s = 0; s < L; ++s) { free(nkey[s]); free(nstart[s]); free(ncand[s]); }
   free(ncount); free(ncand); free(nstart); free(nkey); free(node_of);
   free(order); free(key); free(norm);
+  return 0;
+}
+
+/* ------------------------------------------------------------ back query */
+
+/*
+ * FlashKNN_Back_Query_DL / FlashKNN_Nearest_Back_Query_DL over the tables
+ * FlashKNN.back_query builds (FlashKnnWrapper.py:459-585; kernels
+ * flash_knn_query_dynamic_load.cu:949-1208): xyz_h [*,3] every point in key
+ * order, xyz_l [*,3] the subset in key order, steps_h / steps_l [p+1] the
+ * cell ranges of both, neigh [p*27] (-1 = no cell).  For each point of cell
+ * c, the k nearest subset points of the 27 cells around c.  Rows follow
+ * xyz_h; indices are subset positions (rows of xyz_l); rows ascending by
+ * (distance, position), padding (-1, +inf).  The reference keeps the k best
+ * under strict '<' and writes them in heap order (k > 1) or keeps the first
+ * nearest met (k == 1); the neighbour set is the same up to equal distances.
+ */
+int orc_back_query_tables(const float* xyz_h, const float* xyz_l,
+                          const int32_t* steps_h, const int32_t* steps_l,
+                          const int32_t* neigh, int64_t p, int k, int variant,
+                          int64_t* idx_out, float* dist_out, int nthreads) {
+  if (k < 1 || k > ORC_MAXK) return -1;
+#ifdef _OPENMP
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+#pragma omp parallel for schedule(dynamic, 16)
+#endif
+  for (int64_t c = 0; c < p; ++c) {
+    for (int64_t q = steps_h[c]; q < steps_h[c + 1]; ++q) {
+      float dl[ORC_MAXK];
+      int64_t il[ORC_MAXK];
+      for (int j = 0; j < k; ++j) { dl[j] = INFINITY; il[j] = INT64_MAX; }
+      for (int j = 0; j < 27; ++j) {
+        int32_t nb = neigh[c * 27 + j];
+        if (nb < 0) continue;
+        for (int64_t t = steps_l[nb]; t < steps_l[nb + 1]; ++t)
+          topk_insert(sqdist(xyz_l + 3 * t, xyz_h + 3 * q, variant), t, dl, il, k);
+      }
+      for (int j = 0; j < k; ++j) {
+        idx_out[q * k + j] = il[j] == INT64_MAX ? -1 : il[j];
+        dist_out[q * k + j] = dl[j];
+      }
+    }
+  }
+  return 0;
+}
+
+/*
+ * FlashKNN.back_query end to end (FlashKnnWrapper.py:459-644) from its
+ * inputs: cells = trunc(xyz * (1 / size)) in FP32 (the wrapper's
+ * (xyz / size).long() on CUDA tensors, where PyTorch multiplies by the FP32
+ * reciprocal of the Python scalar),
+ * keyed like FlashKNN_Morton_Encode (16 bits per axis, batch << 48); for
+ * every point i the k nearest subset points sel[j] among the subset points
+ * whose cell is one of the 27 cells around i's cell; reported index = j,
+ * the position in sel (the wrapper's order_l remap).  Ties by the lower j;
+ * padding (-1, +inf); empty_out[i] = 1 when i has no candidate (the wrapper
+ * asserts that none has).  batch may be NULL.
+ */
+int orc_back_query(const float* xyz, int64_t n, const int64_t* sel, int64_t m,
+                   const int64_t* batch, float size, int k, int variant,
+                   int64_t* idx_out, float* dist_out, int32_t* empty_out, int nthreads) {
+  if (k < 1 || k > ORC_MAXK) return -1;
+  int64_t* g = (int64_t*)malloc(sizeof(int64_t) * 3 * (size_t)(n ? n : 1));
+  const float inv = 1.0f / size;
+  for (int64_t i = 0; i < 3 * n; ++i) g[i] = (int64_t)(xyz[i] * inv);
+  int64_t* skey = (int64_t*)malloc(sizeof(int64_t) * (size_t)(m ? m : 1));
+  int64_t* sorder = (int64_t*)malloc(sizeof(int64_t) * (size_t)(m ? m : 1));
+  for (int64_t j = 0; j < m; ++j) {
+    int64_t r = sel[j];
+    skey[j] = orc_morton_key(g[3 * r], g[3 * r + 1], g[3 * r + 2], batch ? batch[r] : 0);
+  }
+  orc_argsort_i64(skey, m, sorder);
+  int64_t* cell_key = (int64_t*)malloc(sizeof(int64_t) * (size_t)(m ? m : 1));
+  int64_t* cell_start = (int64_t*)malloc(sizeof(int64_t) * (size_t)(m + 1));
+  int64_t p = 0;
+  for (int64_t s = 0; s < m; ++s) {
+    int64_t key = skey[sorder[s]];
+    if (s == 0 || key != cell_key[p - 1]) { cell_key[p] = key; cell_start[p] = s; ++p; }
+  }
+  cell_start[p] = m;
+#ifdef _OPENMP
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+#pragma omp parallel for schedule(dynamic, 64)
+#endif
+  for (int64_t i = 0; i < n; ++i) {
+    float dl[ORC_MAXK];
+    int64_t il[ORC_MAXK];
+    for (int j = 0; j < k; ++j) { dl[j] = INFINITY; il[j] = INT64_MAX; }
+    int64_t b = batch ? batch[i] : 0;
+    int any = 0;
+    for (int j = 0; j < 27; ++j) {
+      int64_t key = orc_morton_key(g[3 * i] + axis_offset(j / 9),
+                                   g[3 * i + 1] + axis_offset((j / 3) % 3),
+                                   g[3 * i + 2] + axis_offset(j % 3), b);
+      int64_t c = search_sorted(cell_key, p, key);
+      if (c < 0) continue;
+      for (int64_t s = cell_start[c]; s < cell_start[c + 1]; ++s) {
+        int64_t t = sorder[s];
+        any = 1;
+        topk_insert(sqdist(xyz + 3 * sel[t], xyz + 3 * i, variant), t, dl, il, k);
+      }
+    }
+    for (int j = 0; j < k; ++j) {
+      idx_out[i * k + j] = il[j] == INT64_MAX ? -1 : il[j];
+      dist_out[i * k + j] = dl[j];
+    }
+    if (empty_out) empty_out[i] = any ? 0 : 1;
+  }
+  free(cell_start); free(cell_key); free(sorder); free(skey); free(g);
   return 0;
 }

@@ -67,6 +67,10 @@ def _declare(L):
     L.orc_brute_knn_f64.argtypes = [P, P, I64, P, P, I32, P, P, I32]
     L.orc_backward_f64.restype = None
     L.orc_backward_f64.argtypes = [P, I64, P, I64, P, P, P, I32, P, P]
+    L.orc_back_query_tables.restype = I32
+    L.orc_back_query_tables.argtypes = [P, P, P, P, P, I64, I32, I32, P, P, I32]
+    L.orc_back_query.restype = I32
+    L.orc_back_query.argtypes = [P, I64, P, I64, P, F32, I32, I32, P, P, P, I32]
     L.orc_adaptive_query.restype = I32
     L.orc_adaptive_query.argtypes = [P, P, I64, P, I32, I32, I32, I32, F32, I32, P, P, P, I32]
 
@@ -275,3 +279,42 @@ def adaptive_query(grid, batch, k, xyz=None, min_factor=2, max_factor=8, max_shi
     if rc != 0:
         raise ValueError(f"orc_adaptive_query failed with {rc}")
     return levels, idx, dist
+
+
+def back_query_tables(xyz_h, xyz_l, steps_h, steps_l, neigh, k, variant=DEFAULT_VARIANT,
+                      nthreads=0):
+    """FlashKNN_Back_Query_DL semantics over the wrapper's tables: rows follow
+    xyz_h, indices are rows of xyz_l; (idx int64 [nh,k], dist f32 [nh,k])."""
+    xyz_h = _c(xyz_h, np.float32)
+    xyz_l = _c(xyz_l, np.float32)
+    steps_h = _c(steps_h, np.int32)
+    steps_l = _c(steps_l, np.int32)
+    neigh = _c(neigh, np.int32)
+    p = neigh.shape[0]
+    nh = xyz_h.shape[0]
+    idx = np.empty((nh, k), np.int64)
+    dist = np.empty((nh, k), np.float32)
+    rc = lib().orc_back_query_tables(_ptr(xyz_h), _ptr(xyz_l), _ptr(steps_h), _ptr(steps_l),
+                                     _ptr(neigh), p, k, variant, _ptr(idx), _ptr(dist), nthreads)
+    if rc != 0:
+        raise ValueError(f"orc_back_query_tables failed with {rc}")
+    return idx, dist
+
+
+def back_query(xyz, sel_indices, query_grid_size, k, batch=None, variant=DEFAULT_VARIANT,
+               nthreads=0):
+    """FlashKNN.back_query end to end: (idx int64 [n,k] positions in
+    sel_indices, dist f32 [n,k], empty bool [n])."""
+    xyz = _c(xyz, np.float32)
+    sel_indices = _c(sel_indices, np.int64)
+    batch = _c(batch, np.int64)
+    n, m = xyz.shape[0], sel_indices.shape[0]
+    idx = np.empty((n, k), np.int64)
+    dist = np.empty((n, k), np.float32)
+    empty = np.empty(n, np.int32)
+    rc = lib().orc_back_query(_ptr(xyz), n, _ptr(sel_indices), m, _ptr(batch),
+                              float(np.float32(query_grid_size)), k, variant, _ptr(idx),
+                              _ptr(dist), _ptr(empty), nthreads)
+    if rc != 0:
+        raise ValueError(f"orc_back_query failed with {rc}")
+    return idx, dist, empty.astype(bool)

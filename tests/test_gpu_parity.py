@@ -261,7 +261,8 @@ def test_c4_batched_full_size_properties_and_sampled_rows(fk):
     # sampled rows, bit-exact against the oracle
     rng = np.random.default_rng(1)
     rows = np.sort(rng.choice(n, 20000, replace=False))
-    grid = np.floor(b.xyz / np.float32(S.C4_VOXEL)).astype(np.int64)
+    # knn_offsets voxelises as floor(x * (1 / voxel)) in FP32
+    grid = np.floor(b.xyz * (np.float32(1) / np.float32(S.C4_VOXEL))).astype(np.int64)
     oi, od = O.knn_general(b.xyz, grid, cloud, b.xyz[rows], grid[rows], cloud[rows], 2, 16,
                            pad=rows)
     assert np.array_equal(gi[rows], oi)
