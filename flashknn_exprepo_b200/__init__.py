@@ -7,12 +7,14 @@ Public entry points (mirroring the reference's ``FlashKNN/functions``):
   AdaptiveNeighborhoodFlashKNN
                         -- per-point octree level (adaptive.py)
   xyz2key               -- Morton keys (z_order.py)
+  hierarchy             -- voxel-first subsampling and the DeLA hierarchy
+                           builder (hierarchy.py)
   ops                   -- tensor-level C-ABI calls, incl. the reference
                            table ABI (query_tables, build_tables, ...)
 The CUDA library is libfknn.so next to this file (``python -m
 flashknn_exprepo_b200.build``); nothing falls back to the CPU.
 """
-from . import ops
+from . import hierarchy, ops
 from ._lib import FknnError
 from .adaptive import AdaptiveNeighborhoodFlashKNN
 from .pointops import KNNQuery, knn_query
@@ -20,4 +22,4 @@ from .wrapper import FlashKNN
 from .z_order import xyz2key
 
 __all__ = ["FlashKNN", "AdaptiveNeighborhoodFlashKNN", "KNNQuery", "knn_query", "xyz2key",
-           "ops", "FknnError"]
+           "hierarchy", "ops", "FknnError"]

@@ -91,6 +91,8 @@ _SIGNATURES = {
     "fknn_back_query_workspace_bytes": (_SZ, [_I64, _I64]),
     "fknn_back_query": (ctypes.c_int, [_P, _I64, _P, _I64, _P, _F32, _I32, _I32, _P, _P, _P, _SZ,
                                        _P, _P]),
+    "fknn_voxel_first_workspace_bytes": (_SZ, [_I64]),
+    "fknn_voxel_first": (ctypes.c_int, [_P, _I64, _P, _F32, _P, _P, _P, _SZ, _P]),
     "fknn_adaptive_workspace_bytes": (_SZ, [_I64]),
     "fknn_adaptive_query": (ctypes.c_int, [_P, _P, _I64, _P, _I32, _I32, _I32, _I32, _F32, _I32,
                                            _P, _P, _P, _P, _SZ, _P, _P]),

@@ -13,6 +13,7 @@
 #include "fknn_grid.h"
 #include "fknn_internal.h"
 #include "fknn_tables.h"
+#include "fknn_voxel.h"
 
 namespace fknn {
 
@@ -386,6 +387,24 @@ int fknn_back_query(const float* xyz, int64_t n, const int64_t* sel_indices, int
   f.dist_out = dist_out;
   int launches = 0;
   rc = fknn::run_fused(f, workspace, workspace_bytes, shape, as_stream(stream), &launches);
+  return finish(rc, launches);
+}
+
+size_t fknn_voxel_first_workspace_bytes(int64_t n) {
+  if (n < 0) return 0;
+  return fknn::voxel_first_workspace_bytes(n);
+}
+
+int fknn_voxel_first(const float* xyz, int64_t n, const int64_t* batch_idx, float voxel,
+                     int64_t* out, int64_t* count_out, void* workspace, size_t workspace_bytes,
+                     void* stream) {
+  if (n < 0 || !(voxel > 0.f)) return FKNN_ERR_ARG;
+  if (n > kMaxPoints) return FKNN_ERR_SIZE;
+  if (!workspace || !count_out || (n > 0 && (!xyz || !out))) return FKNN_ERR_ARG;
+  if (!aligned(workspace, 256)) return FKNN_ERR_ARG;
+  const fknn::VoxelArgs v{xyz, batch_idx, n, voxel, out, count_out};
+  int launches = 0;
+  const int rc = fknn::run_voxel_first(v, workspace, workspace_bytes, as_stream(stream), &launches);
   return finish(rc, launches);
 }
 

@@ -145,6 +145,29 @@ def back_query(xyz, sel_indices, query_grid_size, k, batch_idx=None, idx_dtype=t
     return idx, dist, empty
 
 
+def voxel_first(xyz, voxel, batch_idx=None, validate=False):
+    """Voxel-first subsampling: the lowest index of every occupied voxel
+    (voxel = floor(xyz * (1 / voxel))), ascending int64.  Reads the count back
+    (one synchronisation)."""
+    lib = _lib.load()
+    xyz = _require(xyz, "xyz", torch.float32, 2, 3)
+    dev = xyz.device
+    n = xyz.shape[0]
+    if batch_idx is not None:
+        batch_idx = _require(batch_idx, "batch_idx", torch.int64, 1)
+        if batch_idx.numel() != n:
+            raise ValueError("batch_idx must have one entry per point")
+    out = torch.empty(n, dtype=torch.int64, device=dev)
+    count = torch.empty(1, dtype=torch.int64, device=dev)
+    ws = _lib.WORKSPACE.get(lib.fknn_voxel_first_workspace_bytes(n), dev)
+    rc = lib.fknn_voxel_first(ptr(xyz), n, ptr(batch_idx), float(voxel), ptr(out), ptr(count),
+                              ptr(ws), ws.numel(), stream_handle(dev))
+    check(rc, "fknn_voxel_first")
+    if validate:
+        _lib.raise_on_status(ws, "voxel_first")
+    return out[: int(count.item())]
+
+
 def adaptive_query(grid_coord, batch_idx, k, xyz=None, min_factor=2, max_factor=8,
                    max_shift=None, cut_r2=math.inf, idx_dtype=torch.int64, config=None,
                    want_levels=False, validate=False):

@@ -135,6 +135,18 @@ FKNN_API int fknn_back_query(const float* xyz, int64_t n, const int64_t* sel_ind
                     int32_t idx_bits, void* idx_out, float* dist_out, void* workspace,
                     size_t workspace_bytes, const fknn_config* config, void* stream);
 
+/* Voxel-first subsampling, _voxel_first_cuda (Networks/hierarchy.py:23-35):
+ * one representative per occupied voxel -- voxel = floor(xyz * (1/voxel))
+ * in FP32 (PyTorch's evaluation of torch.floor(xyz / voxel) on CUDA), keyed
+ * by its 16-bit-per-axis Morton key (batch << 48 when batch_idx is given,
+ * ids in [0, 32768)) -- the lowest index of each voxel.  out [n] int64
+ * receives the representatives in ascending order, *count_out (int64, device
+ * memory) their number. */
+FKNN_API size_t fknn_voxel_first_workspace_bytes(int64_t n);
+FKNN_API int fknn_voxel_first(const float* xyz, int64_t n, const int64_t* batch_idx, float voxel,
+                     int64_t* out, int64_t* count_out, void* workspace, size_t workspace_bytes,
+                     void* stream);
+
 /* AdaptiveNeighborhoodFlashKNN.query (FlashKNN/functions/adaptive_octree.py
  * :505-612): every point takes its exact top-K over the 27 same-level nodes
  * of the octree level picked by coarse-to-fine candidate counting (descend

@@ -765,3 +765,33 @@ int orc_back_query(const float* xyz, int64_t n, const int64_t* sel, int64_t m,
   free(cell_start); free(cell_key); free(sorder); free(skey); free(g);
   return 0;
 }
+
+/* -------------------------------------------------- voxel-first subsampling */
+
+/*
+ * Voxel-first subsampling (Networks/hierarchy.py:23-35, _voxel_first_cuda):
+ * voxel = floor(xyz * (1 / size)) in FP32 (torch.floor(xyz / size) on CUDA
+ * tensors multiplies by the FP32 reciprocal), key = the 16-bit-per-axis
+ * Morton key of the voxel (xyz2key, no batch unless batch != NULL: then
+ * batch << 48), one representative per key -- the first point of the key in
+ * a stable sort, i.e. the lowest index -- and the representatives' indices
+ * ascending.  out[n] receives them; returns their count.
+ */
+int64_t orc_voxel_first(const float* xyz, int64_t n, const int64_t* batch, float size,
+                        int64_t* out) {
+  const float inv = 1.0f / size;
+  int64_t* key = (int64_t*)malloc(sizeof(int64_t) * (size_t)(n ? n : 1));
+  int64_t* order = (int64_t*)malloc(sizeof(int64_t) * (size_t)(n ? n : 1));
+  unsigned char* keep = (unsigned char*)calloc((size_t)(n ? n : 1), 1);
+  for (int64_t i = 0; i < n; ++i)
+    key[i] = orc_morton_key((int64_t)floorf(xyz[3 * i] * inv), (int64_t)floorf(xyz[3 * i + 1] * inv),
+                            (int64_t)floorf(xyz[3 * i + 2] * inv), batch ? batch[i] : 0);
+  orc_argsort_i64(key, n, order);
+  for (int64_t s = 0; s < n; ++s)
+    if (s == 0 || key[order[s]] != key[order[s - 1]]) keep[order[s]] = 1;
+  int64_t c = 0;
+  for (int64_t i = 0; i < n; ++i)
+    if (keep[i]) out[c++] = i;
+  free(keep); free(order); free(key);
+  return c;
+}

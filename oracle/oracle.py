@@ -71,6 +71,8 @@ def _declare(L):
     L.orc_back_query_tables.argtypes = [P, P, P, P, P, I64, I32, I32, P, P, I32]
     L.orc_back_query.restype = I32
     L.orc_back_query.argtypes = [P, I64, P, I64, P, F32, I32, I32, P, P, P, I32]
+    L.orc_voxel_first.restype = I64
+    L.orc_voxel_first.argtypes = [P, I64, P, F32, P]
     L.orc_adaptive_query.restype = I32
     L.orc_adaptive_query.argtypes = [P, P, I64, P, I32, I32, I32, I32, F32, I32, P, P, P, I32]
 
@@ -318,3 +320,14 @@ def back_query(xyz, sel_indices, query_grid_size, k, batch=None, variant=DEFAULT
     if rc != 0:
         raise ValueError(f"orc_back_query failed with {rc}")
     return idx, dist, empty.astype(bool)
+
+
+def voxel_first(xyz, size, batch=None):
+    """Voxel-first subsampling (one lowest-index point per occupied voxel):
+    int64 indices, ascending."""
+    xyz = _c(xyz, np.float32)
+    batch = _c(batch, np.int64)
+    n = xyz.shape[0]
+    out = np.empty(max(n, 1), np.int64)
+    c = lib().orc_voxel_first(_ptr(xyz), n, _ptr(batch), float(np.float32(size)), _ptr(out))
+    return out[:c].copy()

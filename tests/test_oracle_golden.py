@@ -257,3 +257,47 @@ def test_oracle_back_query_matches_reference_wrapper(case):
     assert np.array_equal(dist.view(np.uint32), np.sort(z["ref_dist"], 1).view(np.uint32))
     ref_sorted = np.take_along_axis(z["ref_idx"], np.argsort(z["ref_dist"], 1, kind="stable"), 1)
     assert same_up_to_kth_ties(idx, dist, ref_sorted, np.sort(z["ref_dist"], 1))
+
+
+def hierarchy_cases():
+    return sorted(f[len("hierarchy_"):-4] for f in os.listdir(GOLDEN)
+                  if f.startswith("hierarchy_") and f.endswith(".npz"))
+
+
+def oracle_hierarchy(xyz, sizes, ks, alpha):
+    """build_flash_hierarchy (Networks/hierarchy.py:38-96) composed from the
+    oracle's voxel-first subsampling, self query and back query."""
+    num_down = int(round(np.log2(alpha)))
+    current, cumulative = xyz, np.arange(len(xyz))
+    forward, levels = [], []
+    for level, (size, k) in enumerate(zip(sizes, ks)):
+        if level:
+            local = O.voxel_first(current, size)
+            current = np.ascontiguousarray(current[local])
+            cumulative = cumulative[local]
+            forward.append(local)
+            levels.append(cumulative)
+        idx, _ = O.knn_offsets(current, np.array([len(current)]), int(k), size, num_down)
+        forward.append(idx.astype(np.int64))
+    backward = []
+    for level in range(len(levels) - 1, -1, -1):
+        size = sizes[level + 1]
+        idx, _, empty = O.back_query(xyz, levels[level], np.float32(2 * size), 1)
+        assert not empty.any()
+        backward.append(idx[:, 0])
+    return forward + backward
+
+
+@pytest.mark.parametrize("case", hierarchy_cases())
+def test_oracle_hierarchy_matches_reference_builder(case):
+    """Voxel-first subsampling and the four-level DeLA hierarchy against the
+    reference's own Networks/hierarchy.py (tests/golden/make_golden_hierarchy.py):
+    every output tensor identical."""
+    z = np.load(os.path.join(GOLDEN, f"hierarchy_{case}.npz"))
+    sizes = [float(s) for s in z["voxel_sizes"]]
+    for i, s in enumerate(sizes):
+        assert np.array_equal(O.voxel_first(z["xyz"], s), z[f"voxel_first_{i}"])
+    outs = oracle_hierarchy(z["xyz"], sizes, [int(k) for k in z["ks"]], int(z["alpha"]))
+    assert len(outs) == int(z["n_outputs"])
+    for i, o in enumerate(outs):
+        assert np.array_equal(o, z[f"ref_{i}"]), i
