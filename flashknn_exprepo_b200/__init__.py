@@ -4,6 +4,10 @@ Public entry points (mirroring the reference's ``FlashKNN/functions``):
   FlashKNN              -- query / selected_query drop-in (wrapper.py)
   knn_query, KNNQuery   -- Pointcept-style offset batching with a
                            differentiable squared distance (pointops.py)
+  ball_query            -- radius-limited grid query, Pointcept's signature
+  grouping, knn_query_and_group, ball_query_and_group
+                        -- neighbour feature gather with a deterministic
+                           backward (pointops.py)
   AdaptiveNeighborhoodFlashKNN
                         -- per-point octree level (adaptive.py)
   xyz2key               -- Morton keys (z_order.py)
@@ -17,9 +21,12 @@ flashknn_exprepo_b200.build``); nothing falls back to the CPU.
 from . import hierarchy, ops
 from ._lib import FknnError
 from .adaptive import AdaptiveNeighborhoodFlashKNN
-from .pointops import KNNQuery, knn_query
+from .pointops import (KNNQuery, ball_query, ball_query_and_group, grouping, knn_query,
+                       knn_query_and_group)
 from .wrapper import FlashKNN
 from .z_order import xyz2key
 
-__all__ = ["FlashKNN", "AdaptiveNeighborhoodFlashKNN", "KNNQuery", "knn_query", "xyz2key",
+__all__ = ["FlashKNN", "AdaptiveNeighborhoodFlashKNN", "KNNQuery", "knn_query", "ball_query",
+           "grouping", "knn_query_and_group", "ball_query_and_group",
+           "xyz2key",
            "hierarchy", "ops", "FknnError"]

@@ -72,6 +72,8 @@ _SIGNATURES = {
     "fknn_workspace_bytes": (_SZ, [_I64, _I64, _I64, _I32]),
     "fknn_knn_offsets": (ctypes.c_int, [_P, _I64, _P, _I64, _P, _I64, _P, _I32, _F32, _I32,
                                         _F32, _P, _P, _P, _SZ, _P, _P]),
+    "fknn_ball_query": (ctypes.c_int, [_P, _I64, _P, _I64, _P, _I64, _P, _I32, _F32, _I32, _F32,
+                                       _P, _P, _P, _SZ, _P, _P]),
     "fknn_knn_grid": (ctypes.c_int, [_P, _P, _P, _I64, _P, _I64, _I32, _I32, _F32, _I32, _P, _P,
                                      _P, _SZ, _P, _P]),
     "fknn_tables_workspace_bytes": (_SZ, [_I64, _I64, _I64]),
@@ -91,6 +93,11 @@ _SIGNATURES = {
     "fknn_back_query_workspace_bytes": (_SZ, [_I64, _I64]),
     "fknn_back_query": (ctypes.c_int, [_P, _I64, _P, _I64, _P, _F32, _I32, _I32, _P, _P, _P, _SZ,
                                        _P, _P]),
+    "fknn_group_workspace_bytes": (_SZ, [_I64, _I32, _I64]),
+    "fknn_group_features": (ctypes.c_int, [_P, _I64, _I32, _P, _I64, _I32, _P, _P, _I32, _P, _P,
+                                           _SZ, _P]),
+    "fknn_group_backward": (ctypes.c_int, [_P, _I64, _I32, _P, _I64, _I32, _I32, _P, _P, _I32, _P,
+                                           _I32, _P, _SZ, _P]),
     "fknn_voxel_first_workspace_bytes": (_SZ, [_I64]),
     "fknn_voxel_first": (ctypes.c_int, [_P, _I64, _P, _F32, _P, _P, _P, _SZ, _P]),
     "fknn_adaptive_workspace_bytes": (_SZ, [_I64]),

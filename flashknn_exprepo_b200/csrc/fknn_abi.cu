@@ -11,6 +11,7 @@
 #include "fknn_backward.h"
 #include "fknn_adaptive.h"
 #include "fknn_grid.h"
+#include "fknn_group.h"
 #include "fknn_internal.h"
 #include "fknn_tables.h"
 #include "fknn_voxel.h"
@@ -183,11 +184,16 @@ size_t fknn_workspace_bytes(int64_t n_support, int64_t n_query, int64_t n_clouds
   return fknn::fused_workspace_bytes(n_support, n_query, n_clouds, query_kind);
 }
 
-int fknn_knn_offsets(const float* xyz, int64_t n, const int64_t* offsets, int64_t n_clouds,
-                     const float* new_xyz, int64_t m, const int64_t* new_offsets, int32_t k,
-                     float voxel, int32_t num_down, float cut_r2, int32_t* idx_out,
-                     float* dist_out, void* workspace, size_t workspace_bytes,
-                     const fknn_config* config, void* stream) {
+}  // extern "C"
+
+namespace {
+
+// Offset-batched grid query shared by fknn_knn_offsets and fknn_ball_query.
+int offsets_query(const float* xyz, int64_t n, const int64_t* offsets, int64_t n_clouds,
+                  const float* new_xyz, int64_t m, const int64_t* new_offsets, int32_t k,
+                  float voxel, int32_t num_down, float cut_r2, bool pad_minus_one,
+                  int32_t* idx_out, float* dist_out, void* workspace, size_t workspace_bytes,
+                  const fknn_config* config, void* stream) {
   int rc = check_k(k);
   if (rc) return rc;
   const bool general = new_xyz != nullptr;
@@ -215,12 +221,39 @@ int fknn_knn_offsets(const float* xyz, int64_t n, const int64_t* offsets, int64_
   f.num_down = num_down;
   f.k = k;
   f.cut_r2 = cut_r2;
+  f.pad_minus_one = pad_minus_one ? 1 : 0;
   f.idx_bits = 32;
   f.idx_out = idx_out;
   f.dist_out = dist_out;
   int launches = 0;
   rc = fknn::run_fused(f, workspace, workspace_bytes, shape, as_stream(stream), &launches);
   return finish(rc, launches);
+}
+
+}  // namespace
+
+extern "C" {
+
+int fknn_knn_offsets(const float* xyz, int64_t n, const int64_t* offsets, int64_t n_clouds,
+                     const float* new_xyz, int64_t m, const int64_t* new_offsets, int32_t k,
+                     float voxel, int32_t num_down, float cut_r2, int32_t* idx_out,
+                     float* dist_out, void* workspace, size_t workspace_bytes,
+                     const fknn_config* config, void* stream) {
+  return offsets_query(xyz, n, offsets, n_clouds, new_xyz, m, new_offsets, k, voxel, num_down,
+                       cut_r2, false, idx_out, dist_out, workspace, workspace_bytes, config,
+                       stream);
+}
+
+int fknn_ball_query(const float* xyz, int64_t n, const int64_t* offsets, int64_t n_clouds,
+                    const float* new_xyz, int64_t m, const int64_t* new_offsets, int32_t nsample,
+                    float voxel, int32_t num_down, float max_radius, int32_t* idx_out,
+                    float* dist_out, void* workspace, size_t workspace_bytes,
+                    const fknn_config* config, void* stream) {
+  if (!(max_radius > 0.f)) return FKNN_ERR_ARG;
+  const float r2 = max_radius * max_radius;  // FP32, as the ball-query kernels square it
+  return offsets_query(xyz, n, offsets, n_clouds, new_xyz, m, new_offsets, nsample, voxel,
+                       num_down, r2, true, idx_out, dist_out, workspace, workspace_bytes, config,
+                       stream);
 }
 
 int fknn_knn_grid(const float* xyz, const int64_t* grid_coord, const int64_t* batch_idx,
@@ -405,6 +438,74 @@ int fknn_voxel_first(const float* xyz, int64_t n, const int64_t* batch_idx, floa
   const fknn::VoxelArgs v{xyz, batch_idx, n, voxel, out, count_out};
   int launches = 0;
   const int rc = fknn::run_voxel_first(v, workspace, workspace_bytes, as_stream(stream), &launches);
+  return finish(rc, launches);
+}
+
+size_t fknn_group_workspace_bytes(int64_t m, int32_t k, int64_t n) {
+  if (m < 0 || k < 1 || n < 0) return 0;
+  return fknn::group_workspace_bytes(m * k, n);
+}
+
+namespace {
+int group_args_check(int64_t n, int32_t c, const int32_t* idx, int64_t m, int32_t k,
+                     void* workspace) {
+  if (n < 0 || m < 0 || c < 1 || k < 1) return FKNN_ERR_ARG;
+  if (n > kMaxPoints || m * static_cast<int64_t>(k) > kMaxPoints) return FKNN_ERR_SIZE;
+  if (!workspace || (m > 0 && !idx)) return FKNN_ERR_ARG;
+  if (!aligned(workspace, 256)) return FKNN_ERR_ARG;
+  return FKNN_OK;
+}
+}  // namespace
+
+int fknn_group_features(const float* feat, int64_t n, int32_t c, const int32_t* idx,
+                        int64_t m, int32_t k, const float* xyz, const float* new_xyz,
+                        int32_t with_xyz, float* out, void* workspace, size_t workspace_bytes,
+                        void* stream) {
+  int rc = group_args_check(n, c, idx, m, k, workspace);
+  if (rc) return rc;
+  if (m > 0 && (!out || (n > 0 && !feat) || (with_xyz && (!new_xyz || (n > 0 && !xyz)))))
+    return FKNN_ERR_ARG;
+  fknn::GroupArgs g{};
+  g.feat = feat;
+  g.n = n;
+  g.c = c;
+  g.idx = idx;
+  g.m = m;
+  g.k = k;
+  g.xyz = xyz;
+  g.new_xyz = new_xyz;
+  g.with_xyz = with_xyz ? 1 : 0;
+  g.out = out;
+  int launches = 0;
+  rc = fknn::run_group_forward(g, workspace, workspace_bytes, as_stream(stream), &launches);
+  return finish(rc, launches);
+}
+
+int fknn_group_backward(const float* grad_out, int64_t n, int32_t c, const int32_t* idx,
+                        int64_t m, int32_t k, int32_t with_xyz, float* grad_feat,
+                        float* grad_xyz, int32_t accumulate_xyz, float* grad_new_xyz,
+                        int32_t accumulate_new_xyz, void* workspace, size_t workspace_bytes,
+                        void* stream) {
+  int rc = group_args_check(n, c, idx, m, k, workspace);
+  if (rc) return rc;
+  if (m > 0 && !grad_out) return FKNN_ERR_ARG;
+  if (!with_xyz && (grad_xyz || grad_new_xyz)) return FKNN_ERR_ARG;
+  if (grad_xyz && !grad_feat) return FKNN_ERR_ARG;  // both come from the segment pass
+  fknn::GroupArgs g{};
+  g.n = n;
+  g.c = c;
+  g.idx = idx;
+  g.m = m;
+  g.k = k;
+  g.with_xyz = with_xyz ? 1 : 0;
+  g.grad_out = grad_out;
+  g.grad_feat = grad_feat;
+  g.grad_xyz = grad_xyz;
+  g.accumulate_xyz = accumulate_xyz ? 1 : 0;
+  g.grad_new_xyz = grad_new_xyz;
+  g.accumulate_new_xyz = accumulate_new_xyz ? 1 : 0;
+  int launches = 0;
+  rc = fknn::run_group_backward(g, workspace, workspace_bytes, as_stream(stream), &launches);
   return finish(rc, launches);
 }
 

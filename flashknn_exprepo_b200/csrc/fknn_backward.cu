@@ -247,6 +247,17 @@ BwdBufs bwd_layout(void* ws, int64_t m, int64_t n, int k, size_t* bytes) {
 
 }  // namespace
 
+size_t segment_tiles(int64_t n) { return static_cast<size_t>(ceil_div(n > 0 ? n : 1, kScanTile)); }
+
+int launch_segment_starts(const uint32_t* count, int64_t n, uint32_t* tiles, int* total,
+                          uint32_t* start, uint32_t* cursor, cudaStream_t s) {
+  const int t = blocks_for(n, kScanTile);
+  k_bwd_tile_sums<<<t, kScanTile, 0, s>>>(count, n, tiles);
+  k_scan_tiles<<<1, 1024, 0, s>>>(tiles, t, total);
+  k_bwd_starts<<<t, kScanTile, 0, s>>>(count, n, tiles, start, cursor);
+  return 3;
+}
+
 size_t backward_workspace_bytes(int64_t m, int64_t n, int k) {
   size_t bytes = 0;
   bwd_layout(nullptr, m, n, k, &bytes);
@@ -274,11 +285,7 @@ int run_backward(const BackwardArgs& a, void* ws, size_t ws_bytes, cudaStream_t 
     ++nl;
   }
   if (want_p) {
-    const int tiles = blocks_for(a.n, kScanTile);
-    k_bwd_tile_sums<<<tiles, kScanTile, 0, s>>>(b.count, a.n, b.tiles);
-    k_scan_tiles<<<1, 1024, 0, s>>>(b.tiles, tiles, b.total);
-    k_bwd_starts<<<tiles, kScanTile, 0, s>>>(b.count, a.n, b.tiles, b.start, b.cursor);
-    nl += 3;
+    nl += launch_segment_starts(b.count, a.n, b.tiles, b.total, b.start, b.cursor, s);
     if (total > 0) {
       const int64_t sb = ceil_div(total, 256);
       k_bwd_scatter<<<static_cast<int>(sb < 8192 ? sb : 8192), 256, 0, s>>>(

@@ -24,6 +24,14 @@ struct BackwardArgs {
 };
 
 size_t backward_workspace_bytes(int64_t m, int64_t n, int k);
+
+// Counting-sort placement of segments: from count[p] (entries per support
+// point) writes start[p] (first slot), start[n] (total) and cursor[p] (one
+// past the last slot, for a scatter that counts down).  tiles holds
+// segment_tiles(n) words; *total receives the total.  Returns launches.
+size_t segment_tiles(int64_t n);
+int launch_segment_starts(const uint32_t* count, int64_t n, uint32_t* tiles, int* total,
+                          uint32_t* start, uint32_t* cursor, cudaStream_t s);
 int run_backward(const BackwardArgs& a, void* ws, size_t ws_bytes, cudaStream_t s, int* launches);
 
 }  // namespace fknn

@@ -665,7 +665,7 @@ int run_fused(const FusedArgs& f, void* ws, size_t ws_bytes, const QueryShape& s
   const float4* qrec = b.srec;
   int n_qrec = static_cast<int>(n);
   const int2* runs = b.runs;
-  int pad_mode = kPadSelf;
+  int pad_mode = f.pad_minus_one ? kPadMinusOne : kPadSelf;
   const void* pad = nullptr;
   const int32_t* group_start = b.cell_start;
   const int32_t* group_row = nullptr;

@@ -29,6 +29,7 @@ struct FusedArgs {
   int num_down;
   int k;
   float cut_r2;
+  int pad_minus_one;             // self query: pad rows with -1 instead of the own index
   int idx_bits;
   void* idx_out;
   float* dist_out;

@@ -43,6 +43,21 @@ def _config_ptr(config):
 def knn_offsets(xyz, offset, k, voxel, num_down=2, new_xyz=None, new_offset=None,
                 cut_r2=math.inf, config=None, validate=False):
     """Pointcept-style batched grid kNN.  Returns (idx int32 [m,k], dist2 f32 [m,k])."""
+    return _offsets_call("fknn_knn_offsets", xyz, offset, k, voxel, num_down, new_xyz,
+                         new_offset, float(cut_r2), config, validate)
+
+
+def ball_query_offsets(xyz, offset, nsample, max_radius, voxel, num_down=2, new_xyz=None,
+                       new_offset=None, config=None, validate=False):
+    """The nsample nearest points within max_radius among the 27 parent cells
+    (fknn_ball_query).  Returns (idx int32 [m,nsample], dist2 f32), rows
+    padded with (-1, +inf)."""
+    return _offsets_call("fknn_ball_query", xyz, offset, nsample, voxel, num_down, new_xyz,
+                         new_offset, float(max_radius), config, validate)
+
+
+def _offsets_call(entry, xyz, offset, k, voxel, num_down, new_xyz, new_offset, last, config,
+                  validate):
     lib = _lib.load()
     xyz = _require(xyz, "xyz", torch.float32, 2, 3)
     dev = xyz.device
@@ -64,12 +79,12 @@ def knn_offsets(xyz, offset, k, voxel, num_down=2, new_xyz=None, new_offset=None
     nbytes = lib.fknn_workspace_bytes(n, m, max(b, 1), kind)
     ws = _lib.WORKSPACE.get(nbytes, dev)
     _, cfg = _config_ptr(config)
-    rc = lib.fknn_knn_offsets(ptr(xyz), n, ptr(offset), b, ptr(new_xyz), m, ptr(new_offset), k,
-                              float(voxel), num_down, float(cut_r2), ptr(idx), ptr(dist),
-                              ptr(ws), ws.numel(), cfg, stream_handle(dev))
-    check(rc, "fknn_knn_offsets")
+    rc = getattr(lib, entry)(ptr(xyz), n, ptr(offset), b, ptr(new_xyz), m, ptr(new_offset), k,
+                             float(voxel), num_down, last, ptr(idx), ptr(dist), ptr(ws),
+                             ws.numel(), cfg, stream_handle(dev))
+    check(rc, entry)
     if validate:
-        _lib.raise_on_status(ws, "knn_offsets")
+        _lib.raise_on_status(ws, entry)
     return idx, dist
 
 
@@ -143,6 +158,49 @@ def back_query(xyz, sel_indices, query_grid_size, k, batch_idx=None, idx_dtype=t
         _lib.raise_on_status(ws, "back_query")
         empty = bool(_lib.read_status(ws) & _lib.DEVICE_NO_CANDIDATES)
     return idx, dist, empty
+
+
+def group_features(feat, idx, xyz=None, new_xyz=None, with_xyz=False, validate=False):
+    """out [m,k,c(+3)]: rows of feat (and xyz[t] - new_xyz[i] first with
+    with_xyz) gathered by idx; idx < 0 gives zeros (fknn_group_features)."""
+    lib = _lib.load()
+    feat = _require(feat, "feat", torch.float32, 2)
+    dev = feat.device
+    idx = _require(idx, "idx", torch.int32, 2)
+    n, c = feat.shape
+    m, k = idx.shape
+    if with_xyz:
+        xyz = _require(xyz, "xyz", torch.float32, 2, 3)
+        new_xyz = _require(new_xyz, "new_xyz", torch.float32, 2, 3)
+        if xyz.shape[0] != n or new_xyz.shape[0] != m:
+            raise ValueError("xyz must have one row per feature row, new_xyz one per idx row")
+    out = torch.empty((m, k, c + (3 if with_xyz else 0)), dtype=torch.float32, device=dev)
+    ws = _lib.WORKSPACE.get(lib.fknn_group_workspace_bytes(m, k, n), dev)
+    rc = lib.fknn_group_features(ptr(feat), n, c, ptr(idx), m, k,
+                                 ptr(xyz) if with_xyz else None,
+                                 ptr(new_xyz) if with_xyz else None, 1 if with_xyz else 0,
+                                 ptr(out), ptr(ws), ws.numel(), stream_handle(dev))
+    check(rc, "fknn_group_features")
+    if validate:
+        _lib.raise_on_status(ws, "group_features")
+    return out
+
+
+def group_backward(grad_out, idx, n, c, with_xyz=False, grad_feat=None, grad_xyz=None,
+                   accumulate_xyz=False, grad_new_xyz=None, accumulate_new_xyz=False):
+    """Deterministic gradients of group_features (fknn_group_backward)."""
+    lib = _lib.load()
+    grad_out = _require(grad_out, "grad_out", torch.float32, 3)
+    dev = grad_out.device
+    idx = _require(idx, "idx", torch.int32, 2)
+    m, k = idx.shape
+    ws = _lib.WORKSPACE.get(lib.fknn_group_workspace_bytes(m, k, n), dev)
+    rc = lib.fknn_group_backward(ptr(grad_out), n, c, ptr(idx), m, k, 1 if with_xyz else 0,
+                                 ptr(grad_feat), ptr(grad_xyz), 1 if accumulate_xyz else 0,
+                                 ptr(grad_new_xyz), 1 if accumulate_new_xyz else 0, ptr(ws),
+                                 ws.numel(), stream_handle(dev))
+    check(rc, "fknn_group_backward")
+    return grad_feat, grad_xyz, grad_new_xyz
 
 
 def voxel_first(xyz, voxel, batch_idx=None, validate=False):

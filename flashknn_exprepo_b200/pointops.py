@@ -74,3 +74,107 @@ def knn_query(nsample, xyz, offset, new_xyz=None, new_offset=None, *, voxel_size
         raise ValueError("new_offset is required with new_xyz")
     return KNNQuery.apply(int(nsample), xyz, offset, new_xyz, new_offset, float(voxel_size),
                           int(num_down), float(cut_radius) * float(cut_radius))
+
+
+def ball_query(nsample, max_radius, min_radius, xyz, offset, new_xyz=None, new_offset=None, *,
+               voxel_size=None, num_down=2):
+    """Pointcept's ``pointops.ball_query`` calling convention
+    (Pointcept/libs/pointops/functions/query.py:73-108) on the grid: the
+    nsample nearest points with squared distance below max_radius^2, rows
+    ascending, padding (-1, 1e10) before the square root, and returns
+    (idx int32 [m, nsample], distance f32 [m, nsample]).
+
+    The default voxel makes a parent cell max_radius wide, so the 27 parent
+    cells hold the whole ball and the rows are exact.  Differences from
+    Pointcept's brute-force kernel: a ball with more than nsample points
+    yields its nsample nearest (Pointcept: a strided subset of them), and
+    min_radius must be 0.
+    """
+    if min_radius != 0:
+        raise ValueError("min_radius > 0 is not supported by the grid ball query")
+    if not max_radius > 0:
+        raise ValueError("max_radius must be positive")
+    if voxel_size is None:
+        voxel_size = float(max_radius) / (1 << num_down)
+    if new_xyz is None or new_offset is None:
+        new_xyz, new_offset = None, None
+    idx, dist2 = ops.ball_query_offsets(xyz, offset, int(nsample), float(max_radius),
+                                        float(voxel_size), int(num_down), new_xyz, new_offset)
+    dist2 = torch.where(idx < 0, torch.full_like(dist2, 1e10), dist2)
+    return idx, torch.sqrt(dist2)
+
+
+class Grouping(torch.autograd.Function):
+    """Gather of neighbour rows with a deterministic hand-written backward
+    (Pointcept/libs/pointops/functions/grouping.py:36-60 semantics)."""
+
+    @staticmethod
+    def forward(ctx, idx, feat, xyz, new_xyz, with_xyz):
+        idx = idx.to(torch.int32).contiguous()
+        out = ops.group_features(feat.float(), idx, xyz, new_xyz, with_xyz)
+        ctx.with_xyz = with_xyz
+        ctx.self_query = with_xyz and new_xyz is xyz
+        ctx.shape = (feat.shape[0], feat.shape[1])
+        ctx.save_for_backward(idx)
+        return out
+
+    @staticmethod
+    def backward(ctx, grad_out):
+        (idx,) = ctx.saved_tensors
+        n, c = ctx.shape
+        grad_out = grad_out.contiguous().float()
+        dev = grad_out.device
+        need_feat, need_xyz, need_new = ctx.needs_input_grad[1:4]
+        if not ctx.with_xyz:
+            need_xyz = need_new = False
+        grad_feat = torch.empty((n, c), dtype=torch.float32, device=dev)
+        grad_xyz = grad_new = None
+        if ctx.self_query and (need_xyz or need_new):
+            grad_xyz = torch.empty((n, 3), dtype=torch.float32, device=dev)
+            ops.group_backward(grad_out, idx, n, c, True, grad_feat, grad_xyz, False, grad_xyz,
+                               True)
+            return None, grad_feat if need_feat else None, grad_xyz, None, None
+        if need_xyz:
+            grad_xyz = torch.empty((n, 3), dtype=torch.float32, device=dev)
+        if need_new:
+            grad_new = torch.empty((idx.shape[0], 3), dtype=torch.float32, device=dev)
+        ops.group_backward(grad_out, idx, n, c, ctx.with_xyz, grad_feat, grad_xyz, False,
+                           grad_new, False)
+        return None, grad_feat if need_feat else None, grad_xyz, grad_new, None
+
+
+def grouping(idx, feat, xyz, new_xyz=None, with_xyz=False):
+    """Pointcept's ``pointops.grouping(idx, feat, xyz, new_xyz, with_xyz)``:
+    (m, nsample, c) or, with ``with_xyz``, (m, nsample, 3 + c) whose first
+    three channels are the neighbour's offset from the query; idx -1 rows are
+    zero."""
+    if new_xyz is None:
+        new_xyz = xyz
+    return Grouping.apply(idx, feat, xyz, new_xyz, bool(with_xyz))
+
+
+def knn_query_and_group(feat, xyz, offset=None, new_xyz=None, new_offset=None, idx=None,
+                        nsample=None, with_xyz=False, *, voxel_size=None, num_down=2):
+    """Pointcept's ``pointops.knn_query_and_group``
+    (Pointcept/libs/pointops/functions/utils.py:5-18): the grid kNN
+    (``knn_query``) unless ``idx`` is given, then ``grouping``.  Returns
+    (grouped features, idx)."""
+    if idx is None:
+        if nsample is None:
+            raise ValueError("nsample is required when idx is not given")
+        idx, _ = knn_query(nsample, xyz, offset, new_xyz, new_offset, voxel_size=voxel_size,
+                           num_down=num_down)
+    return grouping(idx, feat, xyz, new_xyz, with_xyz), idx
+
+
+def ball_query_and_group(feat, xyz, offset=None, new_xyz=None, new_offset=None, idx=None,
+                         max_radio=None, min_radio=0, nsample=None, with_xyz=False, *,
+                         voxel_size=None, num_down=2):
+    """Pointcept's ``pointops.ball_query_and_group`` (utils.py:21-39) on the
+    grid ball query."""
+    if idx is None:
+        if nsample is None or max_radio is None:
+            raise ValueError("nsample and max_radio are required when idx is not given")
+        idx, _ = ball_query(nsample, max_radio, min_radio, xyz, offset, new_xyz, new_offset,
+                            voxel_size=voxel_size, num_down=num_down)
+    return grouping(idx, feat, xyz, new_xyz, with_xyz), idx

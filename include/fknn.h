@@ -107,6 +107,23 @@ FKNN_API int fknn_knn_offsets(const float* xyz, int64_t n, const int64_t* offset
                      float* dist_out, void* workspace, size_t workspace_bytes,
                      const fknn_config* config, void* stream);
 
+/* Radius-limited grid query, the cut-radius variant of the reference query
+ * (FlashKnnWrapper.py:172,370: a candidate counts only when d < cut_r^2)
+ * with the calling convention of Pointcept's ball query
+ * (Pointcept/libs/pointops/functions/query.py:73-108): the nsample nearest
+ * points with squared distance < max_radius^2 among the 27 parent cells,
+ * ascending; rows with fewer are padded with (-1, +inf), also for the self
+ * query.  When voxel * 2^num_down >= max_radius the 27 cells hold the whole
+ * ball and the rows are exact.  (Pointcept's brute-force kernel returns a
+ * strided subset when the ball holds more than nsample points; this returns
+ * the nearest ones.)  Arguments as fknn_knn_offsets; workspace from
+ * fknn_workspace_bytes with the same kind. */
+FKNN_API int fknn_ball_query(const float* xyz, int64_t n, const int64_t* offsets, int64_t n_clouds,
+                    const float* new_xyz, int64_t m, const int64_t* new_offsets, int32_t nsample,
+                    float voxel, int32_t num_down, float max_radius, int32_t* idx_out,
+                    float* dist_out, void* workspace, size_t workspace_bytes,
+                    const fknn_config* config, void* stream);
+
 /* FlashKNN.query (FlashKNN/functions/FlashKnnWrapper.py:165-449) when
  * query_indices == NULL, FlashKNN.selected_query (:646-849) otherwise.
  * grid_coord int64 [n,3], batch_idx int64 [n] (NULL = one cloud), xyz f32
@@ -146,6 +163,31 @@ FKNN_API size_t fknn_voxel_first_workspace_bytes(int64_t n);
 FKNN_API int fknn_voxel_first(const float* xyz, int64_t n, const int64_t* batch_idx, float voxel,
                      int64_t* out, int64_t* count_out, void* workspace, size_t workspace_bytes,
                      void* stream);
+
+/* Neighbour feature grouping, Pointcept's pointops.grouping
+ * (Pointcept/libs/pointops/functions/grouping.py:36-60) as used by
+ * knn_query_and_group (.../functions/utils.py:5-18): out [m,k,c'] with
+ * out[i,j] = [xyz[t] - new_xyz[i] | feat[t]] for t = idx[i,j] (the xyz part,
+ * 3 channels, only when with_xyz != 0; c' = c or c + 3); an index below 0 is
+ * padding and gives a zero row.  feat f32 [n,c], idx int32 [m,k], xyz f32
+ * [n,3] and new_xyz f32 [m,3] (with_xyz only).  Requires m*k < 2^31. */
+FKNN_API size_t fknn_group_workspace_bytes(int64_t m, int32_t k, int64_t n);
+FKNN_API int fknn_group_features(const float* feat, int64_t n, int32_t c, const int32_t* idx,
+                        int64_t m, int32_t k, const float* xyz, const float* new_xyz,
+                        int32_t with_xyz, float* out, void* workspace, size_t workspace_bytes,
+                        void* stream);
+/* Gradients of fknn_group_features for grad_out f32 [m,k,c']: grad_feat
+ * [n,c] (overwritten), grad_xyz [n,3] (with_xyz; added to when
+ * accumulate_xyz != 0) and grad_new_xyz [m,3] (with_xyz; added to when
+ * accumulate_new_xyz != 0; written after grad_xyz, so one buffer may serve
+ * both for a self query).  Every point's sum runs over its entries in
+ * ascending i*k+j order: the result is bitwise reproducible (the reference
+ * op accumulates with atomics).  Any output may be NULL. */
+FKNN_API int fknn_group_backward(const float* grad_out, int64_t n, int32_t c, const int32_t* idx,
+                        int64_t m, int32_t k, int32_t with_xyz, float* grad_feat,
+                        float* grad_xyz, int32_t accumulate_xyz, float* grad_new_xyz,
+                        int32_t accumulate_new_xyz, void* workspace, size_t workspace_bytes,
+                        void* stream);
 
 /* AdaptiveNeighborhoodFlashKNN.query (FlashKNN/functions/adaptive_octree.py
  * :505-612): every point takes its exact top-K over the 27 same-level nodes

@@ -301,3 +301,49 @@ def test_oracle_hierarchy_matches_reference_builder(case):
     assert len(outs) == int(z["n_outputs"])
     for i, o in enumerate(outs):
         assert np.array_equal(o, z[f"ref_{i}"]), i
+
+
+def grouping_cases():
+    return sorted(f[len("grouping_"):-4] for f in os.listdir(GOLDEN)
+                  if f.startswith("grouping_") and f.endswith(".npz"))
+
+
+def grouping_f64(z):
+    """Restatement of pointops.grouping and its gradients in FP64 (numpy)."""
+    idx, feat, xyz = z["idx"], z["feat"].astype(np.float64), z["xyz"].astype(np.float64)
+    new = z["new_xyz"].astype(np.float64)
+    valid = idx >= 0
+    t = np.where(valid, idx, 0)
+    out = np.where(valid[..., None], feat[t], 0.0)
+    g = z["grad_out"].astype(np.float64)
+    grads = {}
+    if bool(z["with_xyz"]):
+        rel = np.where(valid[..., None], xyz[t] - new[:, None, :], 0.0)
+        out = np.concatenate([rel, out], -1)
+        gx = np.zeros_like(xyz)
+        np.add.at(gx, t[valid], g[..., :3][valid])
+        gn = -(g[..., :3] * valid[..., None]).sum(1)
+        if bool(z["separate"]):
+            grads["xyz"], grads["new_xyz"] = gx, gn
+        else:
+            grads["xyz"] = gx + gn
+        g = g[..., 3:]
+    gf = np.zeros_like(feat)
+    np.add.at(gf, t[valid], g[valid])
+    grads["feat"] = gf
+    return out, grads
+
+
+@pytest.mark.parametrize("case", grouping_cases())
+def test_grouping_restatement_matches_pointcept(case):
+    """The grouping semantics (zero rows for idx -1, neighbour offsets first
+    with with_xyz) and gradients against Pointcept's own grouping run with
+    torch autograd (tests/golden/make_golden_grouping.py)."""
+    z = np.load(os.path.join(GOLDEN, f"grouping_{case}.npz"))
+    out, grads = grouping_f64(z)
+    assert np.array_equal(out.astype(np.float32), z["ref_out"])
+    assert np.allclose(grads["feat"], z["ref_grad_feat"], rtol=1e-5, atol=1e-5)
+    if "ref_grad_xyz" in z:
+        assert np.allclose(grads["xyz"], z["ref_grad_xyz"], rtol=1e-5, atol=1e-5)
+    if "ref_grad_new_xyz" in z:
+        assert np.allclose(grads["new_xyz"], z["ref_grad_new_xyz"], rtol=1e-5, atol=1e-5)
