@@ -50,6 +50,10 @@ def parse_args():
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the per-cloud, fwd+bwd and CPU-baseline legs")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer e2e leg")
+    ap.add_argument("--rows-only", action="store_true",
+                    help="only the per-path rows and one distance backward (profiling)")
+    ap.add_argument("--no-tune", action="store_true",
+                    help="default launch shape instead of the autotuned one")
     ap.add_argument("--clouds", type=int, default=16,
                     help="use the first N clouds of the batch (small cases for profiling)")
     return ap.parse_args()
@@ -232,17 +236,22 @@ def run_ours(args, rank, world, local_rank, dist):
     lib = _lib.load()
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
 
+    # --- launch shape picked by the autotuner on this workload (untimed)
+    from flashknn_exprepo_b200 import autotune
+    cfg = None if args.no_tune else autotune.tune_offsets(xyz, off, k, voxel, 2)
+    tuned = autotune.last_results() if cfg is not None else {}
+
     # --- capture the batched pipeline in a CUDA graph
     stream = torch.cuda.Stream(dev)
     stream.wait_stream(torch.cuda.current_stream(dev))
     with torch.cuda.stream(stream):
-        fk.ops.knn_offsets(xyz, off, k, voxel, 2)  # workspace sized, kernels loaded
+        fk.ops.knn_offsets(xyz, off, k, voxel, 2, config=cfg)  # workspace sized, kernels loaded
         torch.cuda.synchronize(dev)
         launches_per_step = fk.ops.last_launch_count()
         lib.fknn_profile_enable(1)
         graph = torch.cuda.CUDAGraph()
         with torch.cuda.graph(graph, stream=stream):
-            idx_g, dist_g = fk.ops.knn_offsets(xyz, off, k, voxel, 2)
+            idx_g, dist_g = fk.ops.knn_offsets(xyz, off, k, voxel, 2, config=cfg)
     torch.cuda.current_stream(dev).wait_stream(stream)
     torch.cuda.synchronize(dev)
 
@@ -281,12 +290,16 @@ def run_ours(args, rank, world, local_rank, dist):
     value = total_queries * args.steps / (total_ms / 1e3)
 
     # parity of the timed graph against a fresh eager call
-    ei, ed = fk.ops.knn_offsets(xyz, off, k, voxel, 2, validate=True)
+    ei, ed = fk.ops.knn_offsets(xyz, off, k, voxel, 2, config=cfg, validate=True)
     graph_matches = bool(torch.equal(ei, idx_g) and torch.equal(ed, dist_g))
 
     out = {"value": value, "ms_per_step": total_ms / args.steps, "n_points": total_queries,
            "clocks": clocks.summary(), "kernel_ms": kern_ms, "launches_per_step": launches_per_step,
-           "graph_matches_eager": graph_matches, "local_n": n}
+           "graph_matches_eager": graph_matches, "local_n": n,
+           "launch_shape": None if cfg is None else {
+               "warps_per_cta": cfg.warps_per_cta, "tile_records": cfg.tile_records,
+               "min_candidates_per_lane": cfg.min_candidates_per_lane,
+               "tuned": next(iter(tuned.values()), None)}}
     del graph
 
     if args.no_e2e:
@@ -416,7 +429,125 @@ def extras_single_gpu(args, fk, torch, dev, batch, voxel, flush):
         ms.append(e0.elapsed_time(e1))
     res["backward_ms"] = sum(ms) / reps
     res["recall"] = fp64_recall(batch, idx.cpu().numpy(), k)
+    res["rows"] = rows_single_gpu(fk, torch, dev, flush, measured_peak_hbm()[0])
     return res
+
+
+def _event_ms(torch, fn, flush, reps=5):
+    """Mean device ms of fn over reps, L2 flushed before each, after 2 warm-ups."""
+    for _ in range(2):
+        fn()
+    torch.cuda.synchronize()
+    total = 0.0
+    for _ in range(reps):
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        fn()
+        e1.record()
+        e1.synchronize()
+        total += e0.elapsed_time(e1)
+    return total / reps
+
+
+def rows_single_gpu(fk, torch, dev, flush, peak_gbs):
+    """The paths around the batched query, each on its own workload:
+    adaptive-neighbourhood query (LiDAR scan), back query and voxel-first
+    subsampling (16-cloud batch), the DeLA hierarchy builder (LiDAR scan),
+    radius-limited query (room) and neighbour feature grouping (16-cloud
+    batch, 64 channels, forward with its HBM roofline, and backward)."""
+    from flashknn_exprepo_b200 import hierarchy, synthetic
+    T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)  # noqa: E731
+    rows = {}
+    # adaptive neighbourhood, LiDAR scan ~118k points, K=16
+    lidar = synthetic.lidar()
+    grid = T(np.floor(lidar / np.float32(synthetic.C3_VOXEL)).astype(np.int64))
+    lx = T(lidar)
+    eager = _event_ms(torch, lambda: fk.ops.adaptive_query(grid, None, 16, xyz=lx), flush)
+    stream = torch.cuda.Stream(dev)
+    stream.wait_stream(torch.cuda.current_stream(dev))
+    with torch.cuda.stream(stream):
+        fk.ops.adaptive_query(grid, None, 16, xyz=lx)   # workspace sized on this stream
+        torch.cuda.synchronize(dev)
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph, stream=stream):
+            fk.ops.adaptive_query(grid, None, 16, xyz=lx)
+    torch.cuda.current_stream(dev).wait_stream(stream)
+    torch.cuda.synchronize(dev)
+    ms = _event_ms(torch, graph.replay, flush)
+    del graph
+    rows["adaptive_lidar_k16"] = {"value": len(lidar) / (ms * 1e-3), "unit": "queries/s",
+                                  "ms": ms, "eager_ms": eager, "n_points": len(lidar),
+                                  "step": "CUDA-graph replay of the whole adaptive pipeline"}
+    # back query K=1 and voxel-first subsampling, 16-cloud batch
+    b = synthetic.uneven_batch()
+    bx = T(b.xyz)
+    bb = T(np.repeat(np.arange(len(b.counts)), b.counts).astype(np.int64))
+    ms = _event_ms(torch, lambda: fk.ops.voxel_first(bx, 0.1, bb), flush)
+    rows["voxel_first_batch"] = {"value": len(b.xyz) / (ms * 1e-3), "unit": "points/s",
+                                 "ms": ms, "voxel_m": 0.1}
+    sel = fk.ops.voxel_first(bx, 0.1, bb)
+    ms = _event_ms(torch, lambda: fk.ops.back_query(bx, sel, 0.2, 1, bb), flush)
+    rows["back_query_batch_k1"] = {"value": len(b.xyz) / (ms * 1e-3), "unit": "queries/s",
+                                   "ms": ms, "subset_points": int(sel.numel()),
+                                   "query_grid_m": 0.2}
+    # DeLA hierarchy (4 levels, K=24, alpha 16) on the voxel-first LiDAR scan
+    lid = T(synthetic.lidar(dedup=True))
+    hierarchy.build_flash_hierarchy(lid)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(3):
+        hierarchy.build_flash_hierarchy(lid)
+    torch.cuda.synchronize()
+    rows["hierarchy_lidar"] = {"value": (time.perf_counter() - t0) / 3 * 1e3, "unit": "ms",
+                               "n_points": int(lid.shape[0]),
+                               "what": "wall clock incl. one count read-back per level"}
+    # radius-limited query, room ~80k points, K=32, r=0.1 m
+    room = T(synthetic.room())
+    ro = torch.tensor([room.shape[0]], device=dev)
+    ms = _event_ms(torch, lambda: fk.ops.ball_query_offsets(room, ro, 32, 0.1, 0.025, 2), flush)
+    rows["ball_query_room_k32"] = {"value": room.shape[0] / (ms * 1e-3), "unit": "queries/s",
+                                   "ms": ms, "radius_m": 0.1}
+    # grouping: 16-cloud batch, K=16, 64 channels
+    off = T(b.offsets)
+    idx, _ = fk.ops.knn_offsets(bx, off, 16, synthetic.C4_VOXEL, 2)
+    feat = torch.randn((len(b.xyz), 64), device=dev)
+    ms = _event_ms(torch, lambda: fk.ops.group_features(feat, idx), flush)
+    m, c = idx.numel(), 64
+    algo = m * c * 4 + m * 4 + len(b.xyz) * c * 4
+    rows["grouping_batch_c64_fwd"] = {
+        "value": algo / (ms * 1e-3) / 1e9, "unit": "GB/s", "ms": ms,
+        "roofline": {"bound": "hbm", "achieved": algo / (ms * 1e-3) / 1e9, "peak": peak_gbs,
+                     "frac": algo / (ms * 1e-3) / 1e9 / peak_gbs,
+                     "algorithmic_bytes": algo}}
+    g = torch.randn((idx.shape[0], 16, 64), device=dev)
+    gf = torch.empty_like(feat)
+    ms = _event_ms(torch, lambda: fk.ops.group_backward(g, idx, len(b.xyz), 64, False, gf), flush)
+    rows["grouping_batch_c64_bwd"] = {"value": ms, "unit": "ms"}
+    return rows
+
+
+def rows_only(args):
+    """One distance backward on the 16-cloud batch and the per-path rows."""
+    import torch
+
+    import flashknn_exprepo_b200 as fk
+    from flashknn_exprepo_b200 import synthetic
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
+    b = synthetic.uneven_batch()
+    x = torch.from_numpy(b.xyz).to(dev)
+    off = torch.from_numpy(b.offsets).to(dev)
+    idx, d = fk.ops.knn_offsets(x, off, args.k, synthetic.C4_VOXEL, 2)
+    g = torch.from_numpy(synthetic.backward_weights(len(b.xyz), args.k)).to(dev)
+    g = g * torch.isfinite(d).to(g.dtype)
+    grad = torch.zeros_like(x)
+    ms = _event_ms(torch, lambda: fk.ops.backward(x, x, idx, d, g, grad_q=grad, grad_p=grad,
+                                                  accumulate=True), flush)
+    return {"backward_ms": ms, "rows": rows_single_gpu(fk, torch, dev, flush,
+                                                       measured_peak_hbm()[0])}
 
 
 def fp64_recall(batch, idx, k, per_cloud=256):
@@ -542,6 +673,10 @@ def main():
         print(json.dumps(run_reference(args)))
         return
 
+    if args.rows_only:
+        print(json.dumps(rows_only(args)))
+        return
+
     dist = None
     if world > 1:
         import datetime
@@ -588,6 +723,7 @@ def main():
         "e2e": out["e2e"], "gpu_launches": out["launches_per_step"] * args.steps,
         "clocks": out["clocks"], "roofline": roofline,
         "graph_matches_eager": out["graph_matches_eager"],
+        "launch_shape": out["launch_shape"],
     }
     if "per_cloud" in out:
         line["per_cloud"] = out["per_cloud"]
@@ -600,6 +736,8 @@ def main():
                              "backward": out.get("backward_ms")}
     if "recall" in out:
         line["recall"] = out["recall"]
+    if "rows" in out:
+        line["rows"] = out["rows"]
     if world == 1 and not args.no_extras:
         from flashknn_exprepo_b200 import synthetic
         b = synthetic.uneven_batch()

@@ -5,9 +5,10 @@
 //
 // Forward: out[i, j, :] = [xyz[t] - new_xyz[i] | feat[t]] for t = idx[i, j]
 // (the xyz part only with with_xyz); an index below 0 is padding and gives a
-// zero row.  One warp per output row, lanes along the channels (float4 when
-// the row allows it): a bandwidth-bound copy whose only re-read is the
-// gathered feature row, served from L2 for the rows that neighbours share.
+// zero row.  Threads run flat over the output words (float4 when the rows
+// allow it), so every warp stores one contiguous run: a bandwidth-bound copy
+// whose only re-read is the gathered feature row, served from L2 for the
+// rows that neighbours share.
 //
 // Backward: grad_feat[t] = sum of grad_out[i, j, feat part] over the entries
 // with idx[i, j] = t, grad_xyz[t] the same over the xyz part and
@@ -42,34 +43,48 @@ __device__ __forceinline__ bool entry_ok(int32_t t, int64_t n, int* status) {
 
 // ------------------------------------------------------------------ forward
 
+// Flat over the output: thread t writes output word t (float4 words when
+// every row is a whole number of aligned float4s, else single floats), so a
+// warp's stores are one contiguous run whatever the channel count.  Stores
+// stream past L2 (st.global.cs): the output is written once and not re-read
+// here.
 __global__ void __launch_bounds__(256)
     kg_forward(const float* __restrict__ feat, int64_t n, int c, const int32_t* __restrict__ idx,
                int64_t rows, int k, const float* __restrict__ xyz,
                const float* __restrict__ new_xyz, int with_xyz, int vec4,
                float* __restrict__ out, int* status) {
-  const int lane = threadIdx.x & 31;
-  const int cw = c + (with_xyz ? 3 : 0);
-  const int64_t warps = static_cast<int64_t>(gridDim.x) * (blockDim.x >> 5);
-  for (int64_t r = static_cast<int64_t>(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5);
-       r < rows; r += warps) {
+  const int off = with_xyz ? 3 : 0;
+  const int cw = c + off;
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  if (vec4) {  // with_xyz == 0, c % 4 == 0
+    const int q4 = c >> 2;
+    const int64_t words = rows * q4;
+    for (int64_t w = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; w < words;
+         w += stride) {
+      const int64_t r = w / q4;
+      const int q = static_cast<int>(w - r * q4);
+      const int32_t t = idx[r];
+      float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (entry_ok(t, n, q == 0 ? status : nullptr))
+        v = __ldg(reinterpret_cast<const float4*>(feat + static_cast<int64_t>(t) * c) + q);
+      __stcs(reinterpret_cast<float4*>(out) + w, v);
+    }
+    return;
+  }
+  const int64_t words = rows * cw;
+  for (int64_t w = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; w < words;
+       w += stride) {
+    const int64_t r = w / cw;
+    const int col = static_cast<int>(w - r * cw);
     const int32_t t = idx[r];
-    const bool ok = entry_ok(t, n, status);
-    float* o = out + r * cw;
-    if (with_xyz && lane < 3) {
-      const int64_t i = r / k;
-      o[lane] = ok ? __fsub_rn(xyz[3 * static_cast<int64_t>(t) + lane], new_xyz[3 * i + lane])
-                   : 0.f;
+    float v = 0.f;
+    if (entry_ok(t, n, col == 0 ? status : nullptr)) {
+      if (col < off)
+        v = __fsub_rn(xyz[3 * static_cast<int64_t>(t) + col], new_xyz[3 * (r / k) + col]);
+      else
+        v = __ldg(feat + static_cast<int64_t>(t) * c + (col - off));
     }
-    float* of = o + (with_xyz ? 3 : 0);
-    const float* src = feat + static_cast<int64_t>(ok ? t : 0) * c;
-    if (vec4) {
-      const float4* s4 = reinterpret_cast<const float4*>(src);
-      float4* d4 = reinterpret_cast<float4*>(of);
-      for (int q = lane; q < (c >> 2); q += 32)
-        d4[q] = ok ? s4[q] : make_float4(0.f, 0.f, 0.f, 0.f);
-    } else {
-      for (int q = lane; q < c; q += 32) of[q] = ok ? src[q] : 0.f;
-    }
+    __stcs(out + w, v);
   }
 }
 
@@ -113,14 +128,34 @@ __device__ __forceinline__ uint32_t warp_sort_u32(uint32_t v) {
   return v;
 }
 
+template <int V>
+struct Vec;
+template <>
+struct Vec<1> {
+  using T = float;
+  __device__ static T zero() { return 0.f; }
+  __device__ static T add(T a, T b) { return __fadd_rn(a, b); }
+};
+template <>
+struct Vec<2> {
+  using T = float2;
+  __device__ static T zero() { return make_float2(0.f, 0.f); }
+  __device__ static T add(T a, T b) { return make_float2(__fadd_rn(a.x, b.x), __fadd_rn(a.y, b.y)); }
+};
+
 // One warp per support point: its entries in ascending order, each row of
-// grad_out added channel by channel in that order.
+// grad_out added channel by channel in that order.  V channels per lane (2
+// when the rows are whole float2s); the rows of four entries are loaded
+// before they are added, in order, so loads overlap.
+template <int V>
 __global__ void __launch_bounds__(256)
     kg_support(const float* __restrict__ grad_out, int c, int with_xyz,
                const uint32_t* __restrict__ start, const uint32_t* __restrict__ seg, int64_t n,
                float* __restrict__ grad_feat, float* __restrict__ grad_xyz, int accumulate_xyz) {
+  using VT = typename Vec<V>::T;
   const int lane = threadIdx.x & 31;
-  const int cw = c + (with_xyz ? 3 : 0);
+  const int off = with_xyz ? 3 : 0;
+  const int cw = c + off;
   const int64_t warps = static_cast<int64_t>(gridDim.x) * (blockDim.x >> 5);
   for (int64_t p = static_cast<int64_t>(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5);
        p < n; p += warps) {
@@ -129,13 +164,26 @@ __global__ void __launch_bounds__(256)
     // walked by repeated selection of the next larger entry.
     uint32_t mine = kNoEntry;
     if (len <= 32) mine = warp_sort_u32(lane < static_cast<int>(len) ? seg[s + lane] : kNoEntry);
-    for (int c0 = 0; c0 < cw; c0 += 32) {
-      const int col = c0 + lane;
-      float acc = 0.f;
+    for (int c0 = 0; c0 < cw; c0 += 32 * V) {
+      const int col = c0 + lane * V;
+      const bool live = col < cw;
+      auto row = [&](uint32_t e) {
+        return *reinterpret_cast<const VT*>(grad_out + static_cast<int64_t>(e) * cw + col);
+      };
+      VT acc = Vec<V>::zero();
       if (len <= 32) {
-        for (uint32_t r = 0; r < len; ++r) {
+        uint32_t r = 0;
+        for (; r + 4 <= len; r += 4) {
+          const uint32_t e0 = __shfl_sync(kFull, mine, r), e1 = __shfl_sync(kFull, mine, r + 1);
+          const uint32_t e2 = __shfl_sync(kFull, mine, r + 2), e3 = __shfl_sync(kFull, mine, r + 3);
+          if (live) {
+            const VT v0 = row(e0), v1 = row(e1), v2 = row(e2), v3 = row(e3);
+            acc = Vec<V>::add(Vec<V>::add(Vec<V>::add(Vec<V>::add(acc, v0), v1), v2), v3);
+          }
+        }
+        for (; r < len; ++r) {
           const uint32_t e = __shfl_sync(kFull, mine, r);
-          if (col < cw) acc = __fadd_rn(acc, grad_out[static_cast<int64_t>(e) * cw + col]);
+          if (live) acc = Vec<V>::add(acc, row(e));
         }
       } else {
         uint32_t last = 0;
@@ -146,19 +194,22 @@ __global__ void __launch_bounds__(256)
             if ((r == 0 || v > last) && v < best) best = v;
           }
           best = __reduce_min_sync(kFull, best);
-          if (col < cw) acc = __fadd_rn(acc, grad_out[static_cast<int64_t>(best) * cw + col]);
+          if (live) acc = Vec<V>::add(acc, row(best));
           last = best;
         }
       }
-      if (col < cw) {
-        if (with_xyz && col < 3) {
+      if (!live) continue;
+      if constexpr (V == 1) {
+        if (col < off) {
           if (grad_xyz) {
             float* g = grad_xyz + 3 * p + col;
             *g = accumulate_xyz ? __fadd_rn(*g, acc) : acc;
           }
         } else {
-          grad_feat[p * c + (col - (with_xyz ? 3 : 0))] = acc;
+          grad_feat[p * c + (col - off)] = acc;
         }
+      } else {  // no xyz part: channel col of the row is channel col of feat
+        *reinterpret_cast<VT*>(grad_feat + p * c + col) = acc;
       }
     }
   }
@@ -210,6 +261,11 @@ GBufs glayout(void* ws, int64_t rows, int64_t n, size_t* bytes) {
   return b;
 }
 
+inline int capped_blocks(int64_t threads) {
+  const int64_t b = ceil_div(threads > 0 ? threads : 1, 256);
+  return static_cast<int>(b < 148 * 32 ? b : 148 * 32);
+}
+
 inline int capped_warp_blocks(int64_t rows) {
   const int64_t b = ceil_div(rows > 0 ? rows : 1, 8);  // 8 warps per 256-thread block
   return static_cast<int>(b < 148 * 16 ? b : 148 * 16);
@@ -240,8 +296,8 @@ int run_group_forward(const GroupArgs& g, void* ws, size_t ws_bytes, cudaStream_
     const bool vec4 = !g.with_xyz && g.c % 4 == 0 &&
                       reinterpret_cast<uintptr_t>(g.feat) % 16 == 0 &&
                       reinterpret_cast<uintptr_t>(g.out) % 16 == 0;
-    (void)cw;
-    kg_forward<<<capped_warp_blocks(rows), 256, 0, s>>>(g.feat, g.n, g.c, g.idx, rows, g.k, g.xyz,
+    const int64_t words = vec4 ? rows * (g.c / 4) : rows * cw;
+    kg_forward<<<capped_blocks(words), 256, 0, s>>>(g.feat, g.n, g.c, g.idx, rows, g.k, g.xyz,
                                                         g.new_xyz, g.with_xyz, vec4 ? 1 : 0,
                                                         g.out, &b.meta->status);
     ++nl;
@@ -280,9 +336,16 @@ int run_group_backward(const GroupArgs& g, void* ws, size_t ws_bytes, cudaStream
       kg_scatter<<<eblocks, 256, 0, s>>>(g.idx, rows, g.n, b.cursor, b.seg);
       ++nl;
     }
-    kg_support<<<capped_warp_blocks(g.n), 256, 0, s>>>(g.grad_out, g.c, g.with_xyz, b.start,
-                                                       b.seg, g.n, g.grad_feat, g.grad_xyz,
-                                                       g.accumulate_xyz);
+    const bool v2 = !g.with_xyz && g.c % 2 == 0 &&
+                    reinterpret_cast<uintptr_t>(g.grad_out) % 8 == 0 &&
+                    reinterpret_cast<uintptr_t>(g.grad_feat) % 8 == 0;
+    if (v2)
+      kg_support<2><<<capped_warp_blocks(g.n), 256, 0, s>>>(g.grad_out, g.c, 0, b.start, b.seg,
+                                                            g.n, g.grad_feat, nullptr, 0);
+    else
+      kg_support<1><<<capped_warp_blocks(g.n), 256, 0, s>>>(g.grad_out, g.c, g.with_xyz, b.start,
+                                                            b.seg, g.n, g.grad_feat, g.grad_xyz,
+                                                            g.accumulate_xyz);
     ++nl;
   }
   if (g.with_xyz && g.grad_new_xyz && g.m > 0) {

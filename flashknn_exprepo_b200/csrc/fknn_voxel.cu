@@ -55,11 +55,21 @@ __global__ void __launch_bounds__(256)
     keys[i] = key;
     vals[i] = static_cast<uint32_t>(i);
   }
+  // OR over the block first: one pair of global atomics per block, not per
+  // warp (all of them hit the same two words)
+  __shared__ uint32_t s_or[2][8];
   const uint32_t lo = __reduce_or_sync(kFull, static_cast<uint32_t>(key));
   const uint32_t hi = __reduce_or_sync(kFull, static_cast<uint32_t>(key >> 32));
+  const int warp = threadIdx.x >> 5;
   if ((threadIdx.x & 31) == 0) {
-    if (lo) atomicOr(bits_or, lo);
-    if (hi) atomicOr(bits_or + 1, hi);
+    s_or[0][warp] = lo;
+    s_or[1][warp] = hi;
+  }
+  __syncthreads();
+  if (threadIdx.x < 2) {
+    uint32_t v = 0;
+    for (int w = 0; w < static_cast<int>(blockDim.x >> 5); ++w) v |= s_or[threadIdx.x][w];
+    if (v) atomicOr(bits_or + threadIdx.x, v);
   }
 }
 

@@ -56,8 +56,10 @@ extern "C" {
 
 /* Optional launch shape of the query kernel; NULL selects the defaults.
  * warps_per_cta in {1,2,4,8}; tile_records (candidate records staged per
- * warp) a multiple of 32 in [64, 4096]; min_candidates_per_lane >= 1 caps
- * how many lanes share one query; ctas_per_sm 0 = occupancy maximum. */
+ * warp) a multiple of 32 in [64, 1024] whose shared memory fits a CTA;
+ * min_candidates_per_lane >= 1 caps how many lanes share one query;
+ * ctas_per_sm 0 = occupancy maximum.  flashknn_exprepo_b200/autotune.py
+ * picks these per K and point density by timing them. */
 typedef struct fknn_config {
   int32_t warps_per_cta;
   int32_t tile_records;

@@ -42,3 +42,16 @@ def test_synthetic_generators_are_seeded():
     counts, seed = S.draw_counts()
     assert len(counts) == 16 and abs(counts.sum() - 1.5e6) <= 0.03 * 1.5e6
     assert counts.min() >= 20000 and counts.max() <= 200000
+
+
+def test_autotune_buckets_and_cache_file(tmp_path, monkeypatch):
+    from flashknn_exprepo_b200 import autotune
+    assert [autotune.k_bucket(k) for k in (1, 2, 3, 16, 17, 33, 64)] == [1, 2, 4, 16, 32, 64, 64]
+    path = tmp_path / "cache.json"
+    monkeypatch.setenv("FKNN_TUNE_CACHE", str(path))
+    autotune._cache.clear()
+    autotune._cache["GPU|k16|d3"] = {"config": [8, 512, 4, 0], "ms": 1.0, "default_ms": 1.2}
+    autotune._save_file()
+    autotune._cache.clear()
+    assert autotune._load_file()["GPU|k16|d3"]["config"] == [8, 512, 4, 0]
+    autotune._cache.clear()
