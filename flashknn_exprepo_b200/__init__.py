@@ -4,6 +4,8 @@ Public entry points (mirroring the reference's ``FlashKNN/functions``):
   FlashKNN              -- query / selected_query drop-in (wrapper.py)
   knn_query, KNNQuery   -- Pointcept-style offset batching with a
                            differentiable squared distance (pointops.py)
+  knn_query_host        -- the same from host buffers to host buffers, copies
+                           overlapped with the query cloud run by cloud run
   ball_query            -- radius-limited grid query, Pointcept's signature
   grouping, knn_query_and_group, ball_query_and_group
                         -- neighbour feature gather with a deterministic
@@ -22,11 +24,12 @@ from . import hierarchy, ops
 from ._lib import FknnError
 from .adaptive import AdaptiveNeighborhoodFlashKNN
 from .pointops import (KNNQuery, ball_query, ball_query_and_group, grouping, knn_query,
-                       knn_query_and_group)
+                       knn_query_and_group, knn_query_host)
 from .wrapper import FlashKNN
 from .z_order import xyz2key
 
-__all__ = ["FlashKNN", "AdaptiveNeighborhoodFlashKNN", "KNNQuery", "knn_query", "ball_query",
+__all__ = ["FlashKNN", "AdaptiveNeighborhoodFlashKNN", "KNNQuery", "knn_query", "knn_query_host",
+           "ball_query",
            "grouping", "knn_query_and_group", "ball_query_and_group",
            "xyz2key",
            "hierarchy", "ops", "FknnError"]

@@ -178,3 +178,61 @@ def ball_query_and_group(feat, xyz, offset=None, new_xyz=None, new_offset=None, 
         idx, _ = ball_query(nsample, max_radio, min_radio, xyz, offset, new_xyz, new_offset,
                             voxel_size=voxel_size, num_down=num_down)
     return grouping(idx, feat, xyz, new_xyz, with_xyz), idx
+
+
+def knn_query_host(nsample, xyz, offset, idx_out=None, dist_out=None, *, voxel_size,
+                   num_down=2, chunks=4, device=None, config=None):
+    """Self query of an offset batch held in host memory, answers written to
+    host memory: the call for a caller whose points arrive from and whose
+    neighbours go back to the CPU.
+
+    The batch is cut into ``chunks`` runs of whole clouds of about equal size.
+    Each run's upload, query and index shift run on the current stream, and
+    its download starts on a second stream as soon as the run is done, so the
+    device-to-host copy of one run overlaps the upload and query of the next
+    (the copies, 8*nsample bytes per point, are the bound on a PCIe host).
+    Clouds are independent, so the answer equals one ``knn_query`` over the
+    whole batch.  ``xyz`` f32 [n,3] and the outputs should be pinned for the
+    copies to be asynchronous; the call returns when the work is queued:
+    synchronise the current stream before reading the outputs.
+    Returns (idx int32 [n, nsample], dist2 f32 [n, nsample]) on the host.
+    """
+    dev = torch.device(device) if device is not None else torch.device("cuda",
+                                                                       torch.cuda.current_device())
+    offset = torch.as_tensor(offset, dtype=torch.int64).cpu()
+    n = int(offset[-1]) if offset.numel() else 0
+    if idx_out is None:
+        idx_out = torch.empty((n, nsample), dtype=torch.int32).pin_memory()
+    if dist_out is None:
+        dist_out = torch.empty((n, nsample), dtype=torch.float32).pin_memory()
+    if n == 0:
+        return idx_out, dist_out
+    # whole-cloud runs of about n / chunks points
+    ends = offset.tolist()
+    cuts, target = [0], n / max(1, chunks)
+    for c, e in enumerate(ends):
+        if e >= target * len(cuts) and c + 1 < len(ends) and len(cuts) < chunks:
+            cuts.append(c + 1)
+    cuts.append(len(ends))
+    compute = torch.cuda.current_stream(dev)
+    copy = torch.cuda.Stream(dev)
+    for a, b in zip(cuts[:-1], cuts[1:]):
+        if a == b:
+            continue
+        start = ends[a - 1] if a else 0
+        stop = ends[b - 1]
+        x = xyz[start:stop].to(dev, non_blocking=True)
+        o = (offset[a:b] - start).to(dev, non_blocking=True)
+        idx, dist = ops.knn_offsets(x, o, nsample, voxel_size, num_down, config=config)
+        if start:
+            idx += start                               # run-local -> batch indices
+        done = torch.cuda.Event()
+        done.record(compute)
+        copy.wait_event(done)
+        with torch.cuda.stream(copy):
+            idx_out[start:stop].copy_(idx, non_blocking=True)
+            dist_out[start:stop].copy_(dist, non_blocking=True)
+        idx.record_stream(copy)
+        dist.record_stream(copy)
+    compute.wait_stream(copy)
+    return idx_out, dist_out

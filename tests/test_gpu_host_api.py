@@ -1,0 +1,41 @@
+"""knn_query_host (host buffers in, host buffers out, copies overlapped with
+the query run by run) returns exactly what one device-side call returns."""
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def fk():
+    import flashknn_exprepo_b200 as fk
+    from flashknn_exprepo_b200.build import build
+    build()
+    return fk
+
+
+@pytest.mark.parametrize("chunks", [1, 3, 4, 40])
+def test_host_query_equals_device_query(fk, chunks):
+    from flashknn_exprepo_b200 import synthetic as S
+    b = S.first_clouds(S.uneven_batch(), 6)
+    xyz = torch.from_numpy(b.xyz).pin_memory()
+    off = torch.from_numpy(b.offsets)
+    idx, dist = fk.knn_query_host(16, xyz, off, voxel_size=S.C4_VOXEL, chunks=chunks)
+    torch.cuda.current_stream().synchronize()
+    di, dd = fk.ops.knn_offsets(xyz.cuda(), off.cuda(), 16, S.C4_VOXEL, 2)
+    assert torch.equal(idx, di.cpu())
+    assert torch.equal(dist.view(torch.int32), dd.cpu().view(torch.int32))
+
+
+def test_host_query_into_caller_buffers(fk):
+    rng = np.random.default_rng(2)
+    xyz = torch.from_numpy(rng.random((5000, 3), dtype=np.float32)).pin_memory()
+    off = torch.tensor([1000, 2500, 5000])
+    idx = torch.full((5000, 8), -7, dtype=torch.int32).pin_memory()
+    dist = torch.empty((5000, 8), dtype=torch.float32).pin_memory()
+    out = fk.knn_query_host(8, xyz, off, idx, dist, voxel_size=0.02, chunks=2)
+    torch.cuda.current_stream().synchronize()
+    assert out[0] is idx and out[1] is dist
+    di, dd = fk.ops.knn_offsets(xyz.cuda(), off.cuda(), 8, 0.02, 2)
+    assert torch.equal(idx, di.cpu()) and torch.equal(dist, dd.cpu())
