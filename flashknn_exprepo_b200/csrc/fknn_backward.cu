@@ -37,21 +37,37 @@ __global__ void __launch_bounds__(256)
     k_bwd_query(const float* __restrict__ q_xyz, int64_t m, const float* __restrict__ p_xyz,
                 int64_t n, const int32_t* __restrict__ idx, const float* __restrict__ dist,
                 const float* __restrict__ grad, int k, float* __restrict__ grad_q, int accumulate,
-                uint32_t* __restrict__ count) {
+                uint32_t* __restrict__ count, int vec4) {
   const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (i >= m) return;
   const float qx = q_xyz[3 * i], qy = q_xyz[3 * i + 1], qz = q_xyz[3 * i + 2];
   float gx = 0.f, gy = 0.f, gz = 0.f;
-  for (int j = 0; j < k; ++j) {
-    const int64_t e = i * k + j;
-    const int32_t t = idx[e];
-    if (!entry_valid(t, n, dist[e])) continue;
+  auto entry = [&](int32_t t, float d, float g) {
+    if (!entry_valid(t, n, d)) return;
     if (count) atomicAdd(&count[t], 1u);
-    if (!grad_q) continue;
-    const float g2 = 2.f * grad[e];
+    if (!grad_q) return;
+    const float g2 = 2.f * g;
     gx = __fmaf_rn(g2, __fsub_rn(qx, p_xyz[3 * static_cast<int64_t>(t)]), gx);
     gy = __fmaf_rn(g2, __fsub_rn(qy, p_xyz[3 * static_cast<int64_t>(t) + 1]), gy);
     gz = __fmaf_rn(g2, __fsub_rn(qz, p_xyz[3 * static_cast<int64_t>(t) + 2]), gz);
+  };
+  if (vec4) {  // k % 4 == 0 and 16-byte aligned rows: 128-bit row loads, j ascending
+    const int4* i4 = reinterpret_cast<const int4*>(idx + i * k);
+    const float4* d4 = reinterpret_cast<const float4*>(dist + i * k);
+    const float4* g4 = reinterpret_cast<const float4*>(grad + i * k);
+    for (int j = 0; j < (k >> 2); ++j) {
+      const int4 t = i4[j];
+      const float4 d = d4[j], g = g4[j];
+      entry(t.x, d.x, g.x);
+      entry(t.y, d.y, g.y);
+      entry(t.z, d.z, g.z);
+      entry(t.w, d.w, g.w);
+    }
+  } else {
+    for (int j = 0; j < k; ++j) {
+      const int64_t e = i * k + j;
+      entry(idx[e], dist[e], grad[e]);
+    }
   }
   if (grad_q) {
     if (accumulate) {
@@ -278,10 +294,12 @@ int run_backward(const BackwardArgs& a, void* ws, size_t ws_bytes, cudaStream_t 
     note_cuda_error(e);
     return FKNN_ERR_CUDA;
   }
+  const auto al16 = [](const void* p) { return reinterpret_cast<uintptr_t>(p) % 16 == 0; };
+  const bool vec4 = a.k % 4 == 0 && al16(a.idx) && al16(a.dist) && al16(a.grad);
   if (a.m > 0 && (a.grad_q || want_p)) {
     k_bwd_query<<<blocks_for(a.m, 256), 256, 0, s>>>(a.q_xyz, a.m, a.p_xyz, a.n, a.idx, a.dist,
                                                      a.grad, a.k, a.grad_q, a.accumulate,
-                                                     want_p ? b.count : nullptr);
+                                                     want_p ? b.count : nullptr, vec4 ? 1 : 0);
     ++nl;
   }
   if (want_p) {
