@@ -115,15 +115,29 @@ __global__ void __launch_bounds__(kScanTile)
 __global__ void __launch_bounds__(256)
     k_bwd_scatter(int64_t total, int64_t n, const int32_t* __restrict__ idx,
                   const float* __restrict__ dist, const float* __restrict__ grad,
-                  uint32_t* __restrict__ cursor, uint64_t* __restrict__ pairs) {
-  for (int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; e < total;
-       e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    const int32_t t = idx[e];
-    if (!entry_valid(t, n, dist[e])) continue;
+                  uint32_t* __restrict__ cursor, uint64_t* __restrict__ pairs, int vec4) {
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  auto put = [&](int64_t e, int32_t t, float d, float g) {
+    if (!entry_valid(t, n, d)) return;
     const uint32_t slot = atomicSub(&cursor[t], 1u) - 1u;
-    const float g2 = -2.f * grad[e];
-    pairs[slot] = (static_cast<uint64_t>(e) << 32) | __float_as_uint(g2);
+    pairs[slot] = (static_cast<uint64_t>(e) << 32) | __float_as_uint(-2.f * g);
+  };
+  if (vec4) {  // total % 4 == 0, 16-byte aligned: four entries (and atomics) in flight
+    for (int64_t w = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+         w < (total >> 2); w += stride) {
+      const int4 t = reinterpret_cast<const int4*>(idx)[w];
+      const float4 d = reinterpret_cast<const float4*>(dist)[w];
+      const float4 g = reinterpret_cast<const float4*>(grad)[w];
+      put(4 * w, t.x, d.x, g.x);
+      put(4 * w + 1, t.y, d.y, g.y);
+      put(4 * w + 2, t.z, d.z, g.z);
+      put(4 * w + 3, t.w, d.w, g.w);
+    }
+    return;
   }
+  for (int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; e < total;
+       e += stride)
+    put(e, idx[e], dist[e], grad[e]);
 }
 
 namespace {
@@ -307,7 +321,7 @@ int run_backward(const BackwardArgs& a, void* ws, size_t ws_bytes, cudaStream_t 
     if (total > 0) {
       const int64_t sb = ceil_div(total, 256);
       k_bwd_scatter<<<static_cast<int>(sb < 8192 ? sb : 8192), 256, 0, s>>>(
-          total, a.n, a.idx, a.dist, a.grad, b.cursor, b.pairs);
+          total, a.n, a.idx, a.dist, a.grad, b.cursor, b.pairs, vec4 ? 1 : 0);
       ++nl;
     }
     k_bwd_support<<<blocks_for(a.n, 128), 128, 0, s>>>(a.q_xyz, a.p_xyz, a.n, a.k, b.start,
