@@ -384,7 +384,8 @@ __global__ void __launch_bounds__(256)
   }
 }
 
-// cand[c] = points in the 27 nodes around node c.
+// cand[c] = points in the 27 nodes around node c.  One warp per node, one
+// lookup per lane, so the 27 probes are in flight together.
 __global__ void __launch_bounds__(256)
     ka_counts(LevelArgs a, const int* count_ptr, const int32_t* __restrict__ node_start, Table t,
               int32_t* __restrict__ cand) {
@@ -392,12 +393,14 @@ __global__ void __launch_bounds__(256)
   const uint64_t* key = sorted_keys(a.sp, a.bits);
   const int bpa = a.meta->bpa;
   const int nodes = *count_ptr;
-  for (int64_t c = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; c < nodes;
-       c += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warps = static_cast<int64_t>(gridDim.x) * (blockDim.x >> 5);
+  for (int64_t c = static_cast<int64_t>(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5);
+       c < nodes; c += warps) {
     const uint64_t nk = key[node_start[c]] >> (3 * a.s);
-    int total = 0;
-    for (int j = 0; j < kNeighbours; ++j) total += neighbour_run(t, nk, a.s, bpa, j).y;
-    cand[c] = total;
+    const int len = lane < kNeighbours ? neighbour_run(t, nk, a.s, bpa, lane).y : 0;
+    const int total = __reduce_add_sync(kFull, len);
+    if (lane == 0) cand[c] = total;
   }
 }
 
@@ -423,22 +426,33 @@ __global__ void __launch_bounds__(256)
 
 // Points whose selection stopped at level L open their query groups: a
 // group is a maximal run of sorted positions with level L and the same
-// level-L node.  group_flag[p] and the group's 27 runs (row p).
+// level-L node.  group_flag[p] and the group's 27 runs (row p).  One warp per
+// 32 consecutive points: every lane decides for its point, then the warp
+// looks up the 27 runs of each group start together, one run per lane.
 __global__ void __launch_bounds__(256)
     ka_finalize(LevelArgs a, int L, Table t, const uint8_t* __restrict__ sel,
                 uint8_t* __restrict__ group_flag, int2* __restrict__ runs) {
   if (L > top_level(a.meta)) return;
   const uint64_t* key = sorted_keys(a.sp, a.bits);
   const int bpa = a.meta->bpa;
-  const int64_t total = a.n * kNeighbours;
-  for (int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; e < total;
-       e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    const int64_t p = e / kNeighbours;
-    const int j = static_cast<int>(e - p * kNeighbours);
-    if (sel[p] != L) continue;
-    const bool start = p == 0 || sel[p - 1] != L || node_head(key, p, 3 * L);
-    if (j == 0) group_flag[p] = start ? 1 : 0;
-    if (start) runs[e] = neighbour_run(t, key[p] >> (3 * L), L, bpa, j);
+  const int lane = threadIdx.x & 31;
+  const int64_t warps = static_cast<int64_t>(gridDim.x) * (blockDim.x >> 5);
+  for (int64_t base = (static_cast<int64_t>(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5)) * 32;
+       base < a.n; base += warps * 32) {
+    const int64_t p = base + lane;
+    bool start = false;
+    if (p < a.n && sel[p] == L) {
+      start = p == 0 || sel[p - 1] != L || node_head(key, p, 3 * L);
+      group_flag[p] = start ? 1 : 0;
+    }
+    uint32_t starts = __ballot_sync(kFull, start);
+    while (starts) {
+      const int src = __ffs(starts) - 1;
+      starts &= starts - 1;
+      const int64_t ps = base + src;
+      if (lane < kNeighbours)
+        runs[ps * kNeighbours + lane] = neighbour_run(t, key[ps] >> (3 * L), L, bpa, lane);
+    }
   }
 }
 
@@ -635,14 +649,14 @@ int run_adaptive(const AdaptiveArgs& f, void* ws, size_t ws_bytes, const QuerySh
     ka_nodes<<<tiles, 256, 0, s>>>(la, b.tile_counts, nodes, b.node_of, b.node_start);
     ka_insert<<<capped_blocks(n), 256, 0, s>>>(la, nodes, b.node_start, tab[lv & 1],
                                                b.slot_of[lv & 1]);
-    ka_counts<<<capped_blocks(n), 256, 0, s>>>(la, nodes, b.node_start, tab[lv & 1], b.cand);
+    ka_counts<<<capped_blocks(n * 32), 256, 0, s>>>(la, nodes, b.node_start, tab[lv & 1], b.cand);
     ka_select<<<blocks_for(n, 256), 256, 0, s>>>(la, b.node_of, b.cand, min_count, max_count,
                                                  b.sel, b.active);
     nl += 6;
     if (lv < top_host) {
       const int up = lv + 1;
-      ka_finalize<<<capped_blocks(n * kNeighbours), 256, 0, s>>>(la, up, tab[up & 1], b.sel,
-                                                                  b.group_flag, b.runs);
+      ka_finalize<<<capped_blocks(n), 256, 0, s>>>(la, up, tab[up & 1], b.sel, b.group_flag,
+                                                    b.runs);
       ka_erase<<<capped_blocks(n), 256, 0, s>>>(la, up, b.level_nodes + up, b.slot_of[up & 1],
                                                 b.tkeys[up & 1]);
       nl += 2;
@@ -650,8 +664,7 @@ int run_adaptive(const AdaptiveArgs& f, void* ws, size_t ws_bytes, const QuerySh
   }
   {
     const LevelArgs la{sp, key_bits, b.meta, n, 0};
-    ka_finalize<<<capped_blocks(n * kNeighbours), 256, 0, s>>>(la, 0, tab[0], b.sel,
-                                                                b.group_flag, b.runs);
+    ka_finalize<<<capped_blocks(n), 256, 0, s>>>(la, 0, tab[0], b.sel, b.group_flag, b.runs);
     ka_group_tiles<<<tiles, 256, 0, s>>>(n, b.group_flag, b.tile_counts);
     k_scan_tiles<<<1, 1024, 0, s>>>(b.tile_counts, tiles, &b.meta->n_groups);
     ka_groups<<<tiles, 256, 0, s>>>(n, b.group_flag, b.tile_counts, &b.meta->n_groups,
