@@ -72,6 +72,7 @@ _SIGNATURES = {
     "fknn_workspace_bytes": (_SZ, [_I64, _I64, _I64, _I32]),
     "fknn_knn_offsets": (ctypes.c_int, [_P, _I64, _P, _I64, _P, _I64, _P, _I32, _F32, _I32,
                                         _F32, _P, _P, _P, _SZ, _P, _P]),
+    "fknn_selftest_bounded_wait": (ctypes.c_int, [_P, _SZ, ctypes.c_uint32, _P]),
     "fknn_ball_query": (ctypes.c_int, [_P, _I64, _P, _I64, _P, _I64, _P, _I32, _F32, _I32, _F32,
                                        _P, _P, _P, _SZ, _P, _P]),
     "fknn_knn_grid": (ctypes.c_int, [_P, _P, _P, _I64, _P, _I64, _I32, _I32, _F32, _I32, _P, _P,

@@ -166,6 +166,13 @@ int fknn_profile_read(float* ms_out, int max) {
   return count;
 }
 
+int fknn_selftest_bounded_wait(void* workspace, size_t workspace_bytes, uint32_t limit,
+                               void* stream) {
+  if (!workspace || limit < 1 || limit > (1u << 20)) return FKNN_ERR_ARG;
+  if (!aligned(workspace, 256)) return FKNN_ERR_ARG;
+  return fknn::run_selftest_wait(workspace, workspace_bytes, limit, as_stream(stream));
+}
+
 int fknn_read_status(const void* workspace, int* status, void* stream) {
   if (!workspace || !status) return FKNN_ERR_ARG;
   cudaError_t e = cudaMemcpyAsync(status, workspace, sizeof(int), cudaMemcpyDeviceToHost,

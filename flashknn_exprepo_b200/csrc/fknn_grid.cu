@@ -678,7 +678,7 @@ int run_fused(const FusedArgs& f, void* ws, size_t ws_bytes, const QueryShape& s
           b.runs);
       ++nl;
       nl += launch_items(b.runs, b.cell_start, nullptr, &b.meta->n_cells, n, shape.tile_records,
-                         b.cands, b.seg_counts, &b.meta->n_items, b.items, s);
+                         b.cands, b.seg_counts, &b.meta->n_items, b.items, s, &b.meta->status, n);
     }
   } else if (kind == FKNN_QUERY_SELECTED) {
     pad_mode = kPadArray64;
@@ -712,7 +712,8 @@ int run_fused(const FusedArgs& f, void* ws, size_t ws_bytes, const QueryShape& s
                                               b.group_start, nullptr);
       nl += 3;
       nl += launch_items(b.runs, b.group_start, b.group_row, &b.meta->n_groups, m,
-                         shape.tile_records, b.cands, b.seg_counts, &b.meta->n_items, b.items, s);
+                         shape.tile_records, b.cands, b.seg_counts, &b.meta->n_items, b.items, s,
+                         &b.meta->status, m);
     }
   } else {  // general queries
     pad_mode = kPadMinusOne;
@@ -739,7 +740,7 @@ int run_fused(const FusedArgs& f, void* ws, size_t ws_bytes, const QueryShape& s
           b.meta, b.runs);
       nl += 4;
       nl += launch_items(b.runs, b.group_start, nullptr, &b.meta->n_groups, m, shape.tile_records,
-                         b.cands, b.seg_counts, &b.meta->n_items, b.items, s, &b.meta->status);
+                         b.cands, b.seg_counts, &b.meta->n_items, b.items, s, &b.meta->status, m);
     }
   }
 

@@ -39,10 +39,15 @@ __global__ void __launch_bounds__(256)
 // One thread per segment of kPackSegment groups.  With items == nullptr it
 // only counts (seg_counts[seg]); otherwise it writes its items at
 // seg_offsets[seg].  Item = (q_start, q_count, g_first, g_count | flags).
+// Caller tables can be malformed: a group whose query range leaves
+// [0, n_queries] is reported and skipped, and no item is written at or past
+// `capacity` (overlapping ranges could otherwise ask for more items than the
+// buffer holds; k_scan_segments clamps the count to match).
 __global__ void __launch_bounds__(256)
     k_pack(const int32_t* __restrict__ group_start, const int32_t* __restrict__ cands,
-           const int* group_count_ptr, int tile, uint32_t* __restrict__ seg_counts,
-           const uint32_t* __restrict__ seg_offsets, int4* __restrict__ items) {
+           const int* group_count_ptr, int tile, int64_t n_queries, int64_t capacity,
+           uint32_t* __restrict__ seg_counts, const uint32_t* __restrict__ seg_offsets,
+           int4* __restrict__ items, int* status) {
   const int n_groups = *group_count_ptr;
   const int64_t n_segs = (n_groups + kPackSegment - 1) / kPackSegment;
   for (int64_t seg = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; seg < n_segs;
@@ -54,7 +59,12 @@ __global__ void __launch_bounds__(256)
     uint32_t count = 0;
     int cur_q0 = 0, cur_qn = 0, cur_g0 = 0, cur_gn = 0, cur_c = 0;
     auto emit = [&](int q0, int qn, int g0, int gn, int flags) {
-      if (items) items[out + count] = make_int4(q0, qn, g0, gn | flags);
+      if (items) {
+        if (static_cast<int64_t>(out) + count < capacity)
+          items[out + count] = make_int4(q0, qn, g0, gn | flags);
+        else
+          raise_status(status, kStatusTable);
+      }
       ++count;
     };
     auto flush = [&]() {
@@ -64,6 +74,10 @@ __global__ void __launch_bounds__(256)
     for (int g = static_cast<int>(g_begin); g < g_end; ++g) {
       const int gs = group_start[g], ge = group_start[g + 1];
       const int c = cands[g];
+      if (gs < 0 || ge > n_queries) {
+        if (items) raise_status(status, kStatusTable);
+        continue;
+      }
       if (ge <= gs) continue;
       if (c > tile) {  // streams its candidates: items of its own
         flush();
@@ -94,10 +108,11 @@ __global__ void __launch_bounds__(256)
 }
 
 // Exclusive scan of the per-segment item counts over the segments that hold
-// groups (the device-side group count bounds the work).
+// groups (the device-side group count bounds the work); the total is clamped
+// to the item buffer's capacity.
 __global__ void __launch_bounds__(1024)
     k_scan_segments(uint32_t* __restrict__ seg_counts, const int* group_count_ptr,
-                    int* __restrict__ total_out) {
+                    int64_t capacity, int* __restrict__ total_out, int* status) {
   __shared__ uint32_t warp_sums[32];
   __shared__ uint32_t s_total;
   const int n_segs = (*group_count_ptr + kPackSegment - 1) / kPackSegment;
@@ -109,13 +124,16 @@ __global__ void __launch_bounds__(1024)
     if (t < n_segs) seg_counts[t] = carry + incl - x;
     carry += s_total;
   }
-  if (threadIdx.x == 0) *total_out = static_cast<int>(carry);
+  if (threadIdx.x == 0) {
+    if (static_cast<int64_t>(carry) > capacity) raise_status(status, kStatusTable);
+    *total_out = static_cast<int>(static_cast<int64_t>(carry) < capacity ? carry : capacity);
+  }
 }
 
 int launch_items(const int2* runs, const int32_t* group_start, const int32_t* group_row,
                  const int* group_count_ptr, int64_t max_groups, int tile, int32_t* cands,
                  uint32_t* seg_counts, int* n_items_ptr, int4* items, cudaStream_t s,
-                 int* status) {
+                 int* status, int64_t n_queries) {
   if (max_groups <= 0) return 0;
   // grids for the host-side bound, capped: the device count drives the loops
   const int64_t gb = ceil_div(max_groups, 256);
@@ -123,11 +141,12 @@ int launch_items(const int2* runs, const int32_t* group_start, const int32_t* gr
   const int64_t sb = ceil_div(ceil_div(max_groups, kPackSegment), 256);
   const int sblocks = static_cast<int>(sb < 1024 ? sb : 1024);
   k_group_cands<<<gblocks, 256, 0, s>>>(runs, group_row, group_count_ptr, cands, status);
-  k_pack<<<sblocks, 256, 0, s>>>(group_start, cands, group_count_ptr, tile, seg_counts, nullptr,
-                                 nullptr);
-  k_scan_segments<<<1, 1024, 0, s>>>(seg_counts, group_count_ptr, n_items_ptr);
-  k_pack<<<sblocks, 256, 0, s>>>(group_start, cands, group_count_ptr, tile, nullptr, seg_counts,
-                                 items);
+  const int64_t capacity = static_cast<int64_t>(items_capacity(max_groups, n_queries));
+  k_pack<<<sblocks, 256, 0, s>>>(group_start, cands, group_count_ptr, tile, n_queries, capacity,
+                                 seg_counts, nullptr, nullptr, status);
+  k_scan_segments<<<1, 1024, 0, s>>>(seg_counts, group_count_ptr, capacity, n_items_ptr, status);
+  k_pack<<<sblocks, 256, 0, s>>>(group_start, cands, group_count_ptr, tile, n_queries, capacity,
+                                 nullptr, seg_counts, items, status);
   return 4;
 }
 

@@ -86,6 +86,15 @@ FKNN_API int fknn_last_launch_count(void);
 FKNN_API int fknn_profile_enable(int slots);
 FKNN_API int fknn_profile_read(float* ms_out, int max);
 
+/* No reference counterpart.  Failure-path self-test: launches one CTA that
+ * waits, with the query kernel's bounded wait, on a shared-memory barrier
+ * that nothing completes, and gives up after `limit` polls (1..2^20),
+ * setting FKNN_DEVICE_TIMEOUT in the workspace's status word (read it with
+ * fknn_read_status).  Nothing faults and nothing is left in flight; the
+ * call lets a test check that a stalled wait ends and is reported. */
+FKNN_API int fknn_selftest_bounded_wait(void* workspace, size_t workspace_bytes, uint32_t limit,
+                               void* stream);
+
 /* --------------------------------------------- fused queries (a1..a9)
  * Grid construction + candidate gather + top-K + remap in one stream of
  * launches.  Output rows follow the caller's query order; indices are in
