@@ -490,24 +490,46 @@ __global__ void __launch_bounds__(256) k_query(QueryLaunch a, int T, int min_can
     sort_network<KCAP, 0, KCAP>(L);
     uint32_t thr = static_cast<uint32_t>(L[KCAP - 1] >> 32);
     int stop = active ? stop_position<KCAP>(L, s, rq, bs) : 0;
-    for (int t = KCAP;; ++t) {
-      const bool live = t < stop;
-      if (!__any_sync(kFull, live)) break;
-      bool acc = false;
-      uint64_t x = kEmpty;
-      if (live) {
-        const uint16_t e = srt16[s.seg + t];
-        const float4 c = tile[s.seg + (e & 1023)];
-        const float d = sq_dist(c.x, c.y, c.z, q.x, q.y, q.z);
-        const uint32_t db = __float_as_uint(d);
-        acc = (d < a.cut_r2) && (db <= thr);
-        if (acc) x = make_key(d, c.w);
-      }
-      if (__any_sync(kFull, acc)) {
-        insert_one<KCAP>(L, x);
-        if (acc) {
+    // Candidate t of the lane's scan: accepted when it beats the K-th.
+    auto test = [&](int t, uint64_t& x) {
+      const uint16_t e = srt16[s.seg + t];
+      const float4 c = tile[s.seg + (e & 1023)];
+      const float d = sq_dist(c.x, c.y, c.z, q.x, q.y, q.z);
+      const bool acc = (d < a.cut_r2) && (__float_as_uint(d) <= thr);
+      if (acc) x = make_key(d, c.w);
+      return acc;
+    };
+    if constexpr (KCAP <= 16) {
+      // Two candidates per iteration, both tested against the same K-th
+      // distance and inserted in order: half the loop and vote overhead, and
+      // two independent loads and distance chains in flight.  (With a
+      // 32- or 64-entry list the extra registers cost more than this saves.)
+      for (int t = KCAP;; t += 2) {
+        const bool live0 = t < stop, live1 = t + 1 < stop;
+        if (!__any_sync(kFull, live0)) break;
+        uint64_t x0 = kEmpty, x1 = kEmpty;
+        const bool acc0 = live0 && test(t, x0);
+        const bool acc1 = live1 && test(t + 1, x1);
+        const bool any0 = __any_sync(kFull, acc0), any1 = __any_sync(kFull, acc1);
+        if (any0) insert_one<KCAP>(L, x0);
+        if (any1) insert_one<KCAP>(L, x1);
+        if (acc0 || acc1) {
           thr = static_cast<uint32_t>(L[KCAP - 1] >> 32);
           stop = min(stop, stop_position<KCAP>(L, s, rq, bs));
+        }
+      }
+    } else {
+      for (int t = KCAP;; ++t) {
+        const bool live = t < stop;
+        if (!__any_sync(kFull, live)) break;
+        uint64_t x = kEmpty;
+        const bool acc = live && test(t, x);
+        if (__any_sync(kFull, acc)) {
+          insert_one<KCAP>(L, x);
+          if (acc) {
+            thr = static_cast<uint32_t>(L[KCAP - 1] >> 32);
+            stop = min(stop, stop_position<KCAP>(L, s, rq, bs));
+          }
         }
       }
     }
