@@ -376,8 +376,11 @@ __global__ void k_hash_clear(const int* cell_count_ptr, uint64_t* __restrict__ h
     hkeys[i] = kHashEmpty;
 }
 
+// Value = the cell's candidate run (start, count), so a lookup needs no
+// further load of the cell starts.
 __global__ void k_hash_insert(const uint64_t* __restrict__ cell_key, const int* cell_count_ptr,
-                              uint64_t* __restrict__ hkeys, int32_t* __restrict__ hvals) {
+                              const int32_t* __restrict__ cell_start, uint64_t* __restrict__ hkeys,
+                              int2* __restrict__ hvals) {
   const int cells = *cell_count_ptr;
   const uint32_t mask = hash_capacity(cells) - 1;
   for (int64_t c = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; c < cells;
@@ -388,7 +391,7 @@ __global__ void k_hash_insert(const uint64_t* __restrict__ cell_key, const int* 
       const unsigned long long prev = atomicCAS(
           reinterpret_cast<unsigned long long*>(hkeys + h), kHashEmpty, key);
       if (prev == kHashEmpty || prev == key) {
-        hvals[h] = static_cast<int32_t>(c);
+        hvals[h] = make_int2(cell_start[c], cell_start[c + 1] - cell_start[c]);
         break;
       }
       h = (h + 1) & mask;
@@ -396,16 +399,16 @@ __global__ void k_hash_insert(const uint64_t* __restrict__ cell_key, const int* 
   }
 }
 
-__device__ __forceinline__ int32_t hash_find(const uint64_t* hkeys, const int32_t* hvals,
+__device__ __forceinline__ int2 hash_find(const uint64_t* hkeys, const int2* hvals,
                                              uint32_t mask, uint64_t key) {
   uint32_t h = hash_slot(key, mask);
   for (uint32_t probe = 0; probe <= mask; ++probe) {
     const uint64_t k = hkeys[h];
     if (k == key) return hvals[h];
-    if (k == kHashEmpty) return -1;
+    if (k == kHashEmpty) break;
     h = (h + 1) & mask;
   }
-  return -1;
+  return make_int2(0, 0);  // no such cell: an empty run
 }
 
 // One thread per (group, neighbour position).  group_key[g] is a key in the
@@ -413,8 +416,8 @@ __device__ __forceinline__ int32_t hash_find(const uint64_t* hkeys, const int32_
 // offset j, or (0, 0) when that cell is empty.
 __global__ void __launch_bounds__(256)
     k_runs(const uint64_t* __restrict__ group_key, const int* group_count_ptr,
-           const uint64_t* __restrict__ hkeys, const int32_t* __restrict__ hvals,
-           const int32_t* __restrict__ cell_start, const int* cell_count_ptr, const Meta* meta,
+           const uint64_t* __restrict__ hkeys, const int2* __restrict__ hvals,
+           const int* cell_count_ptr, const Meta* meta,
            int2* __restrict__ runs) {
   const int64_t total = static_cast<int64_t>(*group_count_ptr) * kNeighbours;
   const int bpa = meta->bpa;
@@ -436,8 +439,7 @@ __global__ void __launch_bounds__(256)
       const uint64_t nk = (cloud << (3 * bpa)) |
                           morton3(static_cast<uint32_t>(x), static_cast<uint32_t>(y),
                                   static_cast<uint32_t>(z));
-      const int32_t hit = hash_find(hkeys, hvals, hmask, nk);
-      if (hit >= 0) run = make_int2(cell_start[hit], cell_start[hit + 1] - cell_start[hit]);
+      run = hash_find(hkeys, hvals, hmask, nk);
     }
     runs[t] = run;
   }
@@ -532,7 +534,7 @@ struct Bufs {
   int32_t* cands;
   uint32_t* seg_counts;
   uint64_t* hkeys;
-  int32_t* hvals;
+  int2* hvals;
   int64_t hash_cap;
 };
 
@@ -561,7 +563,7 @@ Bufs layout(void* ws, int64_t n, int64_t m, int64_t n_clouds, int kind, size_t* 
   b.hash_cap = 16;
   while (b.hash_cap < 2 * n) b.hash_cap <<= 1;
   b.hkeys = a.take<uint64_t>(b.hash_cap);
-  b.hvals = a.take<int32_t>(b.hash_cap);
+  b.hvals = a.take<int2>(b.hash_cap);
   if (kind == FKNN_QUERY_SELECTED) {
     b.pos_of = a.take<int32_t>(n);
     b.cell_of = a.take<int32_t>(n);
@@ -657,8 +659,8 @@ int run_fused(const FusedArgs& f, void* ws, size_t ws_bytes, const QueryShape& s
                                             &b.meta->n_cells, b.cell_key, b.cell_start, b.cell_of);
     k_hash_clear<<<static_cast<int>(b.hash_cap < 1024 * 256 ? ceil_div(b.hash_cap, 256) : 1024), 256, 0,
                    s>>>(&b.meta->n_cells, b.hkeys);
-    k_hash_insert<<<capped_blocks(n), 256, 0, s>>>(b.cell_key, &b.meta->n_cells, b.hkeys,
-                                                     b.hvals);
+    k_hash_insert<<<capped_blocks(n), 256, 0, s>>>(b.cell_key, &b.meta->n_cells, b.cell_start,
+                                                     b.hkeys, b.hvals);
     nl += 5;
   }
 
@@ -674,7 +676,7 @@ int run_fused(const FusedArgs& f, void* ws, size_t ws_bytes, const QueryShape& s
   if (kind == FKNN_QUERY_SELF) {
     if (n > 0) {
       k_runs<<<capped_blocks(n * kNeighbours), 256, 0, s>>>(
-          b.cell_key, &b.meta->n_cells, b.hkeys, b.hvals, b.cell_start, &b.meta->n_cells, b.meta,
+          b.cell_key, &b.meta->n_cells, b.hkeys, b.hvals, &b.meta->n_cells, b.meta,
           b.runs);
       ++nl;
       nl += launch_items(b.runs, b.cell_start, nullptr, &b.meta->n_cells, n, shape.tile_records,
@@ -690,7 +692,7 @@ int run_fused(const FusedArgs& f, void* ws, size_t ws_bytes, const QueryShape& s
     group_count_ptr = &b.meta->n_groups;
     if (n > 0) {
       k_runs<<<capped_blocks(n * kNeighbours), 256, 0, s>>>(
-          b.cell_key, &b.meta->n_cells, b.hkeys, b.hvals, b.cell_start, &b.meta->n_cells, b.meta,
+          b.cell_key, &b.meta->n_cells, b.hkeys, b.hvals, &b.meta->n_cells, b.meta,
           b.runs);
       ++nl;
     }
@@ -736,7 +738,7 @@ int run_fused(const FusedArgs& f, void* ws, size_t ws_bytes, const QueryShape& s
                                               &b.meta->n_groups, b.group_key, b.group_start,
                                               nullptr);
       k_runs<<<capped_blocks(m * kNeighbours), 256, 0, s>>>(
-          b.group_key, &b.meta->n_groups, b.hkeys, b.hvals, b.cell_start, &b.meta->n_cells,
+          b.group_key, &b.meta->n_groups, b.hkeys, b.hvals, &b.meta->n_cells,
           b.meta, b.runs);
       nl += 4;
       nl += launch_items(b.runs, b.group_start, nullptr, &b.meta->n_groups, m, shape.tile_records,
