@@ -491,8 +491,20 @@ def rows_single_gpu(fk, torch, dev, flush, peak_gbs):
     torch.cuda.synchronize(dev)
     ms = _event_ms(torch, graph.replay, flush)
     del graph
+    lib = fk._lib.load()
+    lib.fknn_profile_enable(1)
+    buf = ctypes_float_array(1)
+    qms = []
+    for _ in range(5):
+        flush.zero_()
+        fk.ops.adaptive_query(grid, None, 16, xyz=lx)
+        torch.cuda.synchronize()
+        if lib.fknn_profile_read(ctypes.cast(buf, ctypes.c_void_p), 1) == 1:
+            qms.append(buf[0])
+    lib.fknn_profile_enable(0)
     rows["adaptive_lidar_k16"] = {"value": len(lidar) / (ms * 1e-3), "unit": "queries/s",
                                   "ms": ms, "eager_ms": eager, "n_points": len(lidar),
+                                  "query_kernel_ms": statistics.median(qms) if qms else None,
                                   "step": "CUDA-graph replay of the whole adaptive pipeline"}
     # back query K=1 and voxel-first subsampling, 16-cloud batch
     b = synthetic.uneven_batch()
