@@ -18,17 +18,22 @@
 // B200 layout.  The points are sorted once by (batch, morton(translated
 // grid)); in that order every node of every level is a contiguous range, so
 // no coordinates are copied per level (the reference gathers a copy of every
-// referenced support node, :605-608).  Per level, from the coarsest down:
-//   ka_heads / k_scan_tiles / ka_nodes   node starts (flags + scan)
+// referenced support node, :605-608).  Once for all levels:
+//   ka_heads_all / ka_scan_all           node heads per tile and level (the
+//                                        highest bit in which neighbouring
+//                                        keys differ), scanned per level
+// then per level, from the coarsest down (four launches):
+//   ka_nodes                             node starts; empties the table
+//                                        last used two levels up
 //   ka_insert                            open-addressing table: node key ->
 //                                        (start, count); two tables alternate
 //                                        between consecutive levels
 //   ka_counts                            27-node candidate count per node
-//   ka_select                            per-point level selection step
-//   ka_finalize                          points that stopped one level up
+//   ka_select                            per-point level selection step;
+//                                        points that stopped one level up
 //                                        open query groups there and write
 //                                        their 27 (start, count) runs
-//   ka_erase                             empties the table of that level
+// and ka_finalize opens the groups of the points that reach level 0.
 // A query group is a maximal run of sorted points with the same selected
 // level and node; its runs address the same sorted records as its queries,
 // so the packer and the top-K kernel of the fixed-level path serve it
@@ -64,18 +69,28 @@ __device__ __forceinline__ uint32_t slot_of_key(uint64_t key, uint32_t mask) {
   return static_cast<uint32_t>(key) & mask;
 }
 
+// One 16-byte slot: node key and its run, so a probe is a single load.
+struct __align__(16) Slot {
+  uint64_t key;
+  int2 run;
+};
+
 struct Table {
-  uint64_t* keys;
-  int2* vals;
+  Slot* slots;
   uint32_t mask;
 };
 
 __device__ __forceinline__ int2 table_find(const Table& t, uint64_t key) {
   uint32_t h = slot_of_key(key, t.mask);
   for (uint32_t probe = 0; probe <= t.mask; ++probe) {
-    const uint64_t k = t.keys[h];
-    if (k == key) return t.vals[h];
-    if (k == kEmptyKey) break;
+    const ulonglong2 v = __ldcg(reinterpret_cast<const ulonglong2*>(t.slots + h));
+    if (v.x == key) {
+      int2 r;
+      r.x = static_cast<int>(static_cast<uint32_t>(v.y));
+      r.y = static_cast<int>(static_cast<uint32_t>(v.y >> 32));
+      return r;
+    }
+    if (v.x == kEmptyKey) break;
     h = (h + 1) & t.mask;
   }
   return make_int2(0, 0);
@@ -307,31 +322,74 @@ struct LevelArgs {
   int s;
 };
 
-// Node heads of level s per 2048-position tile.
+// Node heads of every level in one pass.  Position p heads a level-s node
+// when key[p] >> 3s differs from key[p-1] >> 3s, i.e. when the highest bit in
+// which the two keys differ is at least 3s: so p heads the nodes of levels
+// 0..hb/3.  tile_counts[s * n_tiles + tile] = heads of level s in the tile.
 __global__ void __launch_bounds__(256)
-    ka_heads(LevelArgs a, uint32_t* __restrict__ tile_counts) {
-  __shared__ uint32_t warp_sums[32];
-  __shared__ uint32_t s_total;
-  if (a.s > top_level(a.meta)) return;
+    ka_heads_all(LevelArgs a, int n_tiles, uint32_t* __restrict__ tile_counts) {
+  __shared__ uint32_t hist[kMaxLevel + 1];
+  if (threadIdx.x <= kMaxLevel) hist[threadIdx.x] = 0u;
+  __syncthreads();
   const uint64_t* key = sorted_keys(a.sp, a.bits);
   const int64_t base = static_cast<int64_t>(blockIdx.x) * kTile + threadIdx.x * 8;
-  uint32_t heads = 0;
 #pragma unroll
   for (int r = 0; r < 8; ++r) {
     const int64_t p = base + r;
-    if (p < a.n && node_head(key, p, 3 * a.s)) ++heads;
+    if (p >= a.n) break;
+    int lvl = kMaxLevel;
+    if (p > 0) {
+      const uint64_t x = key[p] ^ key[p - 1];
+      if (x == 0) continue;  // same leaf key: heads no node
+      lvl = min((63 - __clzll(static_cast<long long>(x))) / 3, kMaxLevel);
+    }
+    atomicAdd(&hist[lvl], 1u);
   }
-  block_inclusive_scan(heads, warp_sums, &s_total);
-  if (threadIdx.x == 0) tile_counts[blockIdx.x] = s_total;
+  __syncthreads();
+  if (threadIdx.x <= kMaxLevel) {  // heads of level s = points whose lvl >= s
+    uint32_t c = 0;
+    for (int l = threadIdx.x; l <= kMaxLevel; ++l) c += hist[l];
+    tile_counts[static_cast<int64_t>(threadIdx.x) * n_tiles + blockIdx.x] = c;
+  }
+}
+
+// One CTA per level: exclusive scan of that level's tile counts in place,
+// level_nodes[s] = the level's node count.
+__global__ void __launch_bounds__(1024)
+    ka_scan_all(uint32_t* __restrict__ tile_counts, int n_tiles, int* __restrict__ level_nodes) {
+  __shared__ uint32_t warp_sums[32];
+  __shared__ uint32_t s_total;
+  uint32_t* col = tile_counts + static_cast<int64_t>(blockIdx.x) * n_tiles;
+  uint32_t carry = 0;
+  for (int t0 = 0; t0 < n_tiles; t0 += blockDim.x) {
+    const int t = t0 + threadIdx.x;
+    const uint32_t x = t < n_tiles ? col[t] : 0u;
+    const uint32_t incl = block_inclusive_scan(x, warp_sums, &s_total);
+    if (t < n_tiles) col[t] = carry + incl - x;
+    carry += s_total;
+  }
+  if (threadIdx.x == 0) level_nodes[blockIdx.x] = static_cast<int>(carry);
 }
 
 // node_of[p] = node of sorted position p at level s; node_start[c] = first
 // position of node c, node_start[count] = n.
+// Also empties the table this level is about to reuse: it still holds the
+// nodes of level s+2 (erase_count of them, at erase_slot), whose last reader
+// was the finalisation of level s+2 in the previous step.
 __global__ void __launch_bounds__(256)
     ka_nodes(LevelArgs a, const uint32_t* __restrict__ tile_offsets, const int* count_ptr,
-             int32_t* __restrict__ node_of, int32_t* __restrict__ node_start) {
+             int32_t* __restrict__ node_of, int32_t* __restrict__ node_start,
+             const int* erase_count, const int32_t* __restrict__ erase_slot,
+             Slot* __restrict__ table) {
   __shared__ uint32_t warp_sums[32];
-  if (a.s > top_level(a.meta)) return;
+  const int top = top_level(a.meta);
+  if (a.s > top) return;
+  if (a.s + 2 <= top) {
+    const int stale = *erase_count;
+    for (int64_t c = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; c < stale;
+         c += static_cast<int64_t>(gridDim.x) * blockDim.x)
+      table[erase_slot[c]].key = kEmptyKey;
+  }
   const uint64_t* key = sorted_keys(a.sp, a.bits);
   const int64_t base = static_cast<int64_t>(blockIdx.x) * kTile + threadIdx.x * 8;
   uint32_t flags = 0, heads = 0;
@@ -373,9 +431,9 @@ __global__ void __launch_bounds__(256)
     uint32_t h = slot_of_key(nk, t.mask);
     for (uint32_t probe = 0; probe <= t.mask; ++probe) {
       const unsigned long long prev =
-          atomicCAS(reinterpret_cast<unsigned long long*>(t.keys + h), kEmptyKey, nk);
+          atomicCAS(reinterpret_cast<unsigned long long*>(&t.slots[h].key), kEmptyKey, nk);
       if (prev == kEmptyKey) {
-        t.vals[h] = make_int2(st, node_start[c + 1] - st);
+        t.slots[h].run = make_int2(st, node_start[c + 1] - st);
         slot_of[c] = static_cast<int32_t>(h);
         break;
       }
@@ -385,11 +443,17 @@ __global__ void __launch_bounds__(256)
 }
 
 // cand[c] = points in the 27 nodes around node c.  One warp per node, one
-// lookup per lane, so the 27 probes are in flight together.
+// lookup per lane, so the 27 probes are in flight together.  Below the top
+// level only points still active read their count, so a node of at most
+// kScanActive points none of which is active (act_in, the previous level's
+// flags) is skipped.
+constexpr int kScanActive = 128;
+
 __global__ void __launch_bounds__(256)
     ka_counts(LevelArgs a, const int* count_ptr, const int32_t* __restrict__ node_start, Table t,
-              int32_t* __restrict__ cand) {
-  if (a.s > top_level(a.meta)) return;
+              const uint8_t* __restrict__ act_in, int32_t* __restrict__ cand) {
+  const int top = top_level(a.meta);
+  if (a.s > top) return;
   const uint64_t* key = sorted_keys(a.sp, a.bits);
   const int bpa = a.meta->bpa;
   const int nodes = *count_ptr;
@@ -397,30 +461,97 @@ __global__ void __launch_bounds__(256)
   const int64_t warps = static_cast<int64_t>(gridDim.x) * (blockDim.x >> 5);
   for (int64_t c = static_cast<int64_t>(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5);
        c < nodes; c += warps) {
-    const uint64_t nk = key[node_start[c]] >> (3 * a.s);
+    const int32_t st = node_start[c];
+    if (a.s < top) {
+      const int32_t len = node_start[c + 1] - st;
+      if (len <= kScanActive) {
+        bool any = false;
+#pragma unroll
+        for (int i = 0; i < kScanActive / 32; ++i) {
+          const int j = lane + 32 * i;
+          any |= j < len && act_in[st + j] != 0;
+        }
+        if (!__any_sync(kFull, any)) continue;
+      }
+    }
+    const uint64_t nk = key[st] >> (3 * a.s);
     const int len = lane < kNeighbours ? neighbour_run(t, nk, a.s, bpa, lane).y : 0;
     const int total = __reduce_add_sync(kFull, len);
     if (lane == 0) cand[c] = total;
   }
 }
 
-// One step of the coarse-to-fine level selection.
+// New (level, active) of sorted position q after the step at level s; only
+// points still active read their node's count.
+__device__ __forceinline__ void select_step(int64_t q, int s, int top,
+                                            const int32_t* __restrict__ node_of,
+                                            const int32_t* __restrict__ cand,
+                                            const uint8_t* __restrict__ sel_in,
+                                            const uint8_t* __restrict__ act_in, int min_count,
+                                            int max_count, uint8_t* sel_new, uint8_t* act_new) {
+  if (s == top) {
+    *sel_new = static_cast<uint8_t>(top);
+    *act_new = cand[node_of[q]] > max_count;
+  } else if (act_in[q]) {
+    const int cnt = cand[node_of[q]];
+    const bool use = cnt >= min_count;
+    *sel_new = use ? static_cast<uint8_t>(s) : sel_in[q];
+    *act_new = use && cnt > max_count;
+  } else {
+    *sel_new = sel_in[q];
+    *act_new = 0;
+  }
+}
+
+// One step of the coarse-to-fine level selection, fused with the
+// finalisation of level s+1: points whose selection stays at s+1 open their
+// query groups there (a group is a maximal run of sorted positions with the
+// same level and level-(s+1) node) and write the group's 27 runs (row p).
+// The new selection goes to sel_out / act_out, the previous one is read from
+// sel_in / act_in, so a warp can recompute its left neighbour's new level
+// without racing the warp that writes it.  One warp per 32 positions.
 __global__ void __launch_bounds__(256)
     ka_select(LevelArgs a, const int32_t* __restrict__ node_of, const int32_t* __restrict__ cand,
-              int min_count, int max_count, uint8_t* __restrict__ sel,
-              uint8_t* __restrict__ active) {
+              int min_count, int max_count, const uint8_t* __restrict__ sel_in,
+              const uint8_t* __restrict__ act_in, uint8_t* __restrict__ sel_out,
+              uint8_t* __restrict__ act_out, Table t_up, uint8_t* __restrict__ group_flag,
+              int2* __restrict__ runs) {
   const int top = top_level(a.meta);
   if (a.s > top) return;
-  const int64_t p = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (p >= a.n) return;
-  const int cnt = cand[node_of[p]];
-  if (a.s == top) {
-    sel[p] = static_cast<uint8_t>(top);
-    active[p] = cnt > max_count;
-  } else {
-    const bool use = active[p] && cnt >= min_count;
-    if (use) sel[p] = static_cast<uint8_t>(a.s);
-    active[p] = use && cnt > max_count;
+  const uint64_t* key = sorted_keys(a.sp, a.bits);
+  const int bpa = a.meta->bpa;
+  const int L = a.s + 1;  // level finalised here (when <= top)
+  const int lane = threadIdx.x & 31;
+  const int64_t warps = static_cast<int64_t>(gridDim.x) * (blockDim.x >> 5);
+  for (int64_t base = (static_cast<int64_t>(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5)) * 32;
+       base < a.n; base += warps * 32) {
+    const int64_t p = base + lane;
+    uint8_t ns = 0xff, na = 0;
+    if (p < a.n) {
+      select_step(p, a.s, top, node_of, cand, sel_in, act_in, min_count, max_count, &ns, &na);
+      sel_out[p] = ns;
+      act_out[p] = na;
+    }
+    if (L > top) continue;
+    uint8_t prev = static_cast<uint8_t>(__shfl_up_sync(kFull, ns, 1));
+    if (lane == 0 && p > 0 && p < a.n) {  // the previous warp's last position
+      uint8_t pa;
+      select_step(p - 1, a.s, top, node_of, cand, sel_in, act_in, min_count, max_count, &prev,
+                  &pa);
+    }
+    bool start = false;
+    if (p < a.n && ns == L) {
+      start = p == 0 || prev != L || node_head(key, p, 3 * L);
+      group_flag[p] = start ? 1 : 0;
+    }
+    uint32_t starts = __ballot_sync(kFull, start);
+    while (starts) {
+      const int src = __ffs(starts) - 1;
+      starts &= starts - 1;
+      const int64_t ps = base + src;
+      if (lane < kNeighbours)
+        runs[ps * kNeighbours + lane] = neighbour_run(t_up, key[ps] >> (3 * L), L, bpa, lane);
+    }
   }
 }
 
@@ -454,16 +585,6 @@ __global__ void __launch_bounds__(256)
         runs[ps * kNeighbours + lane] = neighbour_run(t, key[ps] >> (3 * L), L, bpa, lane);
     }
   }
-}
-
-__global__ void __launch_bounds__(256)
-    ka_erase(LevelArgs a, int L, const int* count_ptr, const int32_t* __restrict__ slot_of,
-             uint64_t* __restrict__ table_keys) {
-  if (L > top_level(a.meta)) return;
-  const int nodes = *count_ptr;
-  for (int64_t c = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; c < nodes;
-       c += static_cast<int64_t>(gridDim.x) * blockDim.x)
-    table_keys[slot_of[c]] = kEmptyKey;
 }
 
 // ------------------------------------------------------------------ groups
@@ -535,11 +656,10 @@ struct ABufs {
   int32_t* cand;
   int32_t* slot_of[2];
   int* level_nodes;  // [kMaxLevel + 1]
-  uint8_t* sel;
-  uint8_t* active;
+  uint8_t* sel[2];     // selection of the previous / current level (ping-pong by level parity)
+  uint8_t* active[2];
   uint8_t* group_flag;
-  uint64_t* tkeys[2];
-  int2* tvals[2];
+  Slot* tslots[2];
   int64_t cap;
   int2* runs;
   int32_t* group_start;
@@ -560,7 +680,8 @@ ABufs alayout(void* ws, int64_t n, size_t* bytes) {
   b.vals[1] = a.take<uint32_t>(n);
   b.hist = a.take<uint32_t>(sort_hist_elems(n));
   b.totals = a.take<uint32_t>(kSortMaxPasses * 256);
-  b.tile_counts = a.take<uint32_t>(static_cast<size_t>(ceil_div(n > 0 ? n : 1, kTile)));
+  b.tile_counts = a.take<uint32_t>(static_cast<size_t>(kMaxLevel + 1) *
+                                   static_cast<size_t>(ceil_div(n > 0 ? n : 1, kTile)));
   b.rec = a.take<float4>(n);
   b.node_of = a.take<int32_t>(n);
   b.node_start = a.take<int32_t>(n + 1);
@@ -568,14 +689,15 @@ ABufs alayout(void* ws, int64_t n, size_t* bytes) {
   b.slot_of[0] = a.take<int32_t>(n);
   b.slot_of[1] = a.take<int32_t>(n);
   b.level_nodes = a.take<int>(kMaxLevel + 1);
-  b.sel = a.take<uint8_t>(n);
-  b.active = a.take<uint8_t>(n);
+  for (int h = 0; h < 2; ++h) {
+    b.sel[h] = a.take<uint8_t>(n);
+    b.active[h] = a.take<uint8_t>(n);
+  }
   b.group_flag = a.take<uint8_t>(n);
   b.cap = 16;
   while (b.cap < 2 * n) b.cap <<= 1;
   for (int h = 0; h < 2; ++h) {
-    b.tkeys[h] = a.take<uint64_t>(b.cap);
-    b.tvals[h] = a.take<int2>(b.cap);
+    b.tslots[h] = a.take<Slot>(b.cap);
   }
   b.runs = a.take<int2>(static_cast<size_t>(n) * kNeighbours);
   b.group_start = a.take<int32_t>(n + 1);
@@ -615,8 +737,8 @@ int run_adaptive(const AdaptiveArgs& f, void* ws, size_t ws_bytes, const QuerySh
     return FKNN_OK;
   }
   int nl = 0;
-  cudaError_t e = cudaMemsetAsync(b.tkeys[0], 0xff, sizeof(uint64_t) * b.cap, s);
-  if (e == cudaSuccess) e = cudaMemsetAsync(b.tkeys[1], 0xff, sizeof(uint64_t) * b.cap, s);
+  cudaError_t e = cudaMemsetAsync(b.tslots[0], 0xff, sizeof(Slot) * b.cap, s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(b.tslots[1], 0xff, sizeof(Slot) * b.cap, s);
   if (e == cudaSuccess) e = cudaMemsetAsync(b.group_flag, 0, static_cast<size_t>(n), s);
   if (e != cudaSuccess) {
     note_cuda_error(e);
@@ -639,39 +761,42 @@ int run_adaptive(const AdaptiveArgs& f, void* ws, size_t ws_bytes, const QuerySh
   const int tiles = blocks_for(n, kTile);
   const int min_count = f.min_factor * f.k, max_count = f.max_factor * f.k;
   const int top_host = f.max_shift >= 0 ? f.max_shift : kMaxLevel;
-  const Table tab[2] = {{b.tkeys[0], b.tvals[0], static_cast<uint32_t>(b.cap - 1)},
-                        {b.tkeys[1], b.tvals[1], static_cast<uint32_t>(b.cap - 1)}};
+  const Table tab[2] = {{b.tslots[0], static_cast<uint32_t>(b.cap - 1)},
+                        {b.tslots[1], static_cast<uint32_t>(b.cap - 1)}};
+  {
+    const LevelArgs la{sp, key_bits, b.meta, n, 0};
+    ka_heads_all<<<tiles, 256, 0, s>>>(la, tiles, b.tile_counts);
+    ka_scan_all<<<kMaxLevel + 1, 1024, 0, s>>>(b.tile_counts, tiles, b.level_nodes);
+    nl += 2;
+  }
   for (int lv = top_host; lv >= 0; --lv) {
     const LevelArgs la{sp, key_bits, b.meta, n, lv};
     int* nodes = b.level_nodes + lv;
-    ka_heads<<<tiles, 256, 0, s>>>(la, b.tile_counts);
-    k_scan_tiles<<<1, 1024, 0, s>>>(b.tile_counts, tiles, nodes);
-    ka_nodes<<<tiles, 256, 0, s>>>(la, b.tile_counts, nodes, b.node_of, b.node_start);
+    const int* stale = b.level_nodes + (lv + 2 <= kMaxLevel ? lv + 2 : kMaxLevel);
+    ka_nodes<<<tiles, 256, 0, s>>>(la, b.tile_counts + static_cast<int64_t>(lv) * tiles, nodes,
+                                   b.node_of, b.node_start, stale, b.slot_of[lv & 1],
+                                   b.tslots[lv & 1]);
     ka_insert<<<capped_blocks(n), 256, 0, s>>>(la, nodes, b.node_start, tab[lv & 1],
                                                b.slot_of[lv & 1]);
-    ka_counts<<<capped_blocks(n * 32), 256, 0, s>>>(la, nodes, b.node_start, tab[lv & 1], b.cand);
-    ka_select<<<blocks_for(n, 256), 256, 0, s>>>(la, b.node_of, b.cand, min_count, max_count,
-                                                 b.sel, b.active);
-    nl += 6;
-    if (lv < top_host) {
-      const int up = lv + 1;
-      ka_finalize<<<capped_blocks(n), 256, 0, s>>>(la, up, tab[up & 1], b.sel, b.group_flag,
-                                                    b.runs);
-      ka_erase<<<capped_blocks(n), 256, 0, s>>>(la, up, b.level_nodes + up, b.slot_of[up & 1],
-                                                b.tkeys[up & 1]);
-      nl += 2;
-    }
+    const int up = lv + 1;
+    ka_counts<<<capped_blocks(n * 32), 256, 0, s>>>(la, nodes, b.node_start, tab[lv & 1],
+                                                     b.active[up & 1], b.cand);
+    ka_select<<<capped_blocks(n), 256, 0, s>>>(la, b.node_of, b.cand, min_count, max_count,
+                                               b.sel[up & 1], b.active[up & 1], b.sel[lv & 1],
+                                               b.active[lv & 1], tab[up & 1], b.group_flag,
+                                               b.runs);
+    nl += 4;
   }
   {
     const LevelArgs la{sp, key_bits, b.meta, n, 0};
-    ka_finalize<<<capped_blocks(n), 256, 0, s>>>(la, 0, tab[0], b.sel, b.group_flag, b.runs);
+    ka_finalize<<<capped_blocks(n), 256, 0, s>>>(la, 0, tab[0], b.sel[0], b.group_flag, b.runs);
     ka_group_tiles<<<tiles, 256, 0, s>>>(n, b.group_flag, b.tile_counts);
     k_scan_tiles<<<1, 1024, 0, s>>>(b.tile_counts, tiles, &b.meta->n_groups);
     ka_groups<<<tiles, 256, 0, s>>>(n, b.group_flag, b.tile_counts, &b.meta->n_groups,
                                     b.group_start, b.group_row);
     nl += 4;
     if (f.level_out) {
-      ka_levels_out<<<blocks_for(n, 256), 256, 0, s>>>(n, b.rec, b.sel, f.level_out);
+      ka_levels_out<<<blocks_for(n, 256), 256, 0, s>>>(n, b.rec, b.sel[0], f.level_out);
       ++nl;
     }
   }

@@ -355,6 +355,12 @@ __device__ __forceinline__ int axis_offset(int position) {
 // only the used prefix is cleared on every call.
 constexpr uint64_t kHashEmpty = ~0ull;
 
+// One 16-byte slot: cell key and the cell's run, so a probe is one load.
+struct __align__(16) HashSlot {
+  uint64_t key;
+  int2 run;
+};
+
 __device__ __forceinline__ uint32_t hash_capacity(int cells) {
   uint32_t cap = 16;
   while (cap < 2u * static_cast<uint32_t>(cells)) cap <<= 1;
@@ -370,17 +376,17 @@ __device__ __forceinline__ uint32_t hash_slot(uint64_t key, uint32_t mask) {
   return static_cast<uint32_t>(key) & mask;
 }
 
-__global__ void k_hash_clear(const int* cell_count_ptr, uint64_t* __restrict__ hkeys) {
+__global__ void k_hash_clear(const int* cell_count_ptr, HashSlot* __restrict__ table) {
   const uint32_t cap = hash_capacity(*cell_count_ptr);
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < cap; i += gridDim.x * blockDim.x)
-    hkeys[i] = kHashEmpty;
+    table[i].key = kHashEmpty;
 }
 
 // Value = the cell's candidate run (start, count), so a lookup needs no
 // further load of the cell starts.
 __global__ void k_hash_insert(const uint64_t* __restrict__ cell_key, const int* cell_count_ptr,
-                              const int32_t* __restrict__ cell_start, uint64_t* __restrict__ hkeys,
-                              int2* __restrict__ hvals) {
+                              const int32_t* __restrict__ cell_start,
+                              HashSlot* __restrict__ table) {
   const int cells = *cell_count_ptr;
   const uint32_t mask = hash_capacity(cells) - 1;
   for (int64_t c = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; c < cells;
@@ -389,9 +395,9 @@ __global__ void k_hash_insert(const uint64_t* __restrict__ cell_key, const int* 
     uint32_t h = hash_slot(key, mask);
     for (uint32_t probe = 0; probe <= mask; ++probe) {
       const unsigned long long prev = atomicCAS(
-          reinterpret_cast<unsigned long long*>(hkeys + h), kHashEmpty, key);
+          reinterpret_cast<unsigned long long*>(&table[h].key), kHashEmpty, key);
       if (prev == kHashEmpty || prev == key) {
-        hvals[h] = make_int2(cell_start[c], cell_start[c + 1] - cell_start[c]);
+        table[h].run = make_int2(cell_start[c], cell_start[c + 1] - cell_start[c]);
         break;
       }
       h = (h + 1) & mask;
@@ -399,13 +405,14 @@ __global__ void k_hash_insert(const uint64_t* __restrict__ cell_key, const int* 
   }
 }
 
-__device__ __forceinline__ int2 hash_find(const uint64_t* hkeys, const int2* hvals,
-                                             uint32_t mask, uint64_t key) {
+__device__ __forceinline__ int2 hash_find(const HashSlot* table, uint32_t mask, uint64_t key) {
   uint32_t h = hash_slot(key, mask);
   for (uint32_t probe = 0; probe <= mask; ++probe) {
-    const uint64_t k = hkeys[h];
-    if (k == key) return hvals[h];
-    if (k == kHashEmpty) break;
+    const ulonglong2 v = __ldg(reinterpret_cast<const ulonglong2*>(table + h));
+    if (v.x == key)
+      return make_int2(static_cast<int>(static_cast<uint32_t>(v.y)),
+                       static_cast<int>(static_cast<uint32_t>(v.y >> 32)));
+    if (v.x == kHashEmpty) break;
     h = (h + 1) & mask;
   }
   return make_int2(0, 0);  // no such cell: an empty run
@@ -416,8 +423,7 @@ __device__ __forceinline__ int2 hash_find(const uint64_t* hkeys, const int2* hva
 // offset j, or (0, 0) when that cell is empty.
 __global__ void __launch_bounds__(256)
     k_runs(const uint64_t* __restrict__ group_key, const int* group_count_ptr,
-           const uint64_t* __restrict__ hkeys, const int2* __restrict__ hvals,
-           const int* cell_count_ptr, const Meta* meta,
+           const HashSlot* __restrict__ table, const int* cell_count_ptr, const Meta* meta,
            int2* __restrict__ runs) {
   const int64_t total = static_cast<int64_t>(*group_count_ptr) * kNeighbours;
   const int bpa = meta->bpa;
@@ -439,7 +445,7 @@ __global__ void __launch_bounds__(256)
       const uint64_t nk = (cloud << (3 * bpa)) |
                           morton3(static_cast<uint32_t>(x), static_cast<uint32_t>(y),
                                   static_cast<uint32_t>(z));
-      run = hash_find(hkeys, hvals, hmask, nk);
+      run = hash_find(table, hmask, nk);
     }
     runs[t] = run;
   }
@@ -533,8 +539,7 @@ struct Bufs {
   int4* items;
   int32_t* cands;
   uint32_t* seg_counts;
-  uint64_t* hkeys;
-  int2* hvals;
+  HashSlot* hslots;
   int64_t hash_cap;
 };
 
@@ -562,8 +567,7 @@ Bufs layout(void* ws, int64_t n, int64_t m, int64_t n_clouds, int kind, size_t* 
   b.cell_start = a.take<int32_t>(n + 1);
   b.hash_cap = 16;
   while (b.hash_cap < 2 * n) b.hash_cap <<= 1;
-  b.hkeys = a.take<uint64_t>(b.hash_cap);
-  b.hvals = a.take<int2>(b.hash_cap);
+  b.hslots = a.take<HashSlot>(b.hash_cap);
   if (kind == FKNN_QUERY_SELECTED) {
     b.pos_of = a.take<int32_t>(n);
     b.cell_of = a.take<int32_t>(n);
@@ -658,9 +662,9 @@ int run_fused(const FusedArgs& f, void* ws, size_t ws_bytes, const QueryShape& s
     k_cells<uint64_t><<<tiles, 256, 0, s>>>(n, sp64, key_bits, b.tile_counts,
                                             &b.meta->n_cells, b.cell_key, b.cell_start, b.cell_of);
     k_hash_clear<<<static_cast<int>(b.hash_cap < 1024 * 256 ? ceil_div(b.hash_cap, 256) : 1024), 256, 0,
-                   s>>>(&b.meta->n_cells, b.hkeys);
+                   s>>>(&b.meta->n_cells, b.hslots);
     k_hash_insert<<<capped_blocks(n), 256, 0, s>>>(b.cell_key, &b.meta->n_cells, b.cell_start,
-                                                     b.hkeys, b.hvals);
+                                                     b.hslots);
     nl += 5;
   }
 
@@ -676,7 +680,7 @@ int run_fused(const FusedArgs& f, void* ws, size_t ws_bytes, const QueryShape& s
   if (kind == FKNN_QUERY_SELF) {
     if (n > 0) {
       k_runs<<<capped_blocks(n * kNeighbours), 256, 0, s>>>(
-          b.cell_key, &b.meta->n_cells, b.hkeys, b.hvals, &b.meta->n_cells, b.meta,
+          b.cell_key, &b.meta->n_cells, b.hslots, &b.meta->n_cells, b.meta,
           b.runs);
       ++nl;
       nl += launch_items(b.runs, b.cell_start, nullptr, &b.meta->n_cells, n, shape.tile_records,
@@ -692,7 +696,7 @@ int run_fused(const FusedArgs& f, void* ws, size_t ws_bytes, const QueryShape& s
     group_count_ptr = &b.meta->n_groups;
     if (n > 0) {
       k_runs<<<capped_blocks(n * kNeighbours), 256, 0, s>>>(
-          b.cell_key, &b.meta->n_cells, b.hkeys, b.hvals, &b.meta->n_cells, b.meta,
+          b.cell_key, &b.meta->n_cells, b.hslots, &b.meta->n_cells, b.meta,
           b.runs);
       ++nl;
     }
@@ -738,7 +742,7 @@ int run_fused(const FusedArgs& f, void* ws, size_t ws_bytes, const QueryShape& s
                                               &b.meta->n_groups, b.group_key, b.group_start,
                                               nullptr);
       k_runs<<<capped_blocks(m * kNeighbours), 256, 0, s>>>(
-          b.group_key, &b.meta->n_groups, b.hkeys, b.hvals, &b.meta->n_cells,
+          b.group_key, &b.meta->n_groups, b.hslots, &b.meta->n_cells,
           b.meta, b.runs);
       nl += 4;
       nl += launch_items(b.runs, b.group_start, nullptr, &b.meta->n_groups, m, shape.tile_records,
