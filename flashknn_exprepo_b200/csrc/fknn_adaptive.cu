@@ -98,12 +98,12 @@ __device__ __forceinline__ int2 table_find(const Table& t, uint64_t key) {
 
 __device__ __forceinline__ const uint64_t* sorted_keys(const SortPair<uint64_t>& sp,
                                                        const int* bits) {
-  return sp.keys[sort_passes_for_bits(*bits) & 1];
+  return (sort_passes_for_bits(*bits) & 1) ? sp.keys[1] : sp.keys[0];
 }
 
 __device__ __forceinline__ const uint32_t* sorted_vals(const SortPair<uint64_t>& sp,
                                                        const int* bits) {
-  return sp.vals[sort_passes_for_bits(*bits) & 1];
+  return (sort_passes_for_bits(*bits) & 1) ? sp.vals[1] : sp.vals[0];
 }
 
 __device__ __forceinline__ bool node_head(const uint64_t* key, int64_t p, int shift) {
@@ -371,27 +371,21 @@ __global__ void __launch_bounds__(1024)
   if (threadIdx.x == 0) level_nodes[blockIdx.x] = static_cast<int>(carry);
 }
 
+// ---- per-level passes (device functions over an explicit tile, thread or
+// warp range; the kernels below launch them, four per level).  Arrays that a
+// pass rewrites on every level (node starts, node of, counts, selection,
+// slots) are read with ld.global.cg, straight from L2.
+
+// Positions of tile `tile` (kTile of them, 8 per thread of a 256-thread CTA):
 // node_of[p] = node of sorted position p at level s; node_start[c] = first
-// position of node c, node_start[count] = n.
-// Also empties the table this level is about to reuse: it still holds the
-// nodes of level s+2 (erase_count of them, at erase_slot), whose last reader
-// was the finalisation of level s+2 in the previous step.
-__global__ void __launch_bounds__(256)
-    ka_nodes(LevelArgs a, const uint32_t* __restrict__ tile_offsets, const int* count_ptr,
-             int32_t* __restrict__ node_of, int32_t* __restrict__ node_start,
-             const int* erase_count, const int32_t* __restrict__ erase_slot,
-             Slot* __restrict__ table) {
-  __shared__ uint32_t warp_sums[32];
-  const int top = top_level(a.meta);
-  if (a.s > top) return;
-  if (a.s + 2 <= top) {
-    const int stale = *erase_count;
-    for (int64_t c = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; c < stale;
-         c += static_cast<int64_t>(gridDim.x) * blockDim.x)
-      table[erase_slot[c]].key = kEmptyKey;
-  }
+// position of node c, node_start[nodes] = n.  Called by every thread of the
+// CTA (block-wide scan).
+__device__ __forceinline__ void nodes_tile(const LevelArgs& a, int tile,
+                                           const uint32_t* __restrict__ tile_offsets, int nodes,
+                                           int32_t* __restrict__ node_of,
+                                           int32_t* __restrict__ node_start, uint32_t* warp_sums) {
   const uint64_t* key = sorted_keys(a.sp, a.bits);
-  const int64_t base = static_cast<int64_t>(blockIdx.x) * kTile + threadIdx.x * 8;
+  const int64_t base = static_cast<int64_t>(tile) * kTile + threadIdx.x * 8;
   uint32_t flags = 0, heads = 0;
 #pragma unroll
   for (int r = 0; r < 8; ++r) {
@@ -402,7 +396,7 @@ __global__ void __launch_bounds__(256)
     }
   }
   const uint32_t incl = block_inclusive_scan(heads, warp_sums, nullptr);
-  int c = static_cast<int>(tile_offsets[blockIdx.x] + incl - heads) - 1;
+  int c = static_cast<int>(tile_offsets[tile] + incl - heads) - 1;
 #pragma unroll
   for (int r = 0; r < 8; ++r) {
     const int64_t p = base + r;
@@ -412,32 +406,37 @@ __global__ void __launch_bounds__(256)
       node_start[c] = static_cast<int32_t>(p);
     }
     node_of[p] = c;
-    if (p == a.n - 1) node_start[*count_ptr] = static_cast<int32_t>(a.n);
+    if (p == a.n - 1) node_start[nodes] = static_cast<int32_t>(a.n);
   }
 }
 
+// Empties the `stale` slots listed in slot_of (the nodes a table held two
+// levels up), so the table can take this level's nodes.
+__device__ __forceinline__ void erase_nodes(int64_t t, int64_t stride, int stale,
+                                            const int32_t* __restrict__ slot_of,
+                                            Slot* __restrict__ table) {
+  for (int64_t c = t; c < stale; c += stride) table[__ldcg(slot_of + c)].key = kEmptyKey;
+}
+
 // Node key -> (start, count) into the table of this level; the slot is kept
-// for the erase.
-__global__ void __launch_bounds__(256)
-    ka_insert(LevelArgs a, const int* count_ptr, const int32_t* __restrict__ node_start, Table t,
-              int32_t* __restrict__ slot_of) {
-  if (a.s > top_level(a.meta)) return;
+// for the erase.  One thread per node.
+__device__ __forceinline__ void insert_nodes(const LevelArgs& a, int64_t t, int64_t stride,
+                                             int nodes, const int32_t* __restrict__ node_start,
+                                             const Table& tab, int32_t* __restrict__ slot_of) {
   const uint64_t* key = sorted_keys(a.sp, a.bits);
-  const int nodes = *count_ptr;
-  for (int64_t c = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; c < nodes;
-       c += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    const int32_t st = node_start[c];
+  for (int64_t c = t; c < nodes; c += stride) {
+    const int32_t st = __ldcg(node_start + c);
     const uint64_t nk = key[st] >> (3 * a.s);
-    uint32_t h = slot_of_key(nk, t.mask);
-    for (uint32_t probe = 0; probe <= t.mask; ++probe) {
+    uint32_t h = slot_of_key(nk, tab.mask);
+    for (uint32_t probe = 0; probe <= tab.mask; ++probe) {
       const unsigned long long prev =
-          atomicCAS(reinterpret_cast<unsigned long long*>(&t.slots[h].key), kEmptyKey, nk);
+          atomicCAS(reinterpret_cast<unsigned long long*>(&tab.slots[h].key), kEmptyKey, nk);
       if (prev == kEmptyKey) {
-        t.slots[h].run = make_int2(st, node_start[c + 1] - st);
+        tab.slots[h].run = make_int2(st, __ldcg(node_start + c + 1) - st);
         slot_of[c] = static_cast<int32_t>(h);
         break;
       }
-      h = (h + 1) & t.mask;
+      h = (h + 1) & tab.mask;
     }
   }
 }
@@ -449,33 +448,30 @@ __global__ void __launch_bounds__(256)
 // flags) is skipped.
 constexpr int kScanActive = 128;
 
-__global__ void __launch_bounds__(256)
-    ka_counts(LevelArgs a, const int* count_ptr, const int32_t* __restrict__ node_start, Table t,
-              const uint8_t* __restrict__ act_in, int32_t* __restrict__ cand) {
-  const int top = top_level(a.meta);
-  if (a.s > top) return;
+__device__ __forceinline__ void count_nodes(const LevelArgs& a, int top, int64_t w,
+                                            int64_t wstride, int nodes,
+                                            const int32_t* __restrict__ node_start,
+                                            const Table& tab, const uint8_t* __restrict__ act_in,
+                                            int32_t* __restrict__ cand) {
   const uint64_t* key = sorted_keys(a.sp, a.bits);
   const int bpa = a.meta->bpa;
-  const int nodes = *count_ptr;
   const int lane = threadIdx.x & 31;
-  const int64_t warps = static_cast<int64_t>(gridDim.x) * (blockDim.x >> 5);
-  for (int64_t c = static_cast<int64_t>(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5);
-       c < nodes; c += warps) {
-    const int32_t st = node_start[c];
+  for (int64_t c = w; c < nodes; c += wstride) {
+    const int32_t st = __ldcg(node_start + c);
     if (a.s < top) {
-      const int32_t len = node_start[c + 1] - st;
+      const int32_t len = __ldcg(node_start + c + 1) - st;
       if (len <= kScanActive) {
         bool any = false;
 #pragma unroll
         for (int i = 0; i < kScanActive / 32; ++i) {
           const int j = lane + 32 * i;
-          any |= j < len && act_in[st + j] != 0;
+          any |= j < len && __ldcg(act_in + st + j) != 0;
         }
         if (!__any_sync(kFull, any)) continue;
       }
     }
     const uint64_t nk = key[st] >> (3 * a.s);
-    const int len = lane < kNeighbours ? neighbour_run(t, nk, a.s, bpa, lane).y : 0;
+    const int len = lane < kNeighbours ? neighbour_run(tab, nk, a.s, bpa, lane).y : 0;
     const int total = __reduce_add_sync(kFull, len);
     if (lane == 0) cand[c] = total;
   }
@@ -491,17 +487,30 @@ __device__ __forceinline__ void select_step(int64_t q, int s, int top,
                                             int max_count, uint8_t* sel_new, uint8_t* act_new) {
   if (s == top) {
     *sel_new = static_cast<uint8_t>(top);
-    *act_new = cand[node_of[q]] > max_count;
-  } else if (act_in[q]) {
-    const int cnt = cand[node_of[q]];
+    *act_new = __ldcg(cand + __ldcg(node_of + q)) > max_count;
+  } else if (__ldcg(act_in + q)) {
+    const int cnt = __ldcg(cand + __ldcg(node_of + q));
     const bool use = cnt >= min_count;
-    *sel_new = use ? static_cast<uint8_t>(s) : sel_in[q];
+    *sel_new = use ? static_cast<uint8_t>(s) : __ldcg(sel_in + q);
     *act_new = use && cnt > max_count;
   } else {
-    *sel_new = sel_in[q];
+    *sel_new = __ldcg(sel_in + q);
     *act_new = 0;
   }
 }
+
+struct SelectArgs {
+  const int32_t* node_of;
+  const int32_t* cand;
+  int min_count, max_count;
+  const uint8_t* sel_in;
+  const uint8_t* act_in;
+  uint8_t* sel_out;
+  uint8_t* act_out;
+  Table t_up;  // table of level s + 1
+  uint8_t* group_flag;
+  int2* runs;
+};
 
 // One step of the coarse-to-fine level selection, fused with the
 // finalisation of level s+1: points whose selection stays at s+1 open their
@@ -510,39 +519,32 @@ __device__ __forceinline__ void select_step(int64_t q, int s, int top,
 // The new selection goes to sel_out / act_out, the previous one is read from
 // sel_in / act_in, so a warp can recompute its left neighbour's new level
 // without racing the warp that writes it.  One warp per 32 positions.
-__global__ void __launch_bounds__(256)
-    ka_select(LevelArgs a, const int32_t* __restrict__ node_of, const int32_t* __restrict__ cand,
-              int min_count, int max_count, const uint8_t* __restrict__ sel_in,
-              const uint8_t* __restrict__ act_in, uint8_t* __restrict__ sel_out,
-              uint8_t* __restrict__ act_out, Table t_up, uint8_t* __restrict__ group_flag,
-              int2* __restrict__ runs) {
-  const int top = top_level(a.meta);
-  if (a.s > top) return;
+__device__ __forceinline__ void select_positions(const LevelArgs& a, int top, int64_t w,
+                                                 int64_t wstride, const SelectArgs& g) {
   const uint64_t* key = sorted_keys(a.sp, a.bits);
   const int bpa = a.meta->bpa;
   const int L = a.s + 1;  // level finalised here (when <= top)
   const int lane = threadIdx.x & 31;
-  const int64_t warps = static_cast<int64_t>(gridDim.x) * (blockDim.x >> 5);
-  for (int64_t base = (static_cast<int64_t>(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5)) * 32;
-       base < a.n; base += warps * 32) {
+  for (int64_t base = w * 32; base < a.n; base += wstride * 32) {
     const int64_t p = base + lane;
     uint8_t ns = 0xff, na = 0;
     if (p < a.n) {
-      select_step(p, a.s, top, node_of, cand, sel_in, act_in, min_count, max_count, &ns, &na);
-      sel_out[p] = ns;
-      act_out[p] = na;
+      select_step(p, a.s, top, g.node_of, g.cand, g.sel_in, g.act_in, g.min_count, g.max_count,
+                  &ns, &na);
+      g.sel_out[p] = ns;
+      g.act_out[p] = na;
     }
     if (L > top) continue;
     uint8_t prev = static_cast<uint8_t>(__shfl_up_sync(kFull, ns, 1));
     if (lane == 0 && p > 0 && p < a.n) {  // the previous warp's last position
       uint8_t pa;
-      select_step(p - 1, a.s, top, node_of, cand, sel_in, act_in, min_count, max_count, &prev,
-                  &pa);
+      select_step(p - 1, a.s, top, g.node_of, g.cand, g.sel_in, g.act_in, g.min_count,
+                  g.max_count, &prev, &pa);
     }
     bool start = false;
     if (p < a.n && ns == L) {
       start = p == 0 || prev != L || node_head(key, p, 3 * L);
-      group_flag[p] = start ? 1 : 0;
+      g.group_flag[p] = start ? 1 : 0;
     }
     uint32_t starts = __ballot_sync(kFull, start);
     while (starts) {
@@ -550,9 +552,53 @@ __global__ void __launch_bounds__(256)
       starts &= starts - 1;
       const int64_t ps = base + src;
       if (lane < kNeighbours)
-        runs[ps * kNeighbours + lane] = neighbour_run(t_up, key[ps] >> (3 * L), L, bpa, lane);
+        g.runs[ps * kNeighbours + lane] = neighbour_run(g.t_up, key[ps] >> (3 * L), L, bpa, lane);
     }
   }
+}
+
+// ---- per-level kernels
+
+// Also empties the table this level is about to reuse: it still holds the
+// nodes of level s+2 (erase_count of them, at erase_slot), whose last reader
+// was the finalisation of level s+2 in the previous step.
+__global__ void __launch_bounds__(256)
+    ka_nodes(LevelArgs a, const uint32_t* __restrict__ tile_offsets, const int* count_ptr,
+             int32_t* __restrict__ node_of, int32_t* __restrict__ node_start,
+             const int* erase_count, const int32_t* __restrict__ erase_slot,
+             Slot* __restrict__ table) {
+  __shared__ uint32_t warp_sums[32];
+  const int top = top_level(a.meta);
+  if (a.s > top) return;
+  if (a.s + 2 <= top)
+    erase_nodes(static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x,
+                static_cast<int64_t>(gridDim.x) * blockDim.x, *erase_count, erase_slot, table);
+  nodes_tile(a, blockIdx.x, tile_offsets, *count_ptr, node_of, node_start, warp_sums);
+}
+
+__global__ void __launch_bounds__(256)
+    ka_insert(LevelArgs a, const int* count_ptr, const int32_t* __restrict__ node_start, Table t,
+              int32_t* __restrict__ slot_of) {
+  if (a.s > top_level(a.meta)) return;
+  insert_nodes(a, static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x,
+               static_cast<int64_t>(gridDim.x) * blockDim.x, *count_ptr, node_start, t, slot_of);
+}
+
+__global__ void __launch_bounds__(256)
+    ka_counts(LevelArgs a, const int* count_ptr, const int32_t* __restrict__ node_start, Table t,
+              const uint8_t* __restrict__ act_in, int32_t* __restrict__ cand) {
+  const int top = top_level(a.meta);
+  if (a.s > top) return;
+  count_nodes(a, top, (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5,
+              (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5, *count_ptr, node_start, t,
+              act_in, cand);
+}
+
+__global__ void __launch_bounds__(256) ka_select(LevelArgs a, SelectArgs g) {
+  const int top = top_level(a.meta);
+  if (a.s > top) return;
+  select_positions(a, top, (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5,
+                   (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5, g);
 }
 
 // Points whose selection stopped at level L open their query groups: a
@@ -773,18 +819,15 @@ int run_adaptive(const AdaptiveArgs& f, void* ws, size_t ws_bytes, const QuerySh
     const LevelArgs la{sp, key_bits, b.meta, n, lv};
     int* nodes = b.level_nodes + lv;
     const int* stale = b.level_nodes + (lv + 2 <= kMaxLevel ? lv + 2 : kMaxLevel);
+    const int h = lv & 1, up = (lv + 1) & 1;
     ka_nodes<<<tiles, 256, 0, s>>>(la, b.tile_counts + static_cast<int64_t>(lv) * tiles, nodes,
-                                   b.node_of, b.node_start, stale, b.slot_of[lv & 1],
-                                   b.tslots[lv & 1]);
-    ka_insert<<<capped_blocks(n), 256, 0, s>>>(la, nodes, b.node_start, tab[lv & 1],
-                                               b.slot_of[lv & 1]);
-    const int up = lv + 1;
-    ka_counts<<<capped_blocks(n * 32), 256, 0, s>>>(la, nodes, b.node_start, tab[lv & 1],
-                                                     b.active[up & 1], b.cand);
-    ka_select<<<capped_blocks(n), 256, 0, s>>>(la, b.node_of, b.cand, min_count, max_count,
-                                               b.sel[up & 1], b.active[up & 1], b.sel[lv & 1],
-                                               b.active[lv & 1], tab[up & 1], b.group_flag,
-                                               b.runs);
+                                   b.node_of, b.node_start, stale, b.slot_of[h], b.tslots[h]);
+    ka_insert<<<capped_blocks(n), 256, 0, s>>>(la, nodes, b.node_start, tab[h], b.slot_of[h]);
+    ka_counts<<<capped_blocks(n * 32), 256, 0, s>>>(la, nodes, b.node_start, tab[h],
+                                                     b.active[up], b.cand);
+    const SelectArgs sa{b.node_of, b.cand, min_count, max_count, b.sel[up], b.active[up],
+                        b.sel[h], b.active[h], tab[up], b.group_flag, b.runs};
+    ka_select<<<capped_blocks(n), 256, 0, s>>>(la, sa);
     nl += 4;
   }
   {

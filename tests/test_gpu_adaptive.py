@@ -125,3 +125,4 @@ def test_adaptive_errors(fk):
         knn.query(g, b, max_shift=17)
     idx = knn.query(g, b)                            # one voxel: everything ties at 0
     assert idx.shape == (10, 4)
+
