@@ -98,12 +98,12 @@ __device__ __forceinline__ int2 table_find(const Table& t, uint64_t key) {
 
 __device__ __forceinline__ const uint64_t* sorted_keys(const SortPair<uint64_t>& sp,
                                                        const int* bits) {
-  return (sort_passes_for_bits(*bits) & 1) ? sp.keys[1] : sp.keys[0];
+  return sp.key_buf(sort_passes_for_bits(*bits) & 1);
 }
 
 __device__ __forceinline__ const uint32_t* sorted_vals(const SortPair<uint64_t>& sp,
                                                        const int* bits) {
-  return (sort_passes_for_bits(*bits) & 1) ? sp.vals[1] : sp.vals[0];
+  return sp.val_buf(sort_passes_for_bits(*bits) & 1);
 }
 
 __device__ __forceinline__ bool node_head(const uint64_t* key, int64_t p, int shift) {

@@ -282,8 +282,8 @@ __global__ void __launch_bounds__(256)
   __shared__ uint32_t warp_sums[32];
   __shared__ uint32_t s_total;
   const int buf = sorted_buffer(*bits_ptr);
-  const KeyT* keys = sp.keys[buf];
-  const uint32_t* vals = sp.vals[buf];
+  const KeyT* keys = sp.key_buf(buf);
+  const uint32_t* vals = sp.val_buf(buf);
   const int64_t base = static_cast<int64_t>(blockIdx.x) * 2048 + threadIdx.x * 8;
   uint32_t heads = 0;
 #pragma unroll
@@ -315,7 +315,7 @@ __global__ void __launch_bounds__(256)
             KeyT* __restrict__ head_key, int32_t* __restrict__ head_start,
             int32_t* __restrict__ cell_of) {
   __shared__ uint32_t warp_sums[32];
-  const KeyT* keys = sp.keys[sorted_buffer(*bits_ptr)];
+  const KeyT* keys = sp.key_buf(sorted_buffer(*bits_ptr));
   const int64_t base = static_cast<int64_t>(blockIdx.x) * 2048 + threadIdx.x * 8;
   uint32_t flags = 0, heads = 0;
 #pragma unroll
@@ -482,8 +482,8 @@ __global__ void __launch_bounds__(256)
   __shared__ uint32_t warp_sums[32];
   __shared__ uint32_t s_total;
   const int buf = sorted_buffer(*bits_ptr);
-  const uint32_t* keys = sp.keys[buf];
-  const uint32_t* vals = sp.vals[buf];
+  const uint32_t* keys = sp.key_buf(buf);
+  const uint32_t* vals = sp.val_buf(buf);
   const int64_t base = static_cast<int64_t>(blockIdx.x) * 2048 + threadIdx.x * 8;
   uint32_t heads = 0;
 #pragma unroll

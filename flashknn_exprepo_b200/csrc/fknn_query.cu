@@ -146,6 +146,22 @@ __device__ __forceinline__ void merge_with_lane(uint64_t (&L)[KCAP], int mask) {
   }
 }
 
+// Acceptance of a candidate at squared distance d (>= +0 or NaN): d < cut_r2
+// and d no larger than the current K-th.  For non-negative floats the order
+// of the bit patterns is the order of the values, so d < cut_r2 is
+// bits(d) <= bits(cut_r2) - 1 and both tests fold into one unsigned
+// threshold min(K-th bits, cut_limit).  NaN and +inf lie above every limit.
+// cut_r2 <= 0 (or NaN) accepts nothing: queries then take no candidate.
+__device__ __forceinline__ bool cut_accepts_any(float cut_r2) { return cut_r2 > 0.f; }
+
+__device__ __forceinline__ uint32_t cut_limit(float cut_r2) {
+  return __float_as_uint(cut_r2) - 1u;  // valid when cut_accepts_any(cut_r2)
+}
+
+__device__ __forceinline__ uint32_t kth_limit(uint64_t last, uint32_t cut_lim) {
+  return min(static_cast<uint32_t>(last >> 32), cut_lim);
+}
+
 __device__ __forceinline__ int ceil_log2(int v) { return v <= 1 ? 0 : 32 - __clz(v - 1); }
 
 __device__ __forceinline__ float warp_sum(float v) {
@@ -249,8 +265,18 @@ __device__ __forceinline__ int2 load_run(const QueryLaunch& a, int row, int lane
   return run;
 }
 
+// Register budget per list length (CTAs have at most 256 threads).  Without
+// one, ptxas holds the 16-entry kernels to 64 registers and spills; 96 still
+// fits the 20 resident warps per SM that the default tile's shared memory
+// allows.  Lists of up to 8 entries fit in 72 without spilling.
+template <int KCAP>
+constexpr int query_max_regs() {
+  return KCAP <= 8 ? 72 : (KCAP <= 16 ? 96 : (KCAP <= 32 ? 128 : 224));
+}
+
 template <int KCAP, bool EXACT, typename IdxT>
-__global__ void __launch_bounds__(256) k_query(QueryLaunch a, int T, int min_cands_per_lane) {
+__global__ void __maxnreg__(query_max_regs<KCAP>())
+    k_query(QueryLaunch a, int T, int min_cands_per_lane) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw) + warp;
@@ -300,12 +326,14 @@ __global__ void __launch_bounds__(256) k_query(QueryLaunch a, int T, int min_can
       const int G = 1 << lg;
       const int qi = lane >> lg, sub = lane & (G - 1);
       const bool active = qi < qn;
+      const bool takes = active && cut_accepts_any(a.cut_r2);
       float4 q = make_float4(0.f, 0.f, 0.f, 0.f);
       if (active) q = a.qrec[q0 + qi];
       uint64_t L[KCAP];
 #pragma unroll
       for (int j = 0; j < KCAP; ++j) L[j] = kEmpty;
-      uint32_t thr = 0xffffffffu;
+      const uint32_t cut_lim = cut_limit(a.cut_r2);
+      uint32_t thr = cut_lim;
       bool timed_out = false;
       for (int c0 = 0; c0 < total; c0 += T) {
         const int c1 = min(total, c0 + T);
@@ -325,14 +353,14 @@ __global__ void __launch_bounds__(256) k_query(QueryLaunch a, int T, int min_can
         const int cnt = c1 - c0;
         for (int i0 = 0; i0 < cnt; i0 += G) {
           const int i = i0 + sub;
-          const bool ok = active && i < cnt;
+          const bool ok = takes && i < cnt;
           const float4 c = ok ? tile[i] : q;
           const float d = sq_dist(c.x, c.y, c.z, q.x, q.y, q.z);
           const uint32_t db = __float_as_uint(d);
-          const bool acc = ok && (d < a.cut_r2) && (db <= thr);
+          const bool acc = ok && db <= thr;
           if (__any_sync(kFull, acc)) {
             list_insert<KCAP>(L, acc ? make_key(d, c.w) : kEmpty);
-            thr = static_cast<uint32_t>(L[KCAP - 1] >> 32);
+            thr = kth_limit(L[KCAP - 1], cut_lim);
           }
         }
       }
@@ -449,7 +477,7 @@ __global__ void __launch_bounds__(256) k_query(QueryLaunch a, int T, int min_can
       for (int t = lane; t < s.len; t += 32) {
         const uint16_t v = tmp16[s.seg + t];
         const int bkt = v >> 10;
-        srt16[s.seg + hist[bkt] + (v & 1023)] = static_cast<uint16_t>((bkt << 10) | t);
+        srt16[s.seg + hist[bkt] + (v & 1023)] = static_cast<uint16_t>(s.seg + t);
       }
       if (lane == 0) {
         const float mag = fmaxf(fabsf(cx), fmaxf(fabsf(cy), fabsf(cz))) + sqrtf(d2max);
@@ -473,29 +501,28 @@ __global__ void __launch_bounds__(256) k_query(QueryLaunch a, int T, int min_can
     if (active) q = a.qrec[q0 + lane];
     const float rdx = q.x - s.cx, rdy = q.y - s.cy, rdz = q.z - s.cz;
     const float rq = sqrtf(rdx * rdx + rdy * rdy + rdz * rdz);
-    const int len = active ? s.len : 0;
+    const int len = active && cut_accepts_any(a.cut_r2) ? s.len : 0;
+    const uint32_t cut_lim = cut_limit(a.cut_r2);
 
     uint64_t L[KCAP];
 #pragma unroll
     for (int j = 0; j < KCAP; ++j) {
       uint64_t key = kEmpty;
       if (j < len) {
-        const uint16_t e = srt16[s.seg + j];
-        const float4 c = tile[s.seg + (e & 1023)];
+        const float4 c = tile[srt16[s.seg + j]];
         const float d = sq_dist(c.x, c.y, c.z, q.x, q.y, q.z);
-        if (d < a.cut_r2) key = make_key(d, c.w);
+        if (__float_as_uint(d) <= cut_lim) key = make_key(d, c.w);
       }
       L[j] = key;
     }
     sort_network<KCAP, 0, KCAP>(L);
-    uint32_t thr = static_cast<uint32_t>(L[KCAP - 1] >> 32);
-    int stop = active ? stop_position<KCAP>(L, s, rq, bs) : 0;
+    uint32_t thr = kth_limit(L[KCAP - 1], cut_lim);
+    int stop = len > 0 ? stop_position<KCAP>(L, s, rq, bs) : 0;
     // Candidate t of the lane's scan: accepted when it beats the K-th.
     auto test = [&](int t, uint64_t& x) {
-      const uint16_t e = srt16[s.seg + t];
-      const float4 c = tile[s.seg + (e & 1023)];
+      const float4 c = tile[srt16[s.seg + t]];
       const float d = sq_dist(c.x, c.y, c.z, q.x, q.y, q.z);
-      const bool acc = (d < a.cut_r2) && (__float_as_uint(d) <= thr);
+      const bool acc = __float_as_uint(d) <= thr;
       if (acc) x = make_key(d, c.w);
       return acc;
     };
@@ -514,7 +541,7 @@ __global__ void __launch_bounds__(256) k_query(QueryLaunch a, int T, int min_can
         if (any0) insert_one<KCAP>(L, x0);
         if (any1) insert_one<KCAP>(L, x1);
         if (acc0 || acc1) {
-          thr = static_cast<uint32_t>(L[KCAP - 1] >> 32);
+          thr = kth_limit(L[KCAP - 1], cut_lim);
           stop = min(stop, stop_position<KCAP>(L, s, rq, bs));
         }
       }
@@ -527,7 +554,7 @@ __global__ void __launch_bounds__(256) k_query(QueryLaunch a, int T, int min_can
         if (__any_sync(kFull, acc)) {
           insert_one<KCAP>(L, x);
           if (acc) {
-            thr = static_cast<uint32_t>(L[KCAP - 1] >> 32);
+            thr = kth_limit(L[KCAP - 1], cut_lim);
             stop = min(stop, stop_position<KCAP>(L, s, rq, bs));
           }
         }

@@ -169,6 +169,10 @@ template <typename KeyT>
 struct SortPair {
   KeyT* keys[2];
   uint32_t* vals[2];
+  // Buffer b (0 or 1) by select: indexing the arrays with a run-time value
+  // would copy a by-value kernel parameter to local memory.
+  __host__ __device__ KeyT* key_buf(int b) const { return b ? keys[1] : keys[0]; }
+  __host__ __device__ uint32_t* val_buf(int b) const { return b ? vals[1] : vals[0]; }
 };
 
 template <typename KeyT>

@@ -231,8 +231,8 @@ __global__ void __launch_bounds__(256)
   __shared__ uint32_t warp_sums[32];
   __shared__ uint32_t s_total;
   const int buf = sort_passes_for_bits(*bits_ptr) & 1;
-  const uint64_t* keys = sp.keys[buf];
-  const uint32_t* vals = sp.vals[buf];
+  const uint64_t* keys = sp.key_buf(buf);
+  const uint32_t* vals = sp.val_buf(buf);
   const int64_t base = static_cast<int64_t>(blockIdx.x) * 2048 + threadIdx.x * 8;
   uint32_t heads = 0;
   const int sh = 3 * num_down;
@@ -257,7 +257,7 @@ __global__ void __launch_bounds__(256)
                   int64_t* __restrict__ gd, int64_t* __restrict__ pb,
                   uint64_t* __restrict__ pkey, int64_t* __restrict__ n_parents) {
   __shared__ uint32_t warp_sums[32];
-  const uint64_t* keys = sp.keys[sort_passes_for_bits(*bits_ptr) & 1];
+  const uint64_t* keys = sp.key_buf(sort_passes_for_bits(*bits_ptr) & 1);
   const int64_t base = static_cast<int64_t>(blockIdx.x) * 2048 + threadIdx.x * 8;
   const int sh = 3 * num_down;
   uint32_t flags = 0, heads = 0;

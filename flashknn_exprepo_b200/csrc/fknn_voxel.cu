@@ -84,8 +84,8 @@ __global__ void __launch_bounds__(256)
   const int64_t s = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (s >= n) return;
   const int buf = sort_passes_for_bits(*bits) & 1;
-  const uint64_t* key = sp.keys[buf];
-  if (s == 0 || key[s] != key[s - 1]) flag[sp.vals[buf][s]] = 1;
+  const uint64_t* key = sp.key_buf(buf);
+  if (s == 0 || key[s] != key[s - 1]) flag[sp.val_buf(buf)[s]] = 1;
 }
 
 __global__ void __launch_bounds__(256)
