@@ -10,14 +10,16 @@
 //                   range checks, per-cloud bounding boxes (block-aggregated
 //                   atomics)
 //   k_meta          bits per axis of the translated parent coordinates
-//   k_keys          cell key = cloud << 3*bpa | morton(parent - cloud min)
-//   radix sort      stable LSD sort of (cell key, point id), only as many
-//                   8-bit passes as the key has significant bits
-//   k_gather        cell-sorted float4 records (x, y, z, point id) + cell
-//                   heads per 2048-point tile
-//   k_scan_tiles    tile offsets -> number of cells
-//   k_cells         cell keys and starts (cells stay in key order)
-//   k_hash_*        open-addressing table of the cell keys
+//   support cells   counting sort by cell through an open-addressing table
+//                   keyed by cloud << 3*bpa | morton(parent - cloud min):
+//     k_cell_insert   per point its cell's slot and its rank in the cell
+//                     (warp-aggregated count atomics), cell ids in order of
+//                     creation
+//     k_cell_tiles / k_scan_tiles / k_cell_starts
+//                     cell starts in id order, written into the table
+//     k_scatter       float4 records (x, y, z, point id) at start + rank
+//   query cells     (selected / general queries) k_keys, stable LSD radix
+//                   sort of (key, query), k_gather, k_scan_tiles, k_cells
 //   k_runs          27 (start, count) candidate runs per cell / query group,
 //                   centre first, (0,-1,+1)^3 in ij order like the reference
 //                   neighbour table (flash_knn_construction.cu:42-63)
@@ -349,23 +351,26 @@ __device__ __forceinline__ int axis_offset(int position) {
 }
 
 // ------------------------------------------------------- cell hash table
-// Open addressing over the cell keys (linear probing, load <= 1/2): the
-// 27-neighbour lookup costs one or two L2 probes instead of a binary search
-// over all cells.  The table is sized from the device-side cell count, so
-// only the used prefix is cleared on every call.
-constexpr uint64_t kHashEmpty = ~0ull;
+// Open addressing over the support cells (linear probing, capacity >= 2n, so
+// the load stays <= 1/2 whatever the cell count).  A slot holds key + 1 (0 =
+// empty, so the whole table clears with one memset) and the cell's run
+// (start, count): a neighbour lookup is one 16-byte load.
+//
+// The table also builds the cells, as a counting sort by cell instead of a
+// sort by key.  k_cell_insert counts the points of every cell in its slot
+// and gives each point its rank inside the cell; new cells take ids in
+// creation order (one global atomic per CTA); k_cell_tiles / k_scan_tiles /
+// k_cell_starts lay the cells out in id order; k_scatter writes each point's
+// record at start + rank.  Cell and in-cell order are therefore not
+// deterministic, but nothing downstream depends on them: every query's
+// candidates are the same 27 cells and its top-K is exact under the
+// (distance, index) order.
 
-// One 16-byte slot: cell key and the cell's run, so a probe is one load.
+// One 16-byte slot: key + 1 and the cell's run.
 struct __align__(16) HashSlot {
-  uint64_t key;
-  int2 run;
+  uint64_t key;  // cell key + 1; 0 = empty
+  int2 run;      // (start, count)
 };
-
-__device__ __forceinline__ uint32_t hash_capacity(int cells) {
-  uint32_t cap = 16;
-  while (cap < 2u * static_cast<uint32_t>(cells)) cap <<= 1;
-  return cap;
-}
 
 __device__ __forceinline__ uint32_t hash_slot(uint64_t key, uint32_t mask) {
   key ^= key >> 33;
@@ -376,43 +381,158 @@ __device__ __forceinline__ uint32_t hash_slot(uint64_t key, uint32_t mask) {
   return static_cast<uint32_t>(key) & mask;
 }
 
-__global__ void k_hash_clear(const int* cell_count_ptr, HashSlot* __restrict__ table) {
-  const uint32_t cap = hash_capacity(*cell_count_ptr);
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < cap; i += gridDim.x * blockDim.x)
-    table[i].key = kHashEmpty;
+// Warp-cooperative insertion of 2048 points per 256-thread CTA.  Lanes with
+// the same cell key elect one leader, which probes once and adds the group's
+// size to the cell count; slot_of[i] / rank_of[i] = the point's slot and its
+// rank in the cell.  cell_slot[id] = slot of cell id.
+__global__ void __launch_bounds__(256)
+    k_cell_insert(const int4* __restrict__ pc, int64_t n, const int* __restrict__ bbox,
+                  Meta* meta, HashSlot* __restrict__ table, uint32_t mask,
+                  uint32_t* __restrict__ slot_of, uint32_t* __restrict__ rank_of,
+                  uint32_t* __restrict__ cell_slot) {
+  __shared__ uint32_t s_new;
+  __shared__ uint32_t s_base;
+  __shared__ uint32_t s_list[2048];
+  if (threadIdx.x == 0) s_new = 0u;
+  __syncthreads();
+  const int bpa = meta->bpa;
+  const int lane = threadIdx.x & 31;
+  const int64_t base = static_cast<int64_t>(blockIdx.x) * 2048;
+#pragma unroll 2
+  for (int r = 0; r < 8; ++r) {
+    const int64_t i = base + r * 256 + threadIdx.x;
+    const bool valid = i < n;
+    const unsigned vmask = __ballot_sync(kFull, valid);
+    if (!valid) continue;
+    const uint64_t key = cell_key_of(pc[i], bbox, bpa) + 1;
+    const unsigned peers = __match_any_sync(vmask, key);
+    const int leader = __ffs(peers) - 1;
+    uint32_t slot = 0u, before = 0u;
+    if (lane == leader) {
+      uint32_t h = hash_slot(key, mask);
+      bool found = false;
+      for (uint32_t probe = 0; probe <= mask; ++probe) {
+        const unsigned long long prev =
+            atomicCAS(reinterpret_cast<unsigned long long*>(&table[h].key), 0ull, key);
+        if (prev == 0ull) {
+          s_list[atomicAdd(&s_new, 1u)] = h;
+          found = true;
+          break;
+        }
+        if (prev == key) {
+          found = true;
+          break;
+        }
+        h = (h + 1) & mask;
+      }
+      if (found) {
+        slot = h;
+        before = static_cast<uint32_t>(atomicAdd(&table[h].run.y, __popc(peers)));
+      } else {
+        raise_status(&meta->status, kStatusTable);  // cannot happen at load <= 1/2
+      }
+    }
+    slot = __shfl_sync(peers, slot, leader);
+    before = __shfl_sync(peers, before, leader);
+    slot_of[i] = slot;
+    rank_of[i] = before + __popc(peers & lanemask_lt());
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) s_base = s_new ? atomicAdd(reinterpret_cast<unsigned*>(&meta->n_cells), s_new) : 0u;
+  __syncthreads();
+  for (uint32_t j = threadIdx.x; j < s_new; j += blockDim.x) cell_slot[s_base + j] = s_list[j];
 }
 
-// Value = the cell's candidate run (start, count), so a lookup needs no
-// further load of the cell starts.
-__global__ void k_hash_insert(const uint64_t* __restrict__ cell_key, const int* cell_count_ptr,
-                              const int32_t* __restrict__ cell_start,
-                              HashSlot* __restrict__ table) {
+// Points per 2048 cell ids (8 per thread): tile_counts[tile].
+__global__ void __launch_bounds__(256)
+    k_cell_tiles(const int* cell_count_ptr, const uint32_t* __restrict__ cell_slot,
+                 const HashSlot* __restrict__ table, uint32_t* __restrict__ tile_counts) {
+  __shared__ uint32_t warp_sums[32];
+  __shared__ uint32_t s_total;
   const int cells = *cell_count_ptr;
-  const uint32_t mask = hash_capacity(cells) - 1;
-  for (int64_t c = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; c < cells;
-       c += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    const uint64_t key = cell_key[c];
-    uint32_t h = hash_slot(key, mask);
-    for (uint32_t probe = 0; probe <= mask; ++probe) {
-      const unsigned long long prev = atomicCAS(
-          reinterpret_cast<unsigned long long*>(&table[h].key), kHashEmpty, key);
-      if (prev == kHashEmpty || prev == key) {
-        table[h].run = make_int2(cell_start[c], cell_start[c + 1] - cell_start[c]);
-        break;
-      }
-      h = (h + 1) & mask;
+  const int64_t base = static_cast<int64_t>(blockIdx.x) * 2048 + threadIdx.x * 8;
+  uint32_t c = 0;
+#pragma unroll
+  for (int r = 0; r < 8; ++r)
+    if (base + r < cells) c += static_cast<uint32_t>(table[cell_slot[base + r]].run.y);
+  block_inclusive_scan(c, warp_sums, &s_total);
+  if (threadIdx.x == 0) tile_counts[blockIdx.x] = s_total;
+}
+
+// Cell starts in id order from the scanned tile counts: the slot's run,
+// cell_key[id], cell_start[id] (cell_start[cells] = n) and, when asked,
+// slot_cell[slot] = id.
+__global__ void __launch_bounds__(256)
+    k_cell_starts(const int* cell_count_ptr, const uint32_t* __restrict__ cell_slot,
+                  HashSlot* __restrict__ table, const uint32_t* __restrict__ tile_offsets,
+                  int64_t n, uint64_t* __restrict__ cell_key, int32_t* __restrict__ cell_start,
+                  uint32_t* __restrict__ slot_cell) {
+  __shared__ uint32_t warp_sums[32];
+  const int cells = *cell_count_ptr;
+  const int64_t base = static_cast<int64_t>(blockIdx.x) * 2048 + threadIdx.x * 8;
+  uint32_t cnt[8], slot[8], sum = 0;
+#pragma unroll
+  for (int r = 0; r < 8; ++r) {
+    cnt[r] = 0u;
+    slot[r] = 0u;
+    if (base + r < cells) {
+      slot[r] = cell_slot[base + r];
+      cnt[r] = static_cast<uint32_t>(table[slot[r]].run.y);
     }
+    sum += cnt[r];
+  }
+  const uint32_t incl = block_inclusive_scan(sum, warp_sums, nullptr);
+  uint32_t start = tile_offsets[blockIdx.x] + incl - sum;
+#pragma unroll
+  for (int r = 0; r < 8; ++r) {
+    const int64_t c = base + r;
+    if (c >= cells) break;
+    HashSlot& hs = table[slot[r]];
+    hs.run.x = static_cast<int>(start);
+    cell_key[c] = hs.key - 1;
+    cell_start[c] = static_cast<int32_t>(start);
+    if (slot_cell) slot_cell[slot[r]] = static_cast<uint32_t>(c);
+    start += cnt[r];
+    if (c == cells - 1) cell_start[cells] = static_cast<int32_t>(n);
   }
 }
 
+// rec[pos] = (xyz of point i, i) at pos = cell start + rank; optional
+// pos_of[i] = pos and cell_of[pos] = cell id.
+__global__ void __launch_bounds__(256)
+    k_scatter(const float* __restrict__ xyz, const int64_t* __restrict__ index, int64_t n_src,
+              int64_t n, const uint32_t* __restrict__ slot_of, const uint32_t* __restrict__ rank_of,
+              const HashSlot* __restrict__ table, const uint32_t* __restrict__ slot_cell,
+              float4* __restrict__ rec, int32_t* __restrict__ pos_of,
+              int32_t* __restrict__ cell_of, int* status) {
+  const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint32_t slot = slot_of[i];
+  const int64_t pos = static_cast<int64_t>(table[slot].run.x) + rank_of[i];
+  if (pos < 0 || pos >= n) {
+    raise_status(status, kStatusTable);
+    return;
+  }
+  int64_t row = i;
+  if (index) {
+    row = index[i];
+    if (row < 0 || row >= n_src) row = 0;  // reported by k_bbox
+  }
+  rec[pos] = make_float4(xyz[3 * row], xyz[3 * row + 1], xyz[3 * row + 2],
+                         __int_as_float(static_cast<int>(i)));
+  if (pos_of) pos_of[i] = static_cast<int32_t>(pos);
+  if (cell_of) cell_of[pos] = static_cast<int32_t>(slot_cell[slot]);
+}
+
 __device__ __forceinline__ int2 hash_find(const HashSlot* table, uint32_t mask, uint64_t key) {
-  uint32_t h = hash_slot(key, mask);
+  const uint64_t stored = key + 1;
+  uint32_t h = hash_slot(stored, mask);
   for (uint32_t probe = 0; probe <= mask; ++probe) {
     const ulonglong2 v = __ldg(reinterpret_cast<const ulonglong2*>(table + h));
-    if (v.x == key)
+    if (v.x == stored)
       return make_int2(static_cast<int>(static_cast<uint32_t>(v.y)),
                        static_cast<int>(static_cast<uint32_t>(v.y >> 32)));
-    if (v.x == kHashEmpty) break;
+    if (v.x == 0ull) break;
     h = (h + 1) & mask;
   }
   return make_int2(0, 0);  // no such cell: an empty run
@@ -423,12 +543,11 @@ __device__ __forceinline__ int2 hash_find(const HashSlot* table, uint32_t mask, 
 // offset j, or (0, 0) when that cell is empty.
 __global__ void __launch_bounds__(256)
     k_runs(const uint64_t* __restrict__ group_key, const int* group_count_ptr,
-           const HashSlot* __restrict__ table, const int* cell_count_ptr, const Meta* meta,
-           int2* __restrict__ runs) {
+           const HashSlot* __restrict__ table, uint32_t hmask, const int* cell_count_ptr,
+           const Meta* meta, int2* __restrict__ runs) {
   const int64_t total = static_cast<int64_t>(*group_count_ptr) * kNeighbours;
   const int bpa = meta->bpa;
   const int cells = *cell_count_ptr;
-  const uint32_t hmask = hash_capacity(cells) - 1;
   const uint64_t mask = bpa ? ((1ull << (3 * bpa)) - 1) : 0ull;
   const int lim = 1 << bpa;
   for (int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; t < total;
@@ -541,6 +660,7 @@ struct Bufs {
   uint32_t* seg_counts;
   HashSlot* hslots;
   int64_t hash_cap;
+  uint32_t* slot_cell;  // cell id of each occupied slot (selected queries)
 };
 
 Bufs layout(void* ws, int64_t n, int64_t m, int64_t n_clouds, int kind, size_t* bytes) {
@@ -571,6 +691,7 @@ Bufs layout(void* ws, int64_t n, int64_t m, int64_t n_clouds, int kind, size_t* 
   if (kind == FKNN_QUERY_SELECTED) {
     b.pos_of = a.take<int32_t>(n);
     b.cell_of = a.take<int32_t>(n);
+    b.slot_cell = a.take<uint32_t>(b.hash_cap);
   }
   if (kind == FKNN_QUERY_GENERAL) {
     b.runs = a.take<int2>(static_cast<size_t>(m) * kNeighbours);
@@ -624,6 +745,7 @@ int run_fused(const FusedArgs& f, void* ws, size_t ws_bytes, const QueryShape& s
   int nl = 0;
   cudaError_t e;
   const SortPair<uint64_t> sp64{{b.keys64[0], b.keys64[1]}, {b.vals[0], b.vals[1]}};
+  const uint32_t hmask = static_cast<uint32_t>(b.hash_cap - 1);
   const SortPair<uint32_t> sp32{{b.keys32[0], b.keys32[1]}, {b.vals[0], b.vals[1]}};
 
   k_init<<<64, 256, 0, s>>>(b.meta, b.bbox, n_clouds, b.totals, 3 * kSortMaxPasses * 256);
@@ -651,20 +773,24 @@ int run_fused(const FusedArgs& f, void* ws, size_t ws_bytes, const QueryShape& s
 
   // --- support cells
   if (n > 0) {
-    k_keys<<<blocks_for(n, 256), 256, 0, s>>>(b.pc_s, n, b.bbox, b.meta, b.keys64[0], b.vals[0]);
-    ++nl;
-    SortBuffers<uint64_t> sb{{b.keys64[0], b.keys64[1]}, {b.vals[0], b.vals[1]}, b.hist, b.totals};
-    nl += launch_radix_sort(sb, n, key_bits, max_passes, s);
+    // Counting sort by cell through the hash table (slot and rank per point
+    // in vals[0] / vals[1], slot per cell id in keys32[0]).
+    e = cudaMemsetAsync(b.hslots, 0, sizeof(HashSlot) * static_cast<size_t>(b.hash_cap), s);
+    if (e != cudaSuccess) {
+      note_cuda_error(e);
+      return FKNN_ERR_CUDA;
+    }
     const int tiles = blocks_for(n, 2048);
-    k_gather<uint64_t><<<tiles, 256, 0, s>>>(f.xyz, f.sindex, f.n_src, n, sp64, key_bits, b.srec,
-                                             b.pos_of, b.tile_counts);
-    k_scan_tiles<<<1, 1024, 0, s>>>(b.tile_counts, tiles, &b.meta->n_cells);
-    k_cells<uint64_t><<<tiles, 256, 0, s>>>(n, sp64, key_bits, b.tile_counts,
-                                            &b.meta->n_cells, b.cell_key, b.cell_start, b.cell_of);
-    k_hash_clear<<<static_cast<int>(b.hash_cap < 1024 * 256 ? ceil_div(b.hash_cap, 256) : 1024), 256, 0,
-                   s>>>(&b.meta->n_cells, b.hslots);
-    k_hash_insert<<<capped_blocks(n), 256, 0, s>>>(b.cell_key, &b.meta->n_cells, b.cell_start,
-                                                     b.hslots);
+    uint32_t* cell_slot = b.keys32[0];
+    k_cell_insert<<<tiles, 256, 0, s>>>(b.pc_s, n, b.bbox, b.meta, b.hslots, hmask, b.vals[0],
+                                        b.vals[1], cell_slot);
+    k_cell_tiles<<<tiles, 256, 0, s>>>(&b.meta->n_cells, cell_slot, b.hslots, b.tile_counts);
+    k_scan_tiles<<<1, 1024, 0, s>>>(b.tile_counts, tiles, &b.meta->n_points_scanned);
+    k_cell_starts<<<tiles, 256, 0, s>>>(&b.meta->n_cells, cell_slot, b.hslots, b.tile_counts, n,
+                                        b.cell_key, b.cell_start, b.slot_cell);
+    k_scatter<<<blocks_for(n, 256), 256, 0, s>>>(f.xyz, f.sindex, f.n_src, n, b.vals[0], b.vals[1],
+                                                 b.hslots, b.slot_cell, b.srec, b.pos_of,
+                                                 b.cell_of, &b.meta->status);
     nl += 5;
   }
 
@@ -680,7 +806,7 @@ int run_fused(const FusedArgs& f, void* ws, size_t ws_bytes, const QueryShape& s
   if (kind == FKNN_QUERY_SELF) {
     if (n > 0) {
       k_runs<<<capped_blocks(n * kNeighbours), 256, 0, s>>>(
-          b.cell_key, &b.meta->n_cells, b.hslots, &b.meta->n_cells, b.meta,
+          b.cell_key, &b.meta->n_cells, b.hslots, hmask, &b.meta->n_cells, b.meta,
           b.runs);
       ++nl;
       nl += launch_items(b.runs, b.cell_start, nullptr, &b.meta->n_cells, n, shape.tile_records,
@@ -696,7 +822,7 @@ int run_fused(const FusedArgs& f, void* ws, size_t ws_bytes, const QueryShape& s
     group_count_ptr = &b.meta->n_groups;
     if (n > 0) {
       k_runs<<<capped_blocks(n * kNeighbours), 256, 0, s>>>(
-          b.cell_key, &b.meta->n_cells, b.hslots, &b.meta->n_cells, b.meta,
+          b.cell_key, &b.meta->n_cells, b.hslots, hmask, &b.meta->n_cells, b.meta,
           b.runs);
       ++nl;
     }
@@ -742,7 +868,7 @@ int run_fused(const FusedArgs& f, void* ws, size_t ws_bytes, const QueryShape& s
                                               &b.meta->n_groups, b.group_key, b.group_start,
                                               nullptr);
       k_runs<<<capped_blocks(m * kNeighbours), 256, 0, s>>>(
-          b.group_key, &b.meta->n_groups, b.hslots, &b.meta->n_cells,
+          b.group_key, &b.meta->n_groups, b.hslots, hmask, &b.meta->n_cells,
           b.meta, b.runs);
       nl += 4;
       nl += launch_items(b.runs, b.group_start, nullptr, &b.meta->n_groups, m, shape.tile_records,

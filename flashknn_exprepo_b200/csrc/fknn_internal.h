@@ -22,7 +22,8 @@ struct Meta {
   int qkey_bits;    // significant bits of the selected-query cell keys
   int batch_bits;   // bits of the largest batch id
   int max_extent;   // largest per-cloud parent-coordinate extent
-  int reserved[6];
+  int n_points_scanned;  // total of a scan over per-cell point counts (= n)
+  int reserved[5];
 };
 static_assert(sizeof(Meta) == 64, "Meta layout");
 
