@@ -469,8 +469,11 @@ def rows_single_gpu(fk, torch, dev, flush, peak_gbs):
     """The paths around the batched query, each on its own workload:
     adaptive-neighbourhood query (LiDAR scan), back query and voxel-first
     subsampling (16-cloud batch), the DeLA hierarchy builder (LiDAR scan),
-    radius-limited query (room) and neighbour feature grouping (16-cloud
-    batch, 64 channels, forward with its HBM roofline, and backward)."""
+    radius-limited query (room), the room at K=32 through the self query,
+    the selected query (every 4th point) and the reference table ABI, the
+    uniform cube at K=16, the LiDAR scan at alpha 4 and 8, and neighbour
+    feature grouping (16-cloud batch, 64 channels, forward with its HBM
+    roofline, and backward)."""
     from flashknn_exprepo_b200 import hierarchy, synthetic
     T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)  # noqa: E731
     rows = {}
@@ -535,6 +538,42 @@ def rows_single_gpu(fk, torch, dev, flush, peak_gbs):
     ms = _event_ms(torch, lambda: fk.ops.ball_query_offsets(room, ro, 32, 0.1, 0.025, 2), flush)
     rows["ball_query_room_k32"] = {"value": room.shape[0] / (ms * 1e-3), "unit": "queries/s",
                                    "ms": ms, "radius_m": 0.1}
+    # room (C2), K=32, 4 cm voxels, alpha 4: every point, the stride-4 subset
+    # (selected query), and the reference table ABI (tables built once by
+    # fknn_build_tables, which reads the parent count back; query timed alone)
+    rgrid = torch.floor(room / synthetic.C2_VOXEL).long()
+    ms = _event_ms(torch, lambda: fk.ops.knn_grid(room, rgrid, None, 32, 2), flush)
+    rows["self_query_room_k32"] = {"value": room.shape[0] / (ms * 1e-3), "unit": "queries/s",
+                                   "ms": ms, "n_points": int(room.shape[0])}
+    qi = torch.arange(0, room.shape[0], 4, device=dev)
+    ms = _event_ms(torch, lambda: fk.ops.knn_grid(room, rgrid, None, 32, 2, query_indices=qi),
+                   flush)
+    rows["selected_query_room_k32"] = {"value": qi.numel() / (ms * 1e-3), "unit": "queries/s",
+                                       "ms": ms, "n_queries": int(qi.numel()),
+                                       "n_support": int(room.shape[0])}
+    bms = _event_ms(torch, lambda: fk.ops.build_tables(rgrid, None, 2), flush)
+    tb = fk.ops.build_tables(rgrid, None, 2)
+    xs = room[tb["order"]].contiguous()
+    ms = _event_ms(torch, lambda: fk.ops.query_tables(xs, tb["steps"], tb["neigh"], tb["cnt"],
+                                                      32), flush)
+    rows["query_tables_room_k32"] = {"value": room.shape[0] / (ms * 1e-3), "unit": "queries/s",
+                                     "ms": ms, "build_tables_ms": bms,
+                                     "what": "reference table ABI (FlashKNN_Query_Dynamic_Load "
+                                             "boundary): query on caller-built tables"}
+    # uniform cube (C1), 16,384 points, K=16
+    cube = T(synthetic.uniform_cube())
+    co = torch.tensor([cube.shape[0]], device=dev)
+    ms = _event_ms(torch, lambda: fk.ops.knn_offsets(cube, co, 16, synthetic.C1_VOXEL, 2), flush)
+    rows["self_query_cube_k16"] = {"value": cube.shape[0] / (ms * 1e-3), "unit": "queries/s",
+                                   "ms": ms, "n_points": int(cube.shape[0])}
+    # LiDAR scan (C3), K=16, alpha 4 and alpha 8 (num_down 2 and 3)
+    lo_ = torch.tensor([lx.shape[0]], device=dev)
+    for nd, alpha in ((2, 4), (3, 8)):
+        ms = _event_ms(torch, lambda: fk.ops.knn_offsets(lx, lo_, 16, synthetic.C3_VOXEL, nd),
+                       flush)
+        rows[f"self_query_lidar_k16_alpha{alpha}"] = {
+            "value": lx.shape[0] / (ms * 1e-3), "unit": "queries/s", "ms": ms,
+            "n_points": int(lx.shape[0])}
     # grouping: 16-cloud batch, K=16, 64 channels
     off = T(b.offsets)
     idx, _ = fk.ops.knn_offsets(bx, off, 16, synthetic.C4_VOXEL, 2)

@@ -18,8 +18,11 @@
 //     k_cell_tiles / k_scan_tiles / k_cell_starts
 //                     cell starts in id order, written into the table
 //     k_scatter       float4 records (x, y, z, point id) at start + rank
-//   query cells     (selected / general queries) k_keys, stable LSD radix
-//                   sort of (key, query), k_gather, k_scan_tiles, k_cells
+//   query groups    general queries: query cells by the same counting sort
+//                   through a second table; selected queries: support cells
+//                   holding queries, by a counting sort over the dense cell
+//                   ids (k_sel_count / k_sel_tiles / k_sel_starts /
+//                   k_sel_scatter)
 //   k_runs          27 (start, count) candidate runs per cell / query group,
 //                   centre first, (0,-1,+1)^3 in ij order like the reference
 //                   neighbour table (flash_knn_construction.cu:42-63)
@@ -114,12 +117,11 @@ __device__ __forceinline__ int cloud_of(const PointSrc& p, int64_t i, int* statu
 
 // ------------------------------------------------------------------ init
 
-__global__ void k_init(Meta* meta, int* bbox, int64_t n_clouds, uint32_t* totals, int n_totals) {
+__global__ void k_init(Meta* meta, int* bbox, int64_t n_clouds) {
   const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
   if (t < static_cast<int64_t>(sizeof(Meta) / sizeof(int))) reinterpret_cast<int*>(meta)[t] = 0;
   for (int64_t i = t; i < n_clouds * 6; i += stride) bbox[i] = (i % 6) < 3 ? INT_MAX : INT_MIN;
-  for (int64_t i = t; i < n_totals; i += stride) totals[i] = 0u;
 }
 
 // ------------------------------------------------------------------ bbox
@@ -253,97 +255,6 @@ __device__ __forceinline__ uint64_t cell_key_of(int4 c, const int* bbox, int bpa
   return (static_cast<uint64_t>(c.w) << (3 * bpa)) | morton3(x, y, z);
 }
 
-__global__ void __launch_bounds__(256) k_keys(const int4* __restrict__ pc, int64_t n,
-                                              const int* __restrict__ bbox, const Meta* meta,
-                                              uint64_t* __restrict__ keys,
-                                              uint32_t* __restrict__ vals) {
-  const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  keys[i] = cell_key_of(pc[i], bbox, meta->bpa);
-  vals[i] = static_cast<uint32_t>(i);
-}
-
-// --------------------------------------------------------- sorted records
-
-// Which ping-pong buffer holds the sorted data after a sort over `bits`.
-__device__ __forceinline__ int sorted_buffer(int bits) { return sort_passes_for_bits(bits) & 1; }
-
-template <typename KeyT>
-__device__ __forceinline__ bool is_head(const KeyT* keys, int64_t s) {
-  return s == 0 || keys[s] != keys[s - 1];
-}
-
-// Tile of 2048 sorted positions per 256-thread CTA, blocked (8 per thread).
-// rec[s] = (xyz[id], id) with id = sorted value; optional pos_of[id] = s;
-// tile_counts[tile] = number of cell heads in the tile.
-template <typename KeyT>
-__global__ void __launch_bounds__(256)
-    k_gather(const float* __restrict__ xyz, const int64_t* __restrict__ index, int64_t n_src,
-             int64_t n, SortPair<KeyT> sp, const int* bits_ptr, float4* __restrict__ rec,
-             int32_t* __restrict__ pos_of, uint32_t* __restrict__ tile_counts) {
-  __shared__ uint32_t warp_sums[32];
-  __shared__ uint32_t s_total;
-  const int buf = sorted_buffer(*bits_ptr);
-  const KeyT* keys = sp.key_buf(buf);
-  const uint32_t* vals = sp.val_buf(buf);
-  const int64_t base = static_cast<int64_t>(blockIdx.x) * 2048 + threadIdx.x * 8;
-  uint32_t heads = 0;
-#pragma unroll
-  for (int r = 0; r < 8; ++r) {
-    const int64_t s = base + r;
-    if (s >= n) break;
-    const uint32_t id = vals[s];
-    int64_t row = id;
-    if (index) {
-      row = index[id];
-      if (row < 0 || row >= n_src) row = 0;  // reported by k_bbox
-    }
-    rec[s] = make_float4(xyz[3 * row], xyz[3 * row + 1], xyz[3 * row + 2],
-                         __int_as_float(static_cast<int>(id)));
-    if (pos_of) pos_of[id] = static_cast<int32_t>(s);
-    heads += is_head(keys, s) ? 1u : 0u;
-  }
-  block_inclusive_scan(heads, warp_sums, &s_total);
-  if (threadIdx.x == 0) tile_counts[blockIdx.x] = s_total;
-}
-
-// Cell (group) ids from the scanned tile counts.  head_key[c], head_start[c]
-// for every head; cell_of[s] (optional) = cell of sorted position s;
-// head_start[count] = n.
-template <typename KeyT>
-__global__ void __launch_bounds__(256)
-    k_cells(int64_t n, SortPair<KeyT> sp, const int* bits_ptr,
-            const uint32_t* __restrict__ tile_offsets, const int* count_ptr,
-            KeyT* __restrict__ head_key, int32_t* __restrict__ head_start,
-            int32_t* __restrict__ cell_of) {
-  __shared__ uint32_t warp_sums[32];
-  const KeyT* keys = sp.key_buf(sorted_buffer(*bits_ptr));
-  const int64_t base = static_cast<int64_t>(blockIdx.x) * 2048 + threadIdx.x * 8;
-  uint32_t flags = 0, heads = 0;
-#pragma unroll
-  for (int r = 0; r < 8; ++r) {
-    const int64_t s = base + r;
-    if (s < n && is_head(keys, s)) {
-      flags |= 1u << r;
-      ++heads;
-    }
-  }
-  const uint32_t incl = block_inclusive_scan(heads, warp_sums, nullptr);
-  int c = static_cast<int>(tile_offsets[blockIdx.x] + incl - heads) - 1;
-#pragma unroll
-  for (int r = 0; r < 8; ++r) {
-    const int64_t s = base + r;
-    if (s >= n) break;
-    if (flags & (1u << r)) {
-      ++c;
-      head_key[c] = keys[s];
-      head_start[c] = static_cast<int32_t>(s);
-    }
-    if (cell_of) cell_of[s] = c;
-    if (s == n - 1) head_start[*count_ptr] = static_cast<int32_t>(n);
-  }
-}
-
 // ------------------------------------------------------------- neighbours
 
 __device__ __forceinline__ int axis_offset(int position) {
@@ -384,12 +295,12 @@ __device__ __forceinline__ uint32_t hash_slot(uint64_t key, uint32_t mask) {
 // Warp-cooperative insertion of 2048 points per 256-thread CTA.  Lanes with
 // the same cell key elect one leader, which probes once and adds the group's
 // size to the cell count; slot_of[i] / rank_of[i] = the point's slot and its
-// rank in the cell.  cell_slot[id] = slot of cell id.
+// rank in the cell.  cell_slot[id] = slot of cell id; *cell_count = cells.
 __global__ void __launch_bounds__(256)
     k_cell_insert(const int4* __restrict__ pc, int64_t n, const int* __restrict__ bbox,
                   Meta* meta, HashSlot* __restrict__ table, uint32_t mask,
                   uint32_t* __restrict__ slot_of, uint32_t* __restrict__ rank_of,
-                  uint32_t* __restrict__ cell_slot) {
+                  uint32_t* __restrict__ cell_slot, int* cell_count) {
   __shared__ uint32_t s_new;
   __shared__ uint32_t s_base;
   __shared__ uint32_t s_list[2048];
@@ -438,7 +349,8 @@ __global__ void __launch_bounds__(256)
     rank_of[i] = before + __popc(peers & lanemask_lt());
   }
   __syncthreads();
-  if (threadIdx.x == 0) s_base = s_new ? atomicAdd(reinterpret_cast<unsigned*>(&meta->n_cells), s_new) : 0u;
+  if (threadIdx.x == 0)
+    s_base = s_new ? atomicAdd(reinterpret_cast<unsigned*>(cell_count), s_new) : 0u;
   __syncthreads();
   for (uint32_t j = threadIdx.x; j < s_new; j += blockDim.x) cell_slot[s_base + j] = s_list[j];
 }
@@ -461,12 +373,12 @@ __global__ void __launch_bounds__(256)
 
 // Cell starts in id order from the scanned tile counts: the slot's run,
 // cell_key[id], cell_start[id] (cell_start[cells] = n) and, when asked,
-// slot_cell[slot] = id.
+// slot_cell[slot] = id and zero_per_cell[id] = 0.
 __global__ void __launch_bounds__(256)
     k_cell_starts(const int* cell_count_ptr, const uint32_t* __restrict__ cell_slot,
                   HashSlot* __restrict__ table, const uint32_t* __restrict__ tile_offsets,
                   int64_t n, uint64_t* __restrict__ cell_key, int32_t* __restrict__ cell_start,
-                  uint32_t* __restrict__ slot_cell) {
+                  uint32_t* __restrict__ slot_cell, uint32_t* __restrict__ zero_per_cell) {
   __shared__ uint32_t warp_sums[32];
   const int cells = *cell_count_ptr;
   const int64_t base = static_cast<int64_t>(blockIdx.x) * 2048 + threadIdx.x * 8;
@@ -492,6 +404,7 @@ __global__ void __launch_bounds__(256)
     cell_key[c] = hs.key - 1;
     cell_start[c] = static_cast<int32_t>(start);
     if (slot_cell) slot_cell[slot[r]] = static_cast<uint32_t>(c);
+    if (zero_per_cell) zero_per_cell[c] = 0u;
     start += cnt[r];
     if (c == cells - 1) cell_start[cells] = static_cast<int32_t>(n);
   }
@@ -571,80 +484,129 @@ __global__ void __launch_bounds__(256)
 }
 
 // ------------------------------------------------------ selected queries
+// Groups = support cells holding at least one selected query, in cell id
+// order; group_row[g] = that cell (its runs row).  A counting sort over the
+// dense cell ids: k_sel_count (warp-aggregated counts and ranks), two tile
+// scans (non-empty cells, queries), k_sel_starts, k_sel_scatter.
 
-// key = cell of the queried support point, value = output row.
+// Per query r: the cell of its support point and its rank among that
+// cell's queries (qcount is zeroed by k_cell_starts).
 __global__ void __launch_bounds__(256)
-    k_sel_keys(const int64_t* __restrict__ query_indices, int64_t m, int64_t n,
-               const int32_t* __restrict__ pos_of, const int32_t* __restrict__ cell_of,
-               Meta* meta, uint32_t* __restrict__ keys, uint32_t* __restrict__ vals) {
+    k_sel_count(const int64_t* __restrict__ query_indices, int64_t m, int64_t n,
+                const int32_t* __restrict__ pos_of, const int32_t* __restrict__ cell_of,
+                Meta* meta, uint32_t* __restrict__ qcount, uint32_t* __restrict__ cell_r,
+                uint32_t* __restrict__ rank_r) {
   const int64_t r = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (r == 0) {
-    const int p = meta->n_cells;
-    meta->qkey_bits = p > 1 ? 32 - __clz(p - 1) : 0;
-  }
-  if (r >= m) return;
+  const bool valid = r < m;
+  const unsigned vmask = __ballot_sync(kFull, valid);
+  if (!valid) return;
   int64_t qi = query_indices[r];
   if (qi < 0 || qi >= n) {
     raise_status(&meta->status, kStatusTable);
     qi = 0;
   }
-  keys[r] = static_cast<uint32_t>(cell_of[pos_of[qi]]);
-  vals[r] = static_cast<uint32_t>(r);
+  const uint32_t c = static_cast<uint32_t>(cell_of[pos_of[qi]]);
+  const unsigned peers = __match_any_sync(vmask, c);
+  const int leader = __ffs(peers) - 1;
+  uint32_t before = 0u;
+  if ((threadIdx.x & 31) == leader) before = atomicAdd(&qcount[c], static_cast<uint32_t>(__popc(peers)));
+  before = __shfl_sync(peers, before, leader);
+  cell_r[r] = c;
+  rank_r[r] = before + __popc(peers & lanemask_lt());
 }
 
-// qrec[j] = (support xyz of the query, output row) in cell order + heads.
+// Per 2048 cells (8 per thread): non-empty cells and their queries.
 __global__ void __launch_bounds__(256)
-    k_sel_gather(int64_t m, int64_t n, SortPair<uint32_t> sp, const int* bits_ptr,
-                 const int64_t* __restrict__ query_indices, const int32_t* __restrict__ pos_of,
-                 const float4* __restrict__ srec, float4* __restrict__ qrec,
-                 uint32_t* __restrict__ tile_counts) {
+    k_sel_tiles(const int* cell_count_ptr, const uint32_t* __restrict__ qcount,
+                uint32_t* __restrict__ tile_groups, uint32_t* __restrict__ tile_queries) {
   __shared__ uint32_t warp_sums[32];
   __shared__ uint32_t s_total;
-  const int buf = sorted_buffer(*bits_ptr);
-  const uint32_t* keys = sp.key_buf(buf);
-  const uint32_t* vals = sp.val_buf(buf);
+  const int cells = *cell_count_ptr;
   const int64_t base = static_cast<int64_t>(blockIdx.x) * 2048 + threadIdx.x * 8;
-  uint32_t heads = 0;
+  uint32_t g = 0, q = 0;
 #pragma unroll
   for (int r = 0; r < 8; ++r) {
-    const int64_t j = base + r;
-    if (j >= m) break;
-    const uint32_t row = vals[j];
-    int64_t qi = query_indices[row];
-    if (qi < 0 || qi >= n) qi = 0;  // reported by k_sel_keys
-    float4 v = srec[pos_of[qi]];
-    v.w = __int_as_float(static_cast<int>(row));
-    qrec[j] = v;
-    heads += is_head(keys, j) ? 1u : 0u;
+    const uint32_t c = base + r < cells ? qcount[base + r] : 0u;
+    g += c ? 1u : 0u;
+    q += c;
   }
-  block_inclusive_scan(heads, warp_sums, &s_total);
-  if (threadIdx.x == 0) tile_counts[blockIdx.x] = s_total;
+  block_inclusive_scan(g, warp_sums, &s_total);
+  if (threadIdx.x == 0) tile_groups[blockIdx.x] = s_total;
+  block_inclusive_scan(q, warp_sums, &s_total);
+  if (threadIdx.x == 0) tile_queries[blockIdx.x] = s_total;
+}
+
+// Group ids of the non-empty cells from the scanned tile counts:
+// group_start[g] = first query record, group_row[g] = cell, qstart[cell] =
+// first record of the cell's queries; group_start[groups] = m.
+__global__ void __launch_bounds__(256)
+    k_sel_starts(const int* cell_count_ptr, const uint32_t* __restrict__ qcount,
+                 const uint32_t* __restrict__ tile_goff, const uint32_t* __restrict__ tile_qoff,
+                 int64_t m, const int* group_count_ptr, int32_t* __restrict__ group_start,
+                 int32_t* __restrict__ group_row, uint32_t* __restrict__ qstart) {
+  __shared__ uint32_t warp_sums[32];
+  const int cells = *cell_count_ptr;
+  const int64_t base = static_cast<int64_t>(blockIdx.x) * 2048 + threadIdx.x * 8;
+  uint32_t cnt[8], g = 0, q = 0;
+#pragma unroll
+  for (int r = 0; r < 8; ++r) {
+    cnt[r] = base + r < cells ? qcount[base + r] : 0u;
+    g += cnt[r] ? 1u : 0u;
+    q += cnt[r];
+  }
+  const uint32_t gi = block_inclusive_scan(g, warp_sums, nullptr);
+  const uint32_t qi = block_inclusive_scan(q, warp_sums, nullptr);
+  uint32_t gid = tile_goff[blockIdx.x] + gi - g;
+  uint32_t qs = tile_qoff[blockIdx.x] + qi - q;
+#pragma unroll
+  for (int r = 0; r < 8; ++r) {
+    const int64_t c = base + r;
+    if (c >= cells) break;
+    if (cnt[r]) {
+      group_start[gid] = static_cast<int32_t>(qs);
+      group_row[gid] = static_cast<int32_t>(c);
+      qstart[c] = qs;
+      ++gid;
+      qs += cnt[r];
+    }
+    if (c == cells - 1) group_start[*group_count_ptr] = static_cast<int32_t>(m);
+  }
+}
+
+// qrec[qstart[cell] + rank] = (support xyz of query r, output row r).
+__global__ void __launch_bounds__(256)
+    k_sel_scatter(int64_t m, int64_t n, const int64_t* __restrict__ query_indices,
+                  const int32_t* __restrict__ pos_of, const float4* __restrict__ srec,
+                  const uint32_t* __restrict__ cell_r, const uint32_t* __restrict__ rank_r,
+                  const uint32_t* __restrict__ qstart, float4* __restrict__ qrec, int* status) {
+  const int64_t r = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (r >= m) return;
+  int64_t qi = query_indices[r];
+  if (qi < 0 || qi >= n) qi = 0;  // reported by k_sel_count
+  const int64_t pos = static_cast<int64_t>(qstart[cell_r[r]]) + rank_r[r];
+  if (pos < 0 || pos >= m) {
+    raise_status(status, kStatusTable);
+    return;
+  }
+  float4 v = srec[pos_of[qi]];
+  v.w = __int_as_float(static_cast<int>(r));
+  qrec[pos] = v;
 }
 
 // ------------------------------------------------------------ host side
 
 namespace {
 
-// Bits needed to hold any value in [0, count).
-int bits_for_count(int64_t count) {
-  int b = 0;
-  while ((1ll << b) < count) ++b;
-  return b;
-}
-
-int batch_bits_upper(int64_t n_clouds) { return bits_for_count(n_clouds); }
-
 struct Bufs {
   Meta* meta;
   int* bbox;
   int4* pc_s;
   int4* pc_q;
-  uint64_t* keys64[2];
-  uint32_t* keys32[2];
-  uint32_t* vals[2];
-  uint32_t* hist;
-  uint32_t* totals;         // [3][8*256]
+  uint32_t* slot_of;    // per point: cell slot (support, then general queries)
+  uint32_t* rank_of;    // per point: rank inside its cell
+  uint32_t* cell_slot;  // per cell / query group id: its slot
   uint32_t* tile_counts;
+  uint32_t* tile_counts2;
   float4* srec;
   float4* qrec;
   int32_t* pos_of;
@@ -661,6 +623,10 @@ struct Bufs {
   HashSlot* hslots;
   int64_t hash_cap;
   uint32_t* slot_cell;  // cell id of each occupied slot (selected queries)
+  uint32_t* qcount;     // selected queries per support cell
+  uint32_t* qstart;     // first query record of each support cell
+  HashSlot* qslots;     // query-cell table (general queries)
+  int64_t qhash_cap;
 };
 
 Bufs layout(void* ws, int64_t n, int64_t m, int64_t n_clouds, int kind, size_t* bytes) {
@@ -672,16 +638,11 @@ Bufs layout(void* ws, int64_t n, int64_t m, int64_t n_clouds, int kind, size_t* 
   b.bbox = a.take<int>(6 * static_cast<size_t>(n_clouds > 32768 ? n_clouds : 32768));
   b.pc_s = a.take<int4>(n);
   b.pc_q = kind == FKNN_QUERY_GENERAL ? a.take<int4>(m) : nullptr;
-  b.keys64[0] = a.take<uint64_t>(nm);
-  b.keys64[1] = a.take<uint64_t>(nm);
-  // 32-bit keys (selected queries) alias the 64-bit key buffers.
-  b.keys32[0] = reinterpret_cast<uint32_t*>(b.keys64[0]);
-  b.keys32[1] = reinterpret_cast<uint32_t*>(b.keys64[1]);
-  b.vals[0] = a.take<uint32_t>(nm);
-  b.vals[1] = a.take<uint32_t>(nm);
-  b.hist = a.take<uint32_t>(sort_hist_elems(nm));
-  b.totals = a.take<uint32_t>(3 * kSortMaxPasses * 256);
+  b.slot_of = a.take<uint32_t>(nm);
+  b.rank_of = a.take<uint32_t>(nm);
+  b.cell_slot = a.take<uint32_t>(nm);
   b.tile_counts = a.take<uint32_t>(static_cast<size_t>(ceil_div(nm > 0 ? nm : 1, 2048)));
+  b.tile_counts2 = a.take<uint32_t>(static_cast<size_t>(ceil_div(nm > 0 ? nm : 1, 2048)));
   b.srec = a.take<float4>(n);
   b.cell_key = a.take<uint64_t>(n);
   b.cell_start = a.take<int32_t>(n + 1);
@@ -692,10 +653,15 @@ Bufs layout(void* ws, int64_t n, int64_t m, int64_t n_clouds, int kind, size_t* 
     b.pos_of = a.take<int32_t>(n);
     b.cell_of = a.take<int32_t>(n);
     b.slot_cell = a.take<uint32_t>(b.hash_cap);
+    b.qcount = a.take<uint32_t>(n);
+    b.qstart = a.take<uint32_t>(n);
   }
   if (kind == FKNN_QUERY_GENERAL) {
     b.runs = a.take<int2>(static_cast<size_t>(m) * kNeighbours);
     b.group_key = a.take<uint64_t>(m);
+    b.qhash_cap = 16;
+    while (b.qhash_cap < 2 * m) b.qhash_cap <<= 1;
+    b.qslots = a.take<HashSlot>(b.qhash_cap);
   } else {
     b.runs = a.take<int2>(static_cast<size_t>(n) * kNeighbours);
   }
@@ -744,11 +710,9 @@ int run_fused(const FusedArgs& f, void* ws, size_t ws_bytes, const QueryShape& s
   if (ws_bytes < need) return FKNN_ERR_WORKSPACE;
   int nl = 0;
   cudaError_t e;
-  const SortPair<uint64_t> sp64{{b.keys64[0], b.keys64[1]}, {b.vals[0], b.vals[1]}};
   const uint32_t hmask = static_cast<uint32_t>(b.hash_cap - 1);
-  const SortPair<uint32_t> sp32{{b.keys32[0], b.keys32[1]}, {b.vals[0], b.vals[1]}};
 
-  k_init<<<64, 256, 0, s>>>(b.meta, b.bbox, n_clouds, b.totals, 3 * kSortMaxPasses * 256);
+  k_init<<<64, 256, 0, s>>>(b.meta, b.bbox, n_clouds);
   ++nl;
 
   const float inv_voxel = 1.0f / f.voxel;  // host FP32 division, correctly rounded
@@ -767,30 +731,24 @@ int run_fused(const FusedArgs& f, void* ws, size_t ws_bytes, const QueryShape& s
   k_meta<<<1, 1024, 0, s>>>(b.bbox, n_clouds, b.meta);
   ++nl;
 
-  const int max_bits = 3 * (16 - f.num_down) + batch_bits_upper(n_clouds);
-  const int max_passes = sort_passes_for_bits(max_bits);
-  const int* key_bits = &b.meta->key_bits;
-
   // --- support cells
   if (n > 0) {
-    // Counting sort by cell through the hash table (slot and rank per point
-    // in vals[0] / vals[1], slot per cell id in keys32[0]).
+    // Counting sort by cell through the hash table.
     e = cudaMemsetAsync(b.hslots, 0, sizeof(HashSlot) * static_cast<size_t>(b.hash_cap), s);
     if (e != cudaSuccess) {
       note_cuda_error(e);
       return FKNN_ERR_CUDA;
     }
     const int tiles = blocks_for(n, 2048);
-    uint32_t* cell_slot = b.keys32[0];
-    k_cell_insert<<<tiles, 256, 0, s>>>(b.pc_s, n, b.bbox, b.meta, b.hslots, hmask, b.vals[0],
-                                        b.vals[1], cell_slot);
-    k_cell_tiles<<<tiles, 256, 0, s>>>(&b.meta->n_cells, cell_slot, b.hslots, b.tile_counts);
+    k_cell_insert<<<tiles, 256, 0, s>>>(b.pc_s, n, b.bbox, b.meta, b.hslots, hmask, b.slot_of,
+                                        b.rank_of, b.cell_slot, &b.meta->n_cells);
+    k_cell_tiles<<<tiles, 256, 0, s>>>(&b.meta->n_cells, b.cell_slot, b.hslots, b.tile_counts);
     k_scan_tiles<<<1, 1024, 0, s>>>(b.tile_counts, tiles, &b.meta->n_points_scanned);
-    k_cell_starts<<<tiles, 256, 0, s>>>(&b.meta->n_cells, cell_slot, b.hslots, b.tile_counts, n,
-                                        b.cell_key, b.cell_start, b.slot_cell);
-    k_scatter<<<blocks_for(n, 256), 256, 0, s>>>(f.xyz, f.sindex, f.n_src, n, b.vals[0], b.vals[1],
-                                                 b.hslots, b.slot_cell, b.srec, b.pos_of,
-                                                 b.cell_of, &b.meta->status);
+    k_cell_starts<<<tiles, 256, 0, s>>>(&b.meta->n_cells, b.cell_slot, b.hslots, b.tile_counts, n,
+                                        b.cell_key, b.cell_start, b.slot_cell, b.qcount);
+    k_scatter<<<blocks_for(n, 256), 256, 0, s>>>(f.xyz, f.sindex, f.n_src, n, b.slot_of,
+                                                 b.rank_of, b.hslots, b.slot_cell, b.srec,
+                                                 b.pos_of, b.cell_of, &b.meta->status);
     nl += 5;
   }
 
@@ -827,22 +785,22 @@ int run_fused(const FusedArgs& f, void* ws, size_t ws_bytes, const QueryShape& s
       ++nl;
     }
     if (m > 0 && n > 0) {
-      k_sel_keys<<<blocks_for(m, 256), 256, 0, s>>>(f.query_indices, m, n, b.pos_of, b.cell_of,
-                                                    b.meta, b.keys32[0], b.vals[0]);
-      ++nl;
-      SortBuffers<uint32_t> qb{{b.keys32[0], b.keys32[1]}, {b.vals[0], b.vals[1]}, b.hist,
-                               b.totals + kSortMaxPasses * 256};
-      const int qpasses = sort_passes_for_bits(bits_for_count(n));
-      nl += launch_radix_sort(qb, m, &b.meta->qkey_bits, qpasses, s);
-      const int tiles = blocks_for(m, 2048);
-      k_sel_gather<<<tiles, 256, 0, s>>>(m, n, sp32, &b.meta->qkey_bits,
-                                         f.query_indices, b.pos_of, b.srec, b.qrec, b.tile_counts);
-      k_scan_tiles<<<1, 1024, 0, s>>>(b.tile_counts, tiles, &b.meta->n_groups);
-      k_cells<uint32_t><<<tiles, 256, 0, s>>>(m, sp32, &b.meta->qkey_bits, b.tile_counts,
-                                              &b.meta->n_groups,
-                                              reinterpret_cast<uint32_t*>(b.group_row),
-                                              b.group_start, nullptr);
-      nl += 3;
+      // per-query cell and rank in slot_of / rank_of (free again once the
+      // support records are written)
+      const int ctiles = blocks_for(n, 2048);
+      k_sel_count<<<blocks_for(m, 256), 256, 0, s>>>(f.query_indices, m, n, b.pos_of, b.cell_of,
+                                                     b.meta, b.qcount, b.slot_of, b.rank_of);
+      k_sel_tiles<<<ctiles, 256, 0, s>>>(&b.meta->n_cells, b.qcount, b.tile_counts,
+                                         b.tile_counts2);
+      k_scan_tiles<<<1, 1024, 0, s>>>(b.tile_counts, ctiles, &b.meta->n_groups);
+      k_scan_tiles<<<1, 1024, 0, s>>>(b.tile_counts2, ctiles, &b.meta->n_points_scanned);
+      k_sel_starts<<<ctiles, 256, 0, s>>>(&b.meta->n_cells, b.qcount, b.tile_counts,
+                                          b.tile_counts2, m, &b.meta->n_groups, b.group_start,
+                                          b.group_row, b.qstart);
+      k_sel_scatter<<<blocks_for(m, 256), 256, 0, s>>>(m, n, f.query_indices, b.pos_of, b.srec,
+                                                       b.slot_of, b.rank_of, b.qstart, b.qrec,
+                                                       &b.meta->status);
+      nl += 6;
       nl += launch_items(b.runs, b.group_start, b.group_row, &b.meta->n_groups, m,
                          shape.tile_records, b.cands, b.seg_counts, &b.meta->n_items, b.items, s,
                          &b.meta->status, m);
@@ -855,22 +813,32 @@ int run_fused(const FusedArgs& f, void* ws, size_t ws_bytes, const QueryShape& s
     group_start = b.group_start;
     group_count_ptr = &b.meta->n_groups;
     if (m > 0) {
-      k_keys<<<blocks_for(m, 256), 256, 0, s>>>(b.pc_q, m, b.bbox, b.meta, b.keys64[0], b.vals[0]);
-      ++nl;
-      SortBuffers<uint64_t> qb{{b.keys64[0], b.keys64[1]}, {b.vals[0], b.vals[1]}, b.hist,
-                               b.totals + kSortMaxPasses * 256};
-      nl += launch_radix_sort(qb, m, key_bits, max_passes, s);
+      // query groups = query cells, by the same counting sort through a
+      // second table (slot_of / rank_of / cell_slot are free again once the
+      // support records are written)
+      e = cudaMemsetAsync(b.qslots, 0, sizeof(HashSlot) * static_cast<size_t>(b.qhash_cap), s);
+      if (e != cudaSuccess) {
+        note_cuda_error(e);
+        return FKNN_ERR_CUDA;
+      }
+      const uint32_t qmask = static_cast<uint32_t>(b.qhash_cap - 1);
       const int tiles = blocks_for(m, 2048);
-      k_gather<uint64_t><<<tiles, 256, 0, s>>>(f.qxyz, nullptr, m, m, sp64, key_bits, b.qrec,
-                                               nullptr, b.tile_counts);
-      k_scan_tiles<<<1, 1024, 0, s>>>(b.tile_counts, tiles, &b.meta->n_groups);
-      k_cells<uint64_t><<<tiles, 256, 0, s>>>(m, sp64, key_bits, b.tile_counts,
-                                              &b.meta->n_groups, b.group_key, b.group_start,
-                                              nullptr);
+      k_cell_insert<<<tiles, 256, 0, s>>>(b.pc_q, m, b.bbox, b.meta, b.qslots, qmask, b.slot_of,
+                                          b.rank_of, b.cell_slot, &b.meta->n_groups);
+      k_cell_tiles<<<tiles, 256, 0, s>>>(&b.meta->n_groups, b.cell_slot, b.qslots,
+                                         b.tile_counts);
+      k_scan_tiles<<<1, 1024, 0, s>>>(b.tile_counts, tiles, &b.meta->n_points_scanned);
+      k_cell_starts<<<tiles, 256, 0, s>>>(&b.meta->n_groups, b.cell_slot, b.qslots,
+                                          b.tile_counts, m, b.group_key, b.group_start, nullptr,
+                                          nullptr);
+      k_scatter<<<blocks_for(m, 256), 256, 0, s>>>(f.qxyz, nullptr, m, m, b.slot_of, b.rank_of,
+                                                   b.qslots, nullptr, b.qrec, nullptr, nullptr,
+                                                   &b.meta->status);
+      nl += 5;
       k_runs<<<capped_blocks(m * kNeighbours), 256, 0, s>>>(
           b.group_key, &b.meta->n_groups, b.hslots, hmask, &b.meta->n_cells,
           b.meta, b.runs);
-      nl += 4;
+      ++nl;
       nl += launch_items(b.runs, b.group_start, nullptr, &b.meta->n_groups, m, shape.tile_records,
                          b.cands, b.seg_counts, &b.meta->n_items, b.items, s, &b.meta->status, m);
     }
