@@ -8,12 +8,15 @@
 // each key in a stable sort -- the lowest index of the voxel -- and the
 // representatives' indices in ascending order.
 //
-//   kv_keys      keys + the OR of all keys (significant bits of the sort)
-//   radix sort   stable LSD sort of (key, index) over the significant bits
-//   kv_heads     flag[index of every key's first sorted point] = 1
+// No sort is needed for that: the lowest index per key comes from an
+// open-addressing table of the keys (capacity >= 2n, cleared by one memset).
+//   kv_insert    key, one probe per distinct key per warp, the voxel's lowest
+//                index kept in the slot (atomicMax of UINT32_MAX - index, so
+//                a zeroed slot is neutral), the point's slot
+//   kv_flags     flag[i] = (i is the lowest index of its voxel)
 //   kv_tiles / k_scan_tiles / kv_compact
 //                ordered compaction of the flags: the output comes out in
-//                ascending index order without a second sort
+//                ascending index order
 // The count stays on the device (*count_out), so the sequence is a fixed
 // launch list that can be captured in a CUDA graph.
 #include "fknn_common.cuh"
@@ -27,65 +30,80 @@ namespace {
 constexpr int kTile = 2048;  // points per 256-thread CTA (8 each)
 }
 
-// keys[i] = morton16(floor(x * inv)) | batch << 48; OR of all keys into
-// bits_or[0..1] (low / high word).
+struct __align__(16) VoxelSlot {
+  uint64_t key;    // voxel key + 1; 0 = empty
+  uint32_t first;  // UINT32_MAX - lowest index of the voxel (0 = none yet)
+  uint32_t pad;
+};
+
+__device__ __forceinline__ uint32_t voxel_hash(uint64_t key, uint32_t mask) {
+  key ^= key >> 33;
+  key *= 0xff51afd7ed558ccdULL;
+  key ^= key >> 33;
+  key *= 0xc4ceb9fe1a85ec53ULL;
+  key ^= key >> 33;
+  return static_cast<uint32_t>(key) & mask;
+}
+
+// key = morton16(floor(x * inv)) | batch << 48.  Lanes with the same key
+// elect their lowest lane (the lowest index among them), which probes once
+// and offers that index to the slot; slot_of[i] = the point's slot.
 __global__ void __launch_bounds__(256)
-    kv_keys(const float* __restrict__ xyz, const int64_t* __restrict__ batch, int64_t n,
-            float inv, Meta* meta, uint32_t* bits_or, uint64_t* __restrict__ keys,
-            uint32_t* __restrict__ vals) {
+    kv_insert(const float* __restrict__ xyz, const int64_t* __restrict__ batch, int64_t n,
+              float inv, Meta* meta, VoxelSlot* __restrict__ table, uint32_t mask,
+              uint32_t* __restrict__ slot_of) {
   const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-  uint64_t key = 0;
-  if (i < n) {
-    uint32_t c[3];
+  const bool valid = i < n;
+  const unsigned vmask = __ballot_sync(kFull, valid);
+  if (!valid) return;
+  uint32_t c[3];
 #pragma unroll
-    for (int a = 0; a < 3; ++a) {
-      // floor conversion; saturates instead of overflowing for huge values
-      const long long g = __float2ll_rd(__fmul_rn(xyz[3 * i + a], inv));
-      c[a] = static_cast<uint32_t>(g) & 0xffffu;
+  for (int a = 0; a < 3; ++a) {
+    // floor conversion; saturates instead of overflowing for huge values
+    const long long g = __float2ll_rd(__fmul_rn(xyz[3 * i + a], inv));
+    c[a] = static_cast<uint32_t>(g) & 0xffffu;
+  }
+  uint64_t key = morton3(c[0], c[1], c[2]);
+  if (batch) {
+    int64_t b = batch[i];
+    if (b < 0 || b >= 32768) {
+      raise_status(&meta->status, kStatusBatch);
+      b = b < 0 ? 0 : 32767;
     }
-    key = morton3(c[0], c[1], c[2]);
-    if (batch) {
-      int64_t b = batch[i];
-      if (b < 0 || b >= 32768) {
-        raise_status(&meta->status, kStatusBatch);
-        b = b < 0 ? 0 : 32767;
+    key |= static_cast<uint64_t>(b) << 48;
+  }
+  key += 1;
+  const unsigned peers = __match_any_sync(vmask, key);
+  const int leader = __ffs(peers) - 1;
+  uint32_t slot = 0u;
+  if ((threadIdx.x & 31) == leader) {
+    uint32_t h = voxel_hash(key, mask);
+    bool found = false;
+    for (uint32_t probe = 0; probe <= mask; ++probe) {
+      const unsigned long long prev =
+          atomicCAS(reinterpret_cast<unsigned long long*>(&table[h].key), 0ull, key);
+      if (prev == 0ull || prev == key) {
+        found = true;
+        break;
       }
-      key |= static_cast<uint64_t>(b) << 48;
+      h = (h + 1) & mask;
     }
-    keys[i] = key;
-    vals[i] = static_cast<uint32_t>(i);
+    if (found) {
+      atomicMax(&table[h].first, 0xffffffffu - static_cast<uint32_t>(i));
+      slot = h;
+    } else {
+      raise_status(&meta->status, kStatusTable);  // cannot happen at load <= 1/2
+    }
   }
-  // OR over the block first: one pair of global atomics per block, not per
-  // warp (all of them hit the same two words)
-  __shared__ uint32_t s_or[2][8];
-  const uint32_t lo = __reduce_or_sync(kFull, static_cast<uint32_t>(key));
-  const uint32_t hi = __reduce_or_sync(kFull, static_cast<uint32_t>(key >> 32));
-  const int warp = threadIdx.x >> 5;
-  if ((threadIdx.x & 31) == 0) {
-    s_or[0][warp] = lo;
-    s_or[1][warp] = hi;
-  }
-  __syncthreads();
-  if (threadIdx.x < 2) {
-    uint32_t v = 0;
-    for (int w = 0; w < static_cast<int>(blockDim.x >> 5); ++w) v |= s_or[threadIdx.x][w];
-    if (v) atomicOr(bits_or + threadIdx.x, v);
-  }
+  slot_of[i] = __shfl_sync(peers, slot, leader);
 }
 
-__global__ void kv_bits(const uint32_t* bits_or, Meta* meta) {
-  const uint64_t v = (static_cast<uint64_t>(bits_or[1]) << 32) | bits_or[0];
-  meta->key_bits = v ? 64 - __clzll(static_cast<long long>(v)) : 0;
-}
-
-// Every key's first point in the stable order is its lowest index.
 __global__ void __launch_bounds__(256)
-    kv_heads(int64_t n, SortPair<uint64_t> sp, const int* bits, uint8_t* __restrict__ flag) {
-  const int64_t s = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (s >= n) return;
-  const int buf = sort_passes_for_bits(*bits) & 1;
-  const uint64_t* key = sp.key_buf(buf);
-  if (s == 0 || key[s] != key[s - 1]) flag[sp.val_buf(buf)[s]] = 1;
+    kv_flags(int64_t n, const VoxelSlot* __restrict__ table, const uint32_t* __restrict__ slot_of,
+             uint8_t* __restrict__ flag) {
+  const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  flag[i] = (0xffffffffu - table[slot_of[i]].first) == static_cast<uint32_t>(i) ? 1 : 0;
 }
 
 __global__ void __launch_bounds__(256)
@@ -126,11 +144,9 @@ namespace {
 
 struct VBufs {
   Meta* meta;
-  uint32_t* bits_or;
-  uint64_t* keys[2];
-  uint32_t* vals[2];
-  uint32_t* hist;
-  uint32_t* totals;
+  VoxelSlot* table;
+  int64_t cap;
+  uint32_t* slot_of;
   uint32_t* tile_counts;
   uint8_t* flag;
 };
@@ -139,13 +155,10 @@ VBufs vlayout(void* ws, int64_t n, size_t* bytes) {
   Arena a(ws);
   VBufs b{};
   b.meta = a.take<Meta>(1);
-  b.bits_or = a.take<uint32_t>(2);
-  b.keys[0] = a.take<uint64_t>(n);
-  b.keys[1] = a.take<uint64_t>(n);
-  b.vals[0] = a.take<uint32_t>(n);
-  b.vals[1] = a.take<uint32_t>(n);
-  b.hist = a.take<uint32_t>(sort_hist_elems(n));
-  b.totals = a.take<uint32_t>(kSortMaxPasses * 256);
+  b.cap = 16;
+  while (b.cap < 2 * n) b.cap <<= 1;
+  b.table = a.take<VoxelSlot>(b.cap);
+  b.slot_of = a.take<uint32_t>(n);
   b.tile_counts = a.take<uint32_t>(static_cast<size_t>(ceil_div(n > 0 ? n : 1, kTile)));
   b.flag = a.take<uint8_t>(n);
   if (bytes) *bytes = a.used + 256;
@@ -170,9 +183,8 @@ int run_voxel_first(const VoxelArgs& v, void* ws, size_t ws_bytes, cudaStream_t 
   VBufs b = vlayout(ws, v.n, &need);
   if (ws_bytes < need) return FKNN_ERR_WORKSPACE;
   cudaError_t e = cudaMemsetAsync(b.meta, 0, sizeof(Meta), s);
-  if (e == cudaSuccess) e = cudaMemsetAsync(b.bits_or, 0, 2 * sizeof(uint32_t), s);
-  if (e == cudaSuccess) e = cudaMemsetAsync(b.totals, 0, kSortMaxPasses * 256 * sizeof(uint32_t), s);
-  if (e == cudaSuccess && v.n > 0) e = cudaMemsetAsync(b.flag, 0, static_cast<size_t>(v.n), s);
+  if (e == cudaSuccess && v.n > 0)
+    e = cudaMemsetAsync(b.table, 0, sizeof(VoxelSlot) * static_cast<size_t>(b.cap), s);
   if (e == cudaSuccess && v.n == 0) e = cudaMemsetAsync(v.count_out, 0, sizeof(int64_t), s);
   if (e != cudaSuccess) {
     note_cuda_error(e);
@@ -181,20 +193,15 @@ int run_voxel_first(const VoxelArgs& v, void* ws, size_t ws_bytes, cudaStream_t 
   int nl = 0;
   if (v.n > 0) {
     const float inv = 1.0f / v.voxel;  // host FP32 division, correctly rounded
-    kv_keys<<<blocks_for(v.n, 256), 256, 0, s>>>(v.xyz, v.batch, v.n, inv, b.meta, b.bits_or,
-                                                 b.keys[0], b.vals[0]);
-    kv_bits<<<1, 1, 0, s>>>(b.bits_or, b.meta);
-    nl += 2;
-    SortBuffers<uint64_t> sb{{b.keys[0], b.keys[1]}, {b.vals[0], b.vals[1]}, b.hist, b.totals};
-    nl += launch_radix_sort(sb, v.n, &b.meta->key_bits, kSortMaxPasses, s);
-    const SortPair<uint64_t> sp{{b.keys[0], b.keys[1]}, {b.vals[0], b.vals[1]}};
+    kv_insert<<<blocks_for(v.n, 256), 256, 0, s>>>(v.xyz, v.batch, v.n, inv, b.meta, b.table,
+                                                   static_cast<uint32_t>(b.cap - 1), b.slot_of);
     const int tiles = blocks_for(v.n, kTile);
-    kv_heads<<<blocks_for(v.n, 256), 256, 0, s>>>(v.n, sp, &b.meta->key_bits, b.flag);
+    kv_flags<<<blocks_for(v.n, 256), 256, 0, s>>>(v.n, b.table, b.slot_of, b.flag);
     kv_tiles<<<tiles, 256, 0, s>>>(v.n, b.flag, b.tile_counts);
     k_scan_tiles<<<1, 1024, 0, s>>>(b.tile_counts, tiles, &b.meta->n_cells);
     kv_compact<<<tiles, 256, 0, s>>>(v.n, b.flag, b.tile_counts, &b.meta->n_cells, v.out,
                                      v.count_out);
-    nl += 4;
+    nl += 5;
   }
   e = cudaGetLastError();
   if (e != cudaSuccess) {
