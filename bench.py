@@ -560,6 +560,26 @@ def rows_single_gpu(fk, torch, dev, flush, peak_gbs):
                                      "ms": ms, "build_tables_ms": bms,
                                      "what": "reference table ABI (FlashKNN_Query_Dynamic_Load "
                                              "boundary): query on caller-built tables"}
+    # the same stride-4 queries through the selected-query table ABI: qindex =
+    # their sorted positions grouped by parent, steps_query = per-parent offsets
+    inv = torch.empty_like(tb["order"])
+    inv[tb["order"]] = torch.arange(room.shape[0], device=dev)
+    qpos = inv[qi]
+    parent = torch.searchsorted(tb["steps"][1:].long(), qpos, right=True)
+    qindex = qpos[torch.argsort(parent, stable=True)].int()
+    counts = torch.bincount(parent, minlength=tb["neigh"].shape[0])
+    steps_q = torch.cat([counts.new_zeros(1), torch.cumsum(counts, 0)]).int()
+    ms = _event_ms(torch, lambda: fk.ops.selected_query_tables(
+        xs, qindex, tb["steps"], steps_q, tb["neigh"], tb["cnt"], 32), flush)
+    rows["selected_query_tables_room_k32"] = {
+        "value": qi.numel() / (ms * 1e-3), "unit": "queries/s", "ms": ms,
+        "what": "reference table ABI (FlashKNN_Selected_Query_DL boundary)"}
+    # Morton keys and the 27 neighbour keys of the room's parent cells
+    ms = _event_ms(torch, lambda: fk.ops.morton_encode(rgrid), flush)
+    pgrid = torch.unique(rgrid >> 2, dim=0)
+    nms = _event_ms(torch, lambda: fk.ops.morton_neighbor_keys(pgrid), flush)
+    rows["morton_room"] = {"value": ms, "unit": "ms", "neighbor_keys_ms": nms,
+                           "n_points": int(rgrid.shape[0]), "n_parents": int(pgrid.shape[0])}
     # uniform cube (C1), 16,384 points, K=16
     cube = T(synthetic.uniform_cube())
     co = torch.tensor([cube.shape[0]], device=dev)
