@@ -505,9 +505,13 @@ def rows_single_gpu(fk, torch, dev, flush, peak_gbs):
         if lib.fknn_profile_read(ctypes.cast(buf, ctypes.c_void_p), 1) == 1:
             qms.append(buf[0])
     lib.fknn_profile_enable(0)
+    _, _, lv = fk.ops.adaptive_query(grid, None, 16, xyz=lx, want_levels=True)
+    lvl, cnt = torch.unique(lv, return_counts=True)
     rows["adaptive_lidar_k16"] = {"value": len(lidar) / (ms * 1e-3), "unit": "queries/s",
                                   "ms": ms, "eager_ms": eager, "n_points": len(lidar),
                                   "query_kernel_ms": statistics.median(qms) if qms else None,
+                                  "points_per_level": {int(a): int(b) for a, b in
+                                                       zip(lvl.tolist(), cnt.tolist())},
                                   "step": "CUDA-graph replay of the whole adaptive pipeline"}
     # back query K=1 and voxel-first subsampling, 16-cloud batch
     b = synthetic.uneven_batch()
