@@ -57,8 +57,9 @@ constexpr int kTile = 2048;  // sorted positions per 256-thread CTA (8 each)
 constexpr uint64_t kEmptyKey = ~0ull;
 
 // Meta fields: bpa = bits per axis of the key layout, reserved[0] = S (top
-// level), key_bits = 3 * bpa + batch bits.
+// level), reserved[1] = largest batch id + 1, key_bits = 3 * bpa + batch bits.
 __device__ __forceinline__ int top_level(const Meta* m) { return m->reserved[0]; }
+__device__ __forceinline__ int* batch_slots_used(Meta* m) { return &m->reserved[1]; }
 
 __device__ __forceinline__ uint32_t slot_of_key(uint64_t key, uint32_t mask) {
   key ^= key >> 33;
@@ -172,10 +173,12 @@ __global__ void __launch_bounds__(256)
   for (int h = 0; h < 2; ++h)
 #pragma unroll
     for (int a = 0; a < 6; ++a) lo[h][a] = a < 3 ? LLONG_MAX : LLONG_MIN;
+  int b_max = -1;
   for (int r = 0; r < 8; ++r) {
     const int64_t i = base + r * 256 + threadIdx.x;
     if (i >= n) break;
     const int b = batch_of(batch, i, status);
+    b_max = max(b_max, b);
     const long long g[3] = {grid[3 * i], grid[3 * i + 1], grid[3 * i + 2]};
     if (b == b_lo || b == b_hi) {
       const int h = b == b_lo ? 0 : 1;
@@ -193,6 +196,8 @@ __global__ void __launch_bounds__(256)
       }
     }
   }
+  b_max = __reduce_max_sync(kFull, b_max);
+  if ((threadIdx.x & 31) == 0 && b_max >= 0) atomicMax(batch_slots_used(meta), b_max + 1);
 #pragma unroll
   for (int h = 0; h < 2; ++h)
 #pragma unroll
@@ -229,7 +234,8 @@ __global__ void __launch_bounds__(1024)
   __shared__ int s_b[32];
   long long span = 0;
   int maxb = 0;
-  for (int b = threadIdx.x; b < kBatchSlots; b += blockDim.x) {
+  const int used = min(*batch_slots_used(meta), kBatchSlots);  // boxes above are empty
+  for (int b = threadIdx.x; b < used; b += blockDim.x) {
     const long long* bx = box + 6 * static_cast<int64_t>(b);
     if (bx[0] <= bx[3]) {
       span = max(span, max(bx[3] - bx[0], max(bx[4] - bx[1], bx[5] - bx[2])));

@@ -231,6 +231,18 @@ def test_c3_lidar_k16_alpha4_and_8(fk, nd):
     _offsets_case(fk, xyz, np.array([len(xyz)]), 16, S.C3_VOXEL, nd)
 
 
+@pytest.mark.parametrize("n", [5000, 40000])
+def test_sparse_cells_one_point_per_cell(fk, n):
+    """About one point per parent cell, the densest the cell table gets (one
+    cell per point): self and general queries still equal the oracle."""
+    rng = np.random.default_rng(12)
+    xyz = rng.random((n, 3), dtype=np.float32) * np.float32(4)
+    voxel = 0.01  # parent cell 4 cm: ~1 point per cell at these densities
+    _offsets_case(fk, xyz, np.array([n // 2, n]), 8, voxel)
+    q = rng.random((n // 4, 3), dtype=np.float32) * np.float32(4)
+    _offsets_case(fk, xyz, np.array([n]), 8, voxel, 2, q, np.array([n // 4]))
+
+
 def test_general_queries_outside_support(fk):
     rng = np.random.default_rng(11)
     a = rng.random((3000, 3), dtype=np.float32)
