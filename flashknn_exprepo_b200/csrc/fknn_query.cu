@@ -528,16 +528,24 @@ __global__ void __maxnreg__(query_max_regs<KCAP>())
     };
     if constexpr (KCAP <= 16) {
       // Two candidates per iteration, both tested against the same K-th
-      // distance and inserted in order: half the loop and vote overhead, and
-      // two independent loads and distance chains in flight.  (With a
-      // 32- or 64-entry list the extra registers cost more than this saves.)
+      // distance: half the loop and vote overhead, and two independent loads
+      // and distance chains in flight.  (With a 32- or 64-entry list the
+      // extra registers cost more than this saves.)
       for (int t = KCAP;; t += 2) {
         const bool live0 = t < stop, live1 = t + 1 < stop;
         if (!__any_sync(kFull, live0)) break;
         uint64_t x0 = kEmpty, x1 = kEmpty;
         const bool acc0 = live0 && test(t, x0);
         const bool acc1 = live1 && test(t + 1, x1);
-        const bool any0 = __any_sync(kFull, acc0), any1 = __any_sync(kFull, acc1);
+        // A lane that took only its second candidate inserts it in the first
+        // step, so the second step runs only when some lane took both (the
+        // list keeps the K smallest of what it is given, in any order).
+        if (!acc0) {
+          x0 = x1;
+          x1 = kEmpty;
+        }
+        const bool any0 = __any_sync(kFull, acc0 || acc1);
+        const bool any1 = __any_sync(kFull, acc0 && acc1);
         if (any0) insert_one<KCAP>(L, x0);
         if (any1) insert_one<KCAP>(L, x1);
         if (acc0 || acc1) {
