@@ -43,31 +43,33 @@ __device__ __forceinline__ bool entry_ok(int32_t t, int64_t n, int* status) {
 
 // ------------------------------------------------------------------ forward
 
-// Flat over the output: thread t writes output word t (float4 words when
-// every row is a whole number of aligned float4s, else single floats), so a
-// warp's stores are one contiguous run whatever the channel count.  Stores
-// stream past L2 (st.global.cs): the output is written once and not re-read
-// here.
+// Rows of whole aligned float4s (no xyz, c % 4 == 0): a group of tpr lanes
+// (a power of two, tpr >= c/4 up to 32) copies one row, so a warp writes
+// 32/tpr consecutive rows as one contiguous run; the row loop is unrolled so
+// several independent gathers are in flight per thread.  Otherwise flat over
+// the output: thread t writes output float t.  Stores stream past L2
+// (st.global.cs): the output is written once and not re-read here.
 __global__ void __launch_bounds__(256)
     kg_forward(const float* __restrict__ feat, int64_t n, int c, const int32_t* __restrict__ idx,
                int64_t rows, int k, const float* __restrict__ xyz,
-               const float* __restrict__ new_xyz, int with_xyz, int vec4,
+               const float* __restrict__ new_xyz, int with_xyz, int tpr,
                float* __restrict__ out, int* status) {
   const int off = with_xyz ? 3 : 0;
   const int cw = c + off;
   const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
-  if (vec4) {  // with_xyz == 0, c % 4 == 0
+  if (tpr) {  // with_xyz == 0, c % 4 == 0
     const int q4 = c >> 2;
-    const int64_t words = rows * q4;
-    for (int64_t w = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; w < words;
-         w += stride) {
-      const int64_t r = w / q4;
-      const int q = static_cast<int>(w - r * q4);
+    const int sub = threadIdx.x & (tpr - 1);
+    const int64_t row_stride = stride / tpr;
+    const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll 4
+    for (int64_t r = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) / tpr;
+         r < rows; r += row_stride) {
       const int32_t t = idx[r];
-      float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-      if (entry_ok(t, n, q == 0 ? status : nullptr))
-        v = __ldg(reinterpret_cast<const float4*>(feat + static_cast<int64_t>(t) * c) + q);
-      __stcs(reinterpret_cast<float4*>(out) + w, v);
+      const bool ok = entry_ok(t, n, sub == 0 ? status : nullptr);
+      const float4* src = reinterpret_cast<const float4*>(feat + static_cast<int64_t>(t) * c);
+      float4* dst = reinterpret_cast<float4*>(out) + r * q4;
+      for (int q = sub; q < q4; q += tpr) __stcs(dst + q, ok ? __ldg(src + q) : zero);
     }
     return;
   }
@@ -296,9 +298,14 @@ int run_group_forward(const GroupArgs& g, void* ws, size_t ws_bytes, cudaStream_
     const bool vec4 = !g.with_xyz && g.c % 4 == 0 &&
                       reinterpret_cast<uintptr_t>(g.feat) % 16 == 0 &&
                       reinterpret_cast<uintptr_t>(g.out) % 16 == 0;
-    const int64_t words = vec4 ? rows * (g.c / 4) : rows * cw;
+    int tpr = 0;  // lanes per row of the float4 path
+    if (vec4) {
+      tpr = 1;
+      while (tpr < 32 && tpr < g.c / 4) tpr <<= 1;
+    }
+    const int64_t words = vec4 ? rows * tpr : rows * cw;
     kg_forward<<<capped_blocks(words), 256, 0, s>>>(g.feat, g.n, g.c, g.idx, rows, g.k, g.xyz,
-                                                        g.new_xyz, g.with_xyz, vec4 ? 1 : 0,
+                                                        g.new_xyz, g.with_xyz, tpr,
                                                         g.out, &b.meta->status);
     ++nl;
   }
