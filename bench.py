@@ -11,9 +11,10 @@ before every timed step, outside its events.
 
 Also reported on the same line: ``e2e`` (the public ``knn_query`` call with
 host buffers, H2D and D2H inside the timed region), the loop of plain
-per-cloud calls, forward+backward and backward-only time, the query
-kernel's roofline, recall@K against an FP64 brute force (timed), and the
-reference's CPU kNN (nanoflann) timed on the host cores.
+per-cloud calls, forward+backward and backward-only time, the backward's
+error against FP64 finite differences, the query kernel's roofline,
+recall@K against an FP64 brute force (timed), and the reference's CPU kNN
+(nanoflann) timed on the host cores.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--k 16]
 Under torchrun every rank takes a share of the clouds (whole clouds, largest
@@ -442,6 +443,7 @@ def extras_single_gpu(args, fk, torch, dev, batch, voxel, flush):
         e1.synchronize()
         ms.append(e0.elapsed_time(e1))
     res["backward_ms"] = sum(ms) / reps
+    res["fd_check"] = fd_check(fk, torch, dev, batch, k, voxel)
     res["recall"] = fp64_recall(batch, idx.cpu().numpy(), k)
     res["rows"] = rows_single_gpu(fk, torch, dev, flush, measured_peak_hbm()[0])
     return res
@@ -639,6 +641,49 @@ def rows_only(args):
                                                        measured_peak_hbm()[0])}
 
 
+def fd_check(fk, torch, dev, batch, k, voxel, count=2048, h=1e-4):
+    """Max relative error (max-norm) of the backward's coordinate gradient of
+    L = sum w * d against FP64 central finite differences (step h metres,
+    neighbour indices held fixed) on a 2,048-point crop of the first cloud.
+    A perturbed point changes only the terms of its own row and of the rows
+    that name it, so only those are evaluated; the others cancel exactly."""
+    from flashknn_exprepo_b200 import synthetic
+    xyz = synthetic.crop(batch.xyz[: batch.offsets[0]], count,
+                         np.random.default_rng(synthetic.SEED))
+    n = len(xyz)
+    x = torch.from_numpy(xyz).to(dev).requires_grad_(True)
+    idx, d = fk.knn_query(k, x, torch.tensor([n], device=dev), voxel_size=voxel, num_down=2)
+    w = synthetic.backward_weights(n, k)
+    wt = torch.from_numpy(w).to(dev)
+    (wt * torch.isfinite(d).to(wt.dtype) * d.nan_to_num(posinf=0.0)).sum().backward()
+    got = x.grad.cpu().numpy().astype(np.float64)
+    ii = np.where(np.isfinite(d.detach().cpu().numpy()), idx.cpu().numpy(), -1)
+    w64 = w.astype(np.float64)
+    x64 = xyz.astype(np.float64)
+    rows_of = [[a] for a in range(n)]
+    for r, t in zip(*np.nonzero(ii >= 0)):
+        rows_of[ii[r, t]].append(r)
+
+    def loss(xs, rows):
+        sub = ii[rows]
+        ok = sub >= 0
+        dd = ((xs[rows][:, None, :] - xs[np.where(ok, sub, 0)]) ** 2).sum(-1)
+        return float((np.where(ok, w64[rows], 0.0) * dd).sum())
+
+    fd = np.zeros_like(x64)
+    for a in range(n):
+        rows = np.unique(rows_of[a])
+        for c in range(3):
+            xp = x64.copy()
+            xm = x64.copy()
+            xp[a, c] += h
+            xm[a, c] -= h
+            fd[a, c] = (loss(xp, rows) - loss(xm, rows)) / (2 * h)
+    err = float(np.abs(got - fd).max() / max(np.abs(fd).max(), 1e-30))
+    return {"max_rel_err": err, "target": 1e-4, "points": n, "h_m": h,
+            "what": "FP64 central differences of sum(w * d), indices held fixed"}
+
+
 def fp64_recall(batch, idx, k, per_cloud=256):
     """recall@K of the grid kNN against an exact FP64 brute force over whole
     clouds, on a seeded sample of queries per cloud; the brute force runs on
@@ -819,6 +864,8 @@ def main():
         line["batched_vs_per_cloud"] = out["value"] / out["per_cloud"]["value"]
     if "fwd_bwd_ms" in out:
         line["fwd_bwd_ms"] = out["fwd_bwd_ms"]
+    if "fd_check" in out:
+        line["fd_check"] = out["fd_check"]
     if kern:
         line["phases_ms"] = {"construction": out["ms_per_step"] - roofline["kernel_ms"],
                              "query": roofline["kernel_ms"],
