@@ -850,7 +850,8 @@ int run_adaptive(const AdaptiveArgs& f, void* ws, size_t ws_bytes, const QuerySh
     }
   }
   nl += launch_items(b.runs, b.group_start, b.group_row, &b.meta->n_groups, n, shape.tile_records,
-                     b.cands, b.seg_counts, &b.meta->n_items, b.items, s, &b.meta->status, n);
+                     b.cands, b.seg_counts, &b.meta->n_items, b.items, s, &b.meta->status, n,
+                     false);
   e = cudaGetLastError();
   if (e != cudaSuccess) {
     note_cuda_error(e);

@@ -183,6 +183,11 @@ __global__ void __launch_bounds__(256) k_bbox(PointSrc p, int4* __restrict__ pc,
   const int64_t last = min(base + 2047, p.n - 1);
   const int b_lo = cloud_of(p, base, status);
   const int b_hi = cloud_of(p, last, status);
+  // offset batching: a point of this tile below the end of b_lo is in b_lo,
+  // one below the end of b_lo + 1 = b_hi in b_hi; only others search
+  const bool by_offsets = p.offsets && !p.batch;
+  const int64_t end_lo = by_offsets ? p.offsets[b_lo] : 0;
+  const int64_t end_hi = by_offsets && b_hi == b_lo + 1 ? p.offsets[b_hi] : 0;
   Box6 lo, hi;
   lo.reset();
   hi.reset();
@@ -193,7 +198,10 @@ __global__ void __launch_bounds__(256) k_bbox(PointSrc p, int4* __restrict__ pc,
     const int gx = grid_axis(p, i, 0, status) >> p.num_down;
     const int gy = grid_axis(p, i, 1, status) >> p.num_down;
     const int gz = grid_axis(p, i, 2, status) >> p.num_down;
-    const int b = cloud_of(p, i, status);
+    const int b = !by_offsets ? cloud_of(p, i, status)
+                  : i < end_lo  ? b_lo
+                  : i < end_hi  ? b_hi
+                                : cloud_of(p, i, status);
     pc[i] = make_int4(gx, gy, gz, b);
     if (b == b_lo) {
       lo.add(gx, gy, gz);
@@ -451,35 +459,48 @@ __device__ __forceinline__ int2 hash_find(const HashSlot* table, uint32_t mask, 
   return make_int2(0, 0);  // no such cell: an empty run
 }
 
-// One thread per (group, neighbour position).  group_key[g] is a key in the
-// support key space; runs[g*27 + j] = (start, count) of the support cell at
-// offset j, or (0, 0) when that cell is empty.
+// One warp per group, one lane per neighbour position.  group_key[g] is a
+// key in the support key space; runs[g*27 + j] = (start, count) of the
+// support cell at offset j, or (0, 0) when that cell is empty.  With cands,
+// cands[g] = the group's candidate total (the work-item packer's input; a
+// group without candidates sets kStatusNoCandidates in *status).
 __global__ void __launch_bounds__(256)
     k_runs(const uint64_t* __restrict__ group_key, const int* group_count_ptr,
            const HashSlot* __restrict__ table, uint32_t hmask, const int* cell_count_ptr,
-           const Meta* meta, int2* __restrict__ runs) {
-  const int64_t total = static_cast<int64_t>(*group_count_ptr) * kNeighbours;
+           const Meta* meta, int2* __restrict__ runs, int32_t* __restrict__ cands,
+           int* status) {
+  const int groups = *group_count_ptr;
   const int bpa = meta->bpa;
   const int cells = *cell_count_ptr;
   const uint64_t mask = bpa ? ((1ull << (3 * bpa)) - 1) : 0ull;
   const int lim = 1 << bpa;
-  for (int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; t < total;
-       t += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    const int g = static_cast<int>(t / kNeighbours), j = static_cast<int>(t % kNeighbours);
-    const uint64_t key = group_key[g];
-    const uint64_t cloud = key >> (3 * bpa);
-    const uint64_t m = key & mask;
-    const int x = static_cast<int>(compact3(m >> 2)) + axis_offset(j / 9);
-    const int y = static_cast<int>(compact3(m >> 1)) + axis_offset((j / 3) % 3);
-    const int z = static_cast<int>(compact3(m)) + axis_offset(j % 3);
+  const int j = threadIdx.x & 31;
+  const int64_t warps = (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5;
+  for (int64_t g = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+       g < groups; g += warps) {
     int2 run = make_int2(0, 0);
-    if (cells > 0 && x >= 0 && y >= 0 && z >= 0 && x < lim && y < lim && z < lim) {
-      const uint64_t nk = (cloud << (3 * bpa)) |
-                          morton3(static_cast<uint32_t>(x), static_cast<uint32_t>(y),
-                                  static_cast<uint32_t>(z));
-      run = hash_find(table, hmask, nk);
+    if (j < kNeighbours) {
+      const uint64_t key = group_key[g];
+      const uint64_t cloud = key >> (3 * bpa);
+      const uint64_t m = key & mask;
+      const int x = static_cast<int>(compact3(m >> 2)) + axis_offset(j / 9);
+      const int y = static_cast<int>(compact3(m >> 1)) + axis_offset((j / 3) % 3);
+      const int z = static_cast<int>(compact3(m)) + axis_offset(j % 3);
+      if (cells > 0 && x >= 0 && y >= 0 && z >= 0 && x < lim && y < lim && z < lim) {
+        const uint64_t nk = (cloud << (3 * bpa)) |
+                            morton3(static_cast<uint32_t>(x), static_cast<uint32_t>(y),
+                                    static_cast<uint32_t>(z));
+        run = hash_find(table, hmask, nk);
+      }
+      runs[g * kNeighbours + j] = run;
     }
-    runs[t] = run;
+    if (cands) {
+      const int total = __reduce_add_sync(kFull, run.y);
+      if (j == 0) {
+        cands[g] = total;
+        if (total == 0) raise_status(status, kStatusNoCandidates);
+      }
+    }
   }
 }
 
@@ -509,7 +530,8 @@ __global__ void __launch_bounds__(256)
   const unsigned peers = __match_any_sync(vmask, c);
   const int leader = __ffs(peers) - 1;
   uint32_t before = 0u;
-  if ((threadIdx.x & 31) == leader) before = atomicAdd(&qcount[c], static_cast<uint32_t>(__popc(peers)));
+  if ((threadIdx.x & 31) == leader)
+    before = atomicAdd(&qcount[c], static_cast<uint32_t>(__popc(peers)));
   before = __shfl_sync(peers, before, leader);
   cell_r[r] = c;
   rank_r[r] = before + __popc(peers & lanemask_lt());
@@ -763,12 +785,13 @@ int run_fused(const FusedArgs& f, void* ws, size_t ws_bytes, const QueryShape& s
 
   if (kind == FKNN_QUERY_SELF) {
     if (n > 0) {
-      k_runs<<<capped_blocks(n * kNeighbours), 256, 0, s>>>(
-          b.cell_key, &b.meta->n_cells, b.hslots, hmask, &b.meta->n_cells, b.meta,
-          b.runs);
+      k_runs<<<capped_blocks(n * 32), 256, 0, s>>>(b.cell_key, &b.meta->n_cells, b.hslots, hmask,
+                                                   &b.meta->n_cells, b.meta, b.runs, b.cands,
+                                                   &b.meta->status);
       ++nl;
       nl += launch_items(b.runs, b.cell_start, nullptr, &b.meta->n_cells, n, shape.tile_records,
-                         b.cands, b.seg_counts, &b.meta->n_items, b.items, s, &b.meta->status, n);
+                         b.cands, b.seg_counts, &b.meta->n_items, b.items, s, &b.meta->status, n,
+                         true);
     }
   } else if (kind == FKNN_QUERY_SELECTED) {
     pad_mode = kPadArray64;
@@ -779,9 +802,9 @@ int run_fused(const FusedArgs& f, void* ws, size_t ws_bytes, const QueryShape& s
     group_row = b.group_row;
     group_count_ptr = &b.meta->n_groups;
     if (n > 0) {
-      k_runs<<<capped_blocks(n * kNeighbours), 256, 0, s>>>(
-          b.cell_key, &b.meta->n_cells, b.hslots, hmask, &b.meta->n_cells, b.meta,
-          b.runs);
+      k_runs<<<capped_blocks(n * 32), 256, 0, s>>>(b.cell_key, &b.meta->n_cells, b.hslots, hmask,
+                                                   &b.meta->n_cells, b.meta, b.runs, nullptr,
+                                                   nullptr);
       ++nl;
     }
     if (m > 0 && n > 0) {
@@ -803,7 +826,7 @@ int run_fused(const FusedArgs& f, void* ws, size_t ws_bytes, const QueryShape& s
       nl += 6;
       nl += launch_items(b.runs, b.group_start, b.group_row, &b.meta->n_groups, m,
                          shape.tile_records, b.cands, b.seg_counts, &b.meta->n_items, b.items, s,
-                         &b.meta->status, m);
+                         &b.meta->status, m, false);
     }
   } else {  // general queries
     pad_mode = kPadMinusOne;
@@ -835,12 +858,13 @@ int run_fused(const FusedArgs& f, void* ws, size_t ws_bytes, const QueryShape& s
                                                    b.qslots, nullptr, b.qrec, nullptr, nullptr,
                                                    &b.meta->status);
       nl += 5;
-      k_runs<<<capped_blocks(m * kNeighbours), 256, 0, s>>>(
-          b.group_key, &b.meta->n_groups, b.hslots, hmask, &b.meta->n_cells,
-          b.meta, b.runs);
+      k_runs<<<capped_blocks(m * 32), 256, 0, s>>>(b.group_key, &b.meta->n_groups, b.hslots, hmask,
+                                                   &b.meta->n_cells, b.meta, b.runs, b.cands,
+                                                   &b.meta->status);
       ++nl;
       nl += launch_items(b.runs, b.group_start, nullptr, &b.meta->n_groups, m, shape.tile_records,
-                         b.cands, b.seg_counts, &b.meta->n_items, b.items, s, &b.meta->status, m);
+                         b.cands, b.seg_counts, &b.meta->n_items, b.items, s, &b.meta->status, m,
+                         true);
     }
   }
 

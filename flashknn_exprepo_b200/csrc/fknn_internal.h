@@ -77,7 +77,7 @@ int launch_query(const QueryLaunch& q, const QueryShape& shape, cudaStream_t s);
 int launch_items(const int2* runs, const int32_t* group_start, const int32_t* group_row,
                  const int* group_count_ptr, int64_t max_groups, int tile, int32_t* cands,
                  uint32_t* seg_counts, int* n_items_ptr, int4* items, cudaStream_t s,
-                 int* status, int64_t n_queries);
+                 int* status, int64_t n_queries, bool cands_ready);
 size_t items_capacity(int64_t max_groups, int64_t n_queries);
 // Bounded-wait self-test (fknn_selftest.cu): arms a barrier that never
 // completes and waits at most `limit` polls; sets kStatusTimeout.

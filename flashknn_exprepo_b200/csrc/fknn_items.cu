@@ -133,21 +133,22 @@ __global__ void __launch_bounds__(1024)
 int launch_items(const int2* runs, const int32_t* group_start, const int32_t* group_row,
                  const int* group_count_ptr, int64_t max_groups, int tile, int32_t* cands,
                  uint32_t* seg_counts, int* n_items_ptr, int4* items, cudaStream_t s,
-                 int* status, int64_t n_queries) {
+                 int* status, int64_t n_queries, bool cands_ready) {
   if (max_groups <= 0) return 0;
   // grids for the host-side bound, capped: the device count drives the loops
   const int64_t gb = ceil_div(max_groups, 256);
   const int gblocks = static_cast<int>(gb < 2048 ? gb : 2048);
   const int64_t sb = ceil_div(ceil_div(max_groups, kPackSegment), 256);
   const int sblocks = static_cast<int>(sb < 1024 ? sb : 1024);
-  k_group_cands<<<gblocks, 256, 0, s>>>(runs, group_row, group_count_ptr, cands, status);
+  if (!cands_ready)  // else the caller's run kernel wrote cands[g] already
+    k_group_cands<<<gblocks, 256, 0, s>>>(runs, group_row, group_count_ptr, cands, status);
   const int64_t capacity = static_cast<int64_t>(items_capacity(max_groups, n_queries));
   k_pack<<<sblocks, 256, 0, s>>>(group_start, cands, group_count_ptr, tile, n_queries, capacity,
                                  seg_counts, nullptr, nullptr, status);
   k_scan_segments<<<1, 1024, 0, s>>>(seg_counts, group_count_ptr, capacity, n_items_ptr, status);
   k_pack<<<sblocks, 256, 0, s>>>(group_start, cands, group_count_ptr, tile, n_queries, capacity,
                                  nullptr, seg_counts, items, status);
-  return 4;
+  return cands_ready ? 3 : 4;
 }
 
 size_t items_capacity(int64_t max_groups, int64_t n_queries) {

@@ -156,7 +156,7 @@ int run_tables(const TablesArgs& t, void* ws, size_t ws_bytes, const QueryShape&
   if (t.p > 0)
     nl += launch_items(b.runs, selected ? t.steps_query : t.steps, nullptr, &b.meta->n_groups, t.p,
                        shape.tile_records, b.cands, b.seg_counts, &b.meta->n_items, b.items, s,
-                       &b.meta->status, selected ? m : t.n);
+                       &b.meta->status, selected ? m : t.n, false);
   e = cudaGetLastError();
   if (e != cudaSuccess) {
     note_cuda_error(e);
