@@ -1,5 +1,6 @@
-// Stable LSD radix sort (8-bit digits) and tile scans used by the grid
-// construction and the backward pass.
+// Stable LSD radix sort (8-bit digits), used by the reference-table
+// construction and the adaptive octree, and the block / tile scans used by
+// every construction pass and the backward.
 //
 // Counting sort per digit, three launches per pass:
 //   hist    -- per 2048-key tile, a 256-bin histogram built with
