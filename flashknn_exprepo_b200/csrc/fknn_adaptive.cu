@@ -18,28 +18,27 @@
 // B200 layout.  The points are sorted once by (batch, morton(translated
 // grid)); in that order every node of every level is a contiguous range, so
 // no coordinates are copied per level (the reference gathers a copy of every
-// referenced support node, :605-608).  Once for all levels:
+// referenced support node, :605-608).  Node boundaries, node sizes and the
+// 27-node candidate counts do not depend on the selection, so every level is
+// built at once:
 //   ka_heads_all / ka_scan_all           node heads per tile and level (the
 //                                        highest bit in which neighbouring
 //                                        keys differ), scanned per level
-// then per level, from the coarsest down (four launches):
-//   ka_nodes                             node starts; empties the table
-//                                        last used two levels up
-//   ka_insert                            open-addressing table: node key ->
-//                                        (start, count); two tables alternate
-//                                        between consecutive levels
-//   ka_counts                            27-node candidate count per node
-//   ka_select                            per-point level selection step;
-//                                        points that stopped one level up
-//                                        open query groups there and write
-//                                        their 27 (start, count) runs
-// and ka_finalize opens the groups of the points that reach level 0.
+//   ka_level_bases / ka_table_clear      node numbering across levels, table
+//                                        capacity
+//   ka_nodes_all                         node starts of every level
+//   ka_insert_all                        one table for all levels: level key
+//                                        -> (start, count)
+//   ka_counts_all                        27-node candidate count of every node
+//   ka_select_all                        per point: its level, walking the
+//                                        levels from the top in registers;
+//                                        group starts write their 27 runs
 // A query group is a maximal run of sorted points with the same selected
 // level and node; its runs address the same sorted records as its queries,
 // so the packer and the top-K kernel of the fixed-level path serve it
-// unchanged (fknn_items.cu, fknn_query.cu).  Every data-dependent size stays
-// on the device: the pipeline is a fixed launch sequence (levels above the
-// device-side S return at once) and can be captured in a CUDA graph.
+// unchanged (fknn_items.cu, fknn_query.cu).  Every data-dependent size (the
+// top level S included) stays on the device: the pipeline is a fixed launch
+// sequence and can be captured in a CUDA graph.
 #include <climits>
 
 #include "fknn_common.cuh"
@@ -54,7 +53,6 @@ namespace {
 constexpr int kMaxLevel = 16;
 constexpr int kBatchSlots = 32768;
 constexpr int kTile = 2048;  // sorted positions per 256-thread CTA (8 each)
-constexpr uint64_t kEmptyKey = ~0ull;
 
 // Meta fields: bpa = bits per axis of the key layout, reserved[0] = S (top
 // level), reserved[1] = largest batch id + 1, key_bits = 3 * bpa + batch bits.
@@ -70,32 +68,12 @@ __device__ __forceinline__ uint32_t slot_of_key(uint64_t key, uint32_t mask) {
   return static_cast<uint32_t>(key) & mask;
 }
 
-// One 16-byte slot: node key and its run, so a probe is a single load.
+// One 16-byte slot of the node table: level key (0 = empty) and the node's
+// run (start, count).
 struct __align__(16) Slot {
   uint64_t key;
   int2 run;
 };
-
-struct Table {
-  Slot* slots;
-  uint32_t mask;
-};
-
-__device__ __forceinline__ int2 table_find(const Table& t, uint64_t key) {
-  uint32_t h = slot_of_key(key, t.mask);
-  for (uint32_t probe = 0; probe <= t.mask; ++probe) {
-    const ulonglong2 v = __ldcg(reinterpret_cast<const ulonglong2*>(t.slots + h));
-    if (v.x == key) {
-      int2 r;
-      r.x = static_cast<int>(static_cast<uint32_t>(v.y));
-      r.y = static_cast<int>(static_cast<uint32_t>(v.y >> 32));
-      return r;
-    }
-    if (v.x == kEmptyKey) break;
-    h = (h + 1) & t.mask;
-  }
-  return make_int2(0, 0);
-}
 
 __device__ __forceinline__ const uint64_t* sorted_keys(const SortPair<uint64_t>& sp,
                                                        const int* bits) {
@@ -109,24 +87,6 @@ __device__ __forceinline__ const uint32_t* sorted_vals(const SortPair<uint64_t>&
 
 __device__ __forceinline__ bool node_head(const uint64_t* key, int64_t p, int shift) {
   return p == 0 || (key[p] >> shift) != (key[p - 1] >> shift);
-}
-
-// Neighbour j of the node with key nk at level s: runs of the 27 offsets in
-// the reference's order (centre first, (0,-1,+1)^3 ij), or (0,0).
-__device__ __forceinline__ int2 neighbour_run(const Table& t, uint64_t nk, int s, int bpa,
-                                              int j) {
-  const int sb = 3 * (bpa - s);  // spatial bits of a level-s node key
-  const uint64_t batch = nk >> sb;
-  const uint64_t m = sb ? (nk & ((1ull << sb) - 1)) : 0ull;
-  const int lim = 1 << (bpa - s);
-  const int x = static_cast<int>(compact3(m >> 2)) + (j / 9 == 0 ? 0 : (j / 9 == 1 ? -1 : 1));
-  const int jy = (j / 3) % 3, jz = j % 3;
-  const int y = static_cast<int>(compact3(m >> 1)) + (jy == 0 ? 0 : (jy == 1 ? -1 : 1));
-  const int z = static_cast<int>(compact3(m)) + (jz == 0 ? 0 : (jz == 1 ? -1 : 1));
-  if (x < 0 || y < 0 || z < 0 || x >= lim || y >= lim || z >= lim) return make_int2(0, 0);
-  const uint64_t key = (batch << sb) | morton3(static_cast<uint32_t>(x), static_cast<uint32_t>(y),
-                                               static_cast<uint32_t>(z));
-  return table_find(t, key);
 }
 
 }  // namespace
@@ -377,255 +337,240 @@ __global__ void __launch_bounds__(1024)
   if (threadIdx.x == 0) level_nodes[blockIdx.x] = static_cast<int>(carry);
 }
 
-// ---- per-level passes (device functions over an explicit tile, thread or
-// warp range; the kernels below launch them, four per level).  Arrays that a
-// pass rewrites on every level (node starts, node of, counts, selection,
-// slots) are read with ld.global.cg, straight from L2.
+// ---- all levels at once.  Node boundaries, node tables and 27-node counts
+// do not depend on the selection, so they are built for every level in one
+// pass each; only the selection walks the levels, per point, in registers.
+//
+// One open-addressing table holds the nodes of every level under the key
+// level_key(key, s) = (key >> 3s) | 2^(63 - 3s): keys have at most 63 bits,
+// so a level-s node key has at most 63 - 3s bits and the marker bit keeps the
+// levels' key ranges disjoint (and every key non-zero: 0 marks an empty slot).
+// A slot holds the node's run (start, count); cand_slot[slot] its 27-node
+// candidate count.  Global node g of level s is node g - base[s] of that
+// level; base[s + 1] = base[s] + nodes(s) + 1 (one sentinel per level), so
+// node_start[g + 1] - node_start[g] is always the node's size.
 
-// Positions of tile `tile` (kTile of them, 8 per thread of a 256-thread CTA):
-// node_of[p] = node of sorted position p at level s; node_start[c] = first
-// position of node c, node_start[nodes] = n.  Called by every thread of the
-// CTA (block-wide scan).
-__device__ __forceinline__ void nodes_tile(const LevelArgs& a, int tile,
-                                           const uint32_t* __restrict__ tile_offsets, int nodes,
-                                           int32_t* __restrict__ node_of,
-                                           int32_t* __restrict__ node_start, uint32_t* warp_sums) {
-  const uint64_t* key = sorted_keys(a.sp, a.bits);
-  const int64_t base = static_cast<int64_t>(tile) * kTile + threadIdx.x * 8;
-  uint32_t flags = 0, heads = 0;
-#pragma unroll
-  for (int r = 0; r < 8; ++r) {
-    const int64_t p = base + r;
-    if (p < a.n && node_head(key, p, 3 * a.s)) {
-      flags |= 1u << r;
-      ++heads;
-    }
-  }
-  const uint32_t incl = block_inclusive_scan(heads, warp_sums, nullptr);
-  int c = static_cast<int>(tile_offsets[tile] + incl - heads) - 1;
-#pragma unroll
-  for (int r = 0; r < 8; ++r) {
-    const int64_t p = base + r;
-    if (p >= a.n) break;
-    if (flags & (1u << r)) {
-      ++c;
-      node_start[c] = static_cast<int32_t>(p);
-    }
-    node_of[p] = c;
-    if (p == a.n - 1) node_start[nodes] = static_cast<int32_t>(a.n);
-  }
+__device__ __forceinline__ uint64_t level_key(uint64_t key, int s) {
+  return (key >> (3 * s)) | (1ull << (63 - 3 * s));
 }
 
-// Empties the `stale` slots listed in slot_of (the nodes a table held two
-// levels up), so the table can take this level's nodes.
-__device__ __forceinline__ void erase_nodes(int64_t t, int64_t stride, int stale,
-                                            const int32_t* __restrict__ slot_of,
-                                            Slot* __restrict__ table) {
-  for (int64_t c = t; c < stale; c += stride) table[__ldcg(slot_of + c)].key = kEmptyKey;
-}
-
-// Node key -> (start, count) into the table of this level; the slot is kept
-// for the erase.  One thread per node.
-__device__ __forceinline__ void insert_nodes(const LevelArgs& a, int64_t t, int64_t stride,
-                                             int nodes, const int32_t* __restrict__ node_start,
-                                             const Table& tab, int32_t* __restrict__ slot_of) {
-  const uint64_t* key = sorted_keys(a.sp, a.bits);
-  for (int64_t c = t; c < nodes; c += stride) {
-    const int32_t st = __ldcg(node_start + c);
-    const uint64_t nk = key[st] >> (3 * a.s);
-    uint32_t h = slot_of_key(nk, tab.mask);
-    for (uint32_t probe = 0; probe <= tab.mask; ++probe) {
-      const unsigned long long prev =
-          atomicCAS(reinterpret_cast<unsigned long long*>(&tab.slots[h].key), kEmptyKey, nk);
-      if (prev == kEmptyKey) {
-        tab.slots[h].run = make_int2(st, __ldcg(node_start + c + 1) - st);
-        slot_of[c] = static_cast<int32_t>(h);
-        break;
-      }
-      h = (h + 1) & tab.mask;
-    }
-  }
-}
-
-// cand[c] = points in the 27 nodes around node c.  One warp per node, one
-// lookup per lane, so the 27 probes are in flight together.  Below the top
-// level only points still active read their count, so a node of at most
-// kScanActive points none of which is active (act_in, the previous level's
-// flags) is skipped.
-constexpr int kScanActive = 128;
-
-__device__ __forceinline__ void count_nodes(const LevelArgs& a, int top, int64_t w,
-                                            int64_t wstride, int nodes,
-                                            const int32_t* __restrict__ node_start,
-                                            const Table& tab, const uint8_t* __restrict__ act_in,
-                                            int32_t* __restrict__ cand) {
-  const uint64_t* key = sorted_keys(a.sp, a.bits);
-  const int bpa = a.meta->bpa;
-  const int lane = threadIdx.x & 31;
-  for (int64_t c = w; c < nodes; c += wstride) {
-    const int32_t st = __ldcg(node_start + c);
-    if (a.s < top) {
-      const int32_t len = __ldcg(node_start + c + 1) - st;
-      if (len <= kScanActive) {
-        bool any = false;
-#pragma unroll
-        for (int i = 0; i < kScanActive / 32; ++i) {
-          const int j = lane + 32 * i;
-          any |= j < len && __ldcg(act_in + st + j) != 0;
-        }
-        if (!__any_sync(kFull, any)) continue;
-      }
-    }
-    const uint64_t nk = key[st] >> (3 * a.s);
-    const int len = lane < kNeighbours ? neighbour_run(tab, nk, a.s, bpa, lane).y : 0;
-    const int total = __reduce_add_sync(kFull, len);
-    if (lane == 0) cand[c] = total;
-  }
-}
-
-// New (level, active) of sorted position q after the step at level s; only
-// points still active read their node's count.
-__device__ __forceinline__ void select_step(int64_t q, int s, int top,
-                                            const int32_t* __restrict__ node_of,
-                                            const int32_t* __restrict__ cand,
-                                            const uint8_t* __restrict__ sel_in,
-                                            const uint8_t* __restrict__ act_in, int min_count,
-                                            int max_count, uint8_t* sel_new, uint8_t* act_new) {
-  if (s == top) {
-    *sel_new = static_cast<uint8_t>(top);
-    *act_new = __ldcg(cand + __ldcg(node_of + q)) > max_count;
-  } else if (__ldcg(act_in + q)) {
-    const int cnt = __ldcg(cand + __ldcg(node_of + q));
-    const bool use = cnt >= min_count;
-    *sel_new = use ? static_cast<uint8_t>(s) : __ldcg(sel_in + q);
-    *act_new = use && cnt > max_count;
-  } else {
-    *sel_new = __ldcg(sel_in + q);
-    *act_new = 0;
-  }
-}
-
-struct SelectArgs {
-  const int32_t* node_of;
-  const int32_t* cand;
-  int min_count, max_count;
-  const uint8_t* sel_in;
-  const uint8_t* act_in;
-  uint8_t* sel_out;
-  uint8_t* act_out;
-  Table t_up;  // table of level s + 1
-  uint8_t* group_flag;
-  int2* runs;
+struct LTable {
+  Slot* slots;
+  const int* mask_word;  // capacity - 1, set on the device
 };
 
-// One step of the coarse-to-fine level selection, fused with the
-// finalisation of level s+1: points whose selection stays at s+1 open their
-// query groups there (a group is a maximal run of sorted positions with the
-// same level and level-(s+1) node) and write the group's 27 runs (row p).
-// The new selection goes to sel_out / act_out, the previous one is read from
-// sel_in / act_in, so a warp can recompute its left neighbour's new level
-// without racing the warp that writes it.  One warp per 32 positions.
-__device__ __forceinline__ void select_positions(const LevelArgs& a, int top, int64_t w,
-                                                 int64_t wstride, const SelectArgs& g) {
+__device__ __forceinline__ int level_find(const Slot* slots, uint32_t mask, uint64_t v) {
+  uint32_t h = slot_of_key(v, mask);
+  for (uint32_t probe = 0; probe <= mask; ++probe) {
+    const uint64_t k = __ldcg(&slots[h].key);
+    if (k == v) return static_cast<int>(h);
+    if (k == 0ull) break;
+    h = (h + 1) & mask;
+  }
+  return -1;
+}
+
+// Run of neighbour j of the level-s node with node key nk (table slot), or
+// (0, 0) when the neighbour is outside the grid or empty.
+__device__ __forceinline__ int level_neighbour_slot(const Slot* slots, uint32_t mask, uint64_t nk,
+                                                   int s, int bpa, int j) {
+  const int sb = 3 * (bpa - s);  // spatial bits of a level-s node key
+  const uint64_t batch = nk >> sb;
+  const uint64_t m = sb ? (nk & ((1ull << sb) - 1)) : 0ull;
+  const int lim = 1 << (bpa - s);
+  const int x = static_cast<int>(compact3(m >> 2)) + (j / 9 == 0 ? 0 : (j / 9 == 1 ? -1 : 1));
+  const int jy = (j / 3) % 3, jz = j % 3;
+  const int y = static_cast<int>(compact3(m >> 1)) + (jy == 0 ? 0 : (jy == 1 ? -1 : 1));
+  const int z = static_cast<int>(compact3(m)) + (jz == 0 ? 0 : (jz == 1 ? -1 : 1));
+  if (x < 0 || y < 0 || z < 0 || x >= lim || y >= lim || z >= lim) return -1;
+  const uint64_t key = (batch << sb) | morton3(static_cast<uint32_t>(x), static_cast<uint32_t>(y),
+                                               static_cast<uint32_t>(z));
+  return level_find(slots, mask, key | (1ull << (63 - 3 * s)));
+}
+
+// Level of global node g (base[] has top + 2 entries).
+__device__ __forceinline__ int level_of_node(const int* base, int top, int64_t g) {
+  int s = 0;
+  while (s < top && g >= base[s + 1]) ++s;
+  return s;
+}
+
+// Meta words of the all-levels pipeline.
+__device__ __forceinline__ int* level_mask_word(Meta* m) { return &m->reserved[2]; }
+
+// One warp: base[s] for s = 0..top+1 and the table mask (capacity = next
+// power of two >= 2 x all nodes).
+__global__ void ka_level_bases(const int* __restrict__ level_nodes, Meta* meta,
+                               int* __restrict__ base, int64_t max_cap) {
+  if (threadIdx.x != 0) return;
+  const int top = top_level(meta);
+  int b = 0;
+  for (int s = 0; s <= top; ++s) {
+    base[s] = b;
+    b += level_nodes[s] + 1;
+  }
+  base[top + 1] = b;
+  int64_t cap = 16;
+  while (cap < 2 * static_cast<int64_t>(b)) cap <<= 1;
+  if (cap > max_cap) {  // cannot happen: b <= (top + 1) * (n + 1)
+    raise_status(&meta->status, kStatusTable);
+    cap = max_cap;
+  }
+  *level_mask_word(meta) = static_cast<int>(cap - 1);
+}
+
+__global__ void __launch_bounds__(256)
+    ka_table_clear(Slot* __restrict__ slots, const Meta* meta) {
+  const int64_t cap = static_cast<int64_t>(static_cast<uint32_t>(meta->reserved[2])) + 1;
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < cap;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    slots[i].key = 0ull;
+}
+
+// Head level of sorted position p: p heads the nodes of levels 0..hl, or
+// hl = -1 when its key equals its predecessor's.
+__device__ __forceinline__ int head_level(const uint64_t* key, int64_t p) {
+  if (p == 0) return kMaxLevel;
+  const uint64_t x = key[p] ^ key[p - 1];
+  if (x == 0) return -1;
+  return min((63 - __clzll(static_cast<long long>(x))) / 3, kMaxLevel);
+}
+
+// Node starts of every level: tile of 2048 positions, 8 per thread, one
+// block scan per level over the precomputed per-level tile offsets.
+__global__ void __launch_bounds__(256)
+    ka_nodes_all(LevelArgs a, int n_tiles, const uint32_t* __restrict__ tile_offsets,
+                 const int* __restrict__ level_nodes, const int* __restrict__ base,
+                 int32_t* __restrict__ node_start) {
+  __shared__ uint32_t warp_sums[32];
+  const int top = top_level(a.meta);
   const uint64_t* key = sorted_keys(a.sp, a.bits);
-  const int bpa = a.meta->bpa;
-  const int L = a.s + 1;  // level finalised here (when <= top)
-  const int lane = threadIdx.x & 31;
-  for (int64_t base = w * 32; base < a.n; base += wstride * 32) {
-    const int64_t p = base + lane;
-    uint8_t ns = 0xff, na = 0;
-    if (p < a.n) {
-      select_step(p, a.s, top, g.node_of, g.cand, g.sel_in, g.act_in, g.min_count, g.max_count,
-                  &ns, &na);
-      g.sel_out[p] = ns;
-      g.act_out[p] = na;
-    }
-    if (L > top) continue;
-    uint8_t prev = static_cast<uint8_t>(__shfl_up_sync(kFull, ns, 1));
-    if (lane == 0 && p > 0 && p < a.n) {  // the previous warp's last position
-      uint8_t pa;
-      select_step(p - 1, a.s, top, g.node_of, g.cand, g.sel_in, g.act_in, g.min_count,
-                  g.max_count, &prev, &pa);
-    }
-    bool start = false;
-    if (p < a.n && ns == L) {
-      start = p == 0 || prev != L || node_head(key, p, 3 * L);
-      g.group_flag[p] = start ? 1 : 0;
-    }
-    uint32_t starts = __ballot_sync(kFull, start);
-    while (starts) {
-      const int src = __ffs(starts) - 1;
-      starts &= starts - 1;
-      const int64_t ps = base + src;
-      if (lane < kNeighbours)
-        g.runs[ps * kNeighbours + lane] = neighbour_run(g.t_up, key[ps] >> (3 * L), L, bpa, lane);
+  const int64_t p0 = static_cast<int64_t>(blockIdx.x) * kTile + threadIdx.x * 8;
+  int hl[8];
+#pragma unroll
+  for (int r = 0; r < 8; ++r) hl[r] = p0 + r < a.n ? head_level(key, p0 + r) : -1;
+  for (int s = 0; s <= top; ++s) {
+    uint32_t heads = 0;
+#pragma unroll
+    for (int r = 0; r < 8; ++r) heads += hl[r] >= s ? 1u : 0u;
+    const uint32_t incl = block_inclusive_scan(heads, warp_sums, nullptr);
+    int64_t g = base[s] + static_cast<int64_t>(tile_offsets[static_cast<int64_t>(s) * n_tiles +
+                                                            blockIdx.x]) + incl - heads;
+#pragma unroll
+    for (int r = 0; r < 8; ++r)
+      if (hl[r] >= s) node_start[g++] = static_cast<int32_t>(p0 + r);
+    if (p0 <= a.n - 1 && a.n - 1 < p0 + 8)  // the sentinel after the level's last node
+      node_start[base[s] + level_nodes[s]] = static_cast<int32_t>(a.n);
+  }
+}
+
+// Every node of every level into the table: (start, count) under its level
+// key; slot_of_node[g] = its slot.  One thread per global node.
+__global__ void __launch_bounds__(256)
+    ka_insert_all(LevelArgs a, const int* __restrict__ base, const int32_t* __restrict__ node_start,
+                  Slot* __restrict__ slots, int32_t* __restrict__ slot_of_node) {
+  const int top = top_level(a.meta);
+  const uint32_t mask = static_cast<uint32_t>(a.meta->reserved[2]);
+  const uint64_t* key = sorted_keys(a.sp, a.bits);
+  const int64_t total = base[top + 1];
+  for (int64_t g = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; g < total;
+       g += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int s = level_of_node(base, top, g);
+    if (g == base[s + 1] - 1) continue;  // the level's sentinel
+    const int32_t st = node_start[g];
+    const uint64_t v = level_key(key[st], s);
+    uint32_t h = slot_of_key(v, mask);
+    for (uint32_t probe = 0; probe <= mask; ++probe) {
+      const unsigned long long prev =
+          atomicCAS(reinterpret_cast<unsigned long long*>(&slots[h].key), 0ull, v);
+      if (prev == 0ull) {
+        slots[h].run = make_int2(st, node_start[g + 1] - st);
+        slot_of_node[g] = static_cast<int32_t>(h);
+        break;
+      }
+      h = (h + 1) & mask;
     }
   }
 }
 
-// ---- per-level kernels
-
-// Also empties the table this level is about to reuse: it still holds the
-// nodes of level s+2 (erase_count of them, at erase_slot), whose last reader
-// was the finalisation of level s+2 in the previous step.
+// cand_slot[slot of node] = points in the 27 same-level nodes around it.
+// One warp per node, one lookup per lane.
 __global__ void __launch_bounds__(256)
-    ka_nodes(LevelArgs a, const uint32_t* __restrict__ tile_offsets, const int* count_ptr,
-             int32_t* __restrict__ node_of, int32_t* __restrict__ node_start,
-             const int* erase_count, const int32_t* __restrict__ erase_slot,
-             Slot* __restrict__ table) {
-  __shared__ uint32_t warp_sums[32];
+    ka_counts_all(LevelArgs a, const int* __restrict__ base,
+                  const int32_t* __restrict__ node_start, const Slot* __restrict__ slots,
+                  const int32_t* __restrict__ slot_of_node, int32_t* __restrict__ cand_slot) {
   const int top = top_level(a.meta);
-  if (a.s > top) return;
-  if (a.s + 2 <= top)
-    erase_nodes(static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x,
-                static_cast<int64_t>(gridDim.x) * blockDim.x, *erase_count, erase_slot, table);
-  nodes_tile(a, blockIdx.x, tile_offsets, *count_ptr, node_of, node_start, warp_sums);
-}
-
-__global__ void __launch_bounds__(256)
-    ka_insert(LevelArgs a, const int* count_ptr, const int32_t* __restrict__ node_start, Table t,
-              int32_t* __restrict__ slot_of) {
-  if (a.s > top_level(a.meta)) return;
-  insert_nodes(a, static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x,
-               static_cast<int64_t>(gridDim.x) * blockDim.x, *count_ptr, node_start, t, slot_of);
-}
-
-__global__ void __launch_bounds__(256)
-    ka_counts(LevelArgs a, const int* count_ptr, const int32_t* __restrict__ node_start, Table t,
-              const uint8_t* __restrict__ act_in, int32_t* __restrict__ cand) {
-  const int top = top_level(a.meta);
-  if (a.s > top) return;
-  count_nodes(a, top, (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5,
-              (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5, *count_ptr, node_start, t,
-              act_in, cand);
-}
-
-__global__ void __launch_bounds__(256) ka_select(LevelArgs a, SelectArgs g) {
-  const int top = top_level(a.meta);
-  if (a.s > top) return;
-  select_positions(a, top, (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5,
-                   (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5, g);
-}
-
-// Points whose selection stopped at level L open their query groups: a
-// group is a maximal run of sorted positions with level L and the same
-// level-L node.  group_flag[p] and the group's 27 runs (row p).  One warp per
-// 32 consecutive points: every lane decides for its point, then the warp
-// looks up the 27 runs of each group start together, one run per lane.
-__global__ void __launch_bounds__(256)
-    ka_finalize(LevelArgs a, int L, Table t, const uint8_t* __restrict__ sel,
-                uint8_t* __restrict__ group_flag, int2* __restrict__ runs) {
-  if (L > top_level(a.meta)) return;
-  const uint64_t* key = sorted_keys(a.sp, a.bits);
+  const uint32_t mask = static_cast<uint32_t>(a.meta->reserved[2]);
   const int bpa = a.meta->bpa;
+  const uint64_t* key = sorted_keys(a.sp, a.bits);
+  const int64_t total = base[top + 1];
   const int lane = threadIdx.x & 31;
-  const int64_t warps = static_cast<int64_t>(gridDim.x) * (blockDim.x >> 5);
-  for (int64_t base = (static_cast<int64_t>(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5)) * 32;
+  const int64_t warps = (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5;
+  for (int64_t g = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; g < total;
+       g += warps) {
+    const int s = level_of_node(base, top, g);
+    if (g == base[s + 1] - 1) continue;  // sentinel (warp-uniform)
+    const uint64_t nk = key[node_start[g]] >> (3 * s);
+    int len = 0;
+    if (lane < kNeighbours) {
+      const int h = level_neighbour_slot(slots, mask, nk, s, bpa, lane);
+      if (h >= 0) len = __ldcg(&slots[h].run.y);
+    }
+    const int t = __reduce_add_sync(kFull, len);
+    if (lane == 0) cand_slot[slot_of_node[g]] = t;
+  }
+}
+
+// Selected level of sorted position q: from the top level down, an active
+// point moves to level s when its level-s count is >= min_count and stays
+// active while it is > max_count (adaptive_octree.py:312-351).
+__device__ __forceinline__ int select_level(const uint64_t* key, int64_t q, int top,
+                                            const Slot* slots, uint32_t mask,
+                                            const int32_t* cand_slot, int min_count,
+                                            int max_count) {
+  const uint64_t k = key[q];
+  int sel = top;
+  int h = level_find(slots, mask, level_key(k, top));
+  bool act = h >= 0 && __ldcg(cand_slot + h) > max_count;
+  for (int s = top - 1; s >= 0 && act; --s) {
+    h = level_find(slots, mask, level_key(k, s));
+    const int cnt = h >= 0 ? __ldcg(cand_slot + h) : 0;
+    const bool use = cnt >= min_count;
+    if (use) sel = s;
+    act = use && cnt > max_count;
+  }
+  return sel;
+}
+
+// Level selection of every point, then the query groups: a group is a
+// maximal run of sorted positions with the same selected level L and the
+// same level-L node; its start writes group_flag and the 27 runs (row p).
+// One warp per 32 positions; lane 0 recomputes its predecessor's level.
+__global__ void __launch_bounds__(256)
+    ka_select_all(LevelArgs a, const Slot* __restrict__ slots,
+                  const int32_t* __restrict__ cand_slot, int min_count, int max_count,
+                  uint8_t* __restrict__ sel_out, uint8_t* __restrict__ group_flag,
+                  int2* __restrict__ runs) {
+  const int top = top_level(a.meta);
+  const uint32_t mask = static_cast<uint32_t>(a.meta->reserved[2]);
+  const int bpa = a.meta->bpa;
+  const uint64_t* key = sorted_keys(a.sp, a.bits);
+  const int lane = threadIdx.x & 31;
+  const int64_t warps = (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5;
+  for (int64_t base = ((static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5) * 32;
        base < a.n; base += warps * 32) {
     const int64_t p = base + lane;
+    int L = -1;
+    if (p < a.n) {
+      L = select_level(key, p, top, slots, mask, cand_slot, min_count, max_count);
+      sel_out[p] = static_cast<uint8_t>(L);
+    }
+    int prev = __shfl_up_sync(kFull, L, 1);
+    if (lane == 0 && p > 0 && p < a.n)
+      prev = select_level(key, p - 1, top, slots, mask, cand_slot, min_count, max_count);
     bool start = false;
-    if (p < a.n && sel[p] == L) {
-      start = p == 0 || sel[p - 1] != L || node_head(key, p, 3 * L);
+    if (p < a.n) {
+      start = p == 0 || prev != L || node_head(key, p, 3 * L);
       group_flag[p] = start ? 1 : 0;
     }
     uint32_t starts = __ballot_sync(kFull, start);
@@ -633,8 +578,16 @@ __global__ void __launch_bounds__(256)
       const int src = __ffs(starts) - 1;
       starts &= starts - 1;
       const int64_t ps = base + src;
-      if (lane < kNeighbours)
-        runs[ps * kNeighbours + lane] = neighbour_run(t, key[ps] >> (3 * L), L, bpa, lane);
+      const int Ls = __shfl_sync(kFull, L, src);
+      if (lane < kNeighbours) {
+        const int h = level_neighbour_slot(slots, mask, key[ps] >> (3 * Ls), Ls, bpa, lane);
+        int2 run = make_int2(0, 0);
+        if (h >= 0) {
+          run.x = __ldcg(&slots[h].run.x);
+          run.y = __ldcg(&slots[h].run.y);
+        }
+        runs[ps * kNeighbours + lane] = run;
+      }
     }
   }
 }
@@ -703,16 +656,15 @@ struct ABufs {
   uint32_t* totals;
   uint32_t* tile_counts;
   float4* rec;
-  int32_t* node_of;
-  int32_t* node_start;
-  int32_t* cand;
-  int32_t* slot_of[2];
-  int* level_nodes;  // [kMaxLevel + 1]
-  uint8_t* sel[2];     // selection of the previous / current level (ping-pong by level parity)
-  uint8_t* active[2];
+  int* level_nodes;        // [kMaxLevel + 1]
+  int* level_base;         // [kMaxLevel + 2]
+  int32_t* node_start;     // nodes of every level, one sentinel per level
+  int32_t* slot_of_node;
+  Slot* slots;             // node table of every level
+  int32_t* cand_slot;      // 27-node count per slot
+  int64_t cap;             // table capacity for the largest possible node count
+  uint8_t* sel;
   uint8_t* group_flag;
-  Slot* tslots[2];
-  int64_t cap;
   int2* runs;
   int32_t* group_start;
   int32_t* group_row;
@@ -735,22 +687,18 @@ ABufs alayout(void* ws, int64_t n, size_t* bytes) {
   b.tile_counts = a.take<uint32_t>(static_cast<size_t>(kMaxLevel + 1) *
                                    static_cast<size_t>(ceil_div(n > 0 ? n : 1, kTile)));
   b.rec = a.take<float4>(n);
-  b.node_of = a.take<int32_t>(n);
-  b.node_start = a.take<int32_t>(n + 1);
-  b.cand = a.take<int32_t>(n);
-  b.slot_of[0] = a.take<int32_t>(n);
-  b.slot_of[1] = a.take<int32_t>(n);
   b.level_nodes = a.take<int>(kMaxLevel + 1);
-  for (int h = 0; h < 2; ++h) {
-    b.sel[h] = a.take<uint8_t>(n);
-    b.active[h] = a.take<uint8_t>(n);
-  }
-  b.group_flag = a.take<uint8_t>(n);
+  b.level_base = a.take<int>(kMaxLevel + 2);
+  // at most n nodes (+ a sentinel) on each of the kMaxLevel + 1 levels
+  const int64_t max_nodes = static_cast<int64_t>(kMaxLevel + 1) * (n + 1);
+  b.node_start = a.take<int32_t>(max_nodes);
+  b.slot_of_node = a.take<int32_t>(max_nodes);
   b.cap = 16;
-  while (b.cap < 2 * n) b.cap <<= 1;
-  for (int h = 0; h < 2; ++h) {
-    b.tslots[h] = a.take<Slot>(b.cap);
-  }
+  while (b.cap < 2 * max_nodes) b.cap <<= 1;
+  b.slots = a.take<Slot>(b.cap);
+  b.cand_slot = a.take<int32_t>(b.cap);
+  b.sel = a.take<uint8_t>(n);
+  b.group_flag = a.take<uint8_t>(n);
   b.runs = a.take<int2>(static_cast<size_t>(n) * kNeighbours);
   b.group_start = a.take<int32_t>(n + 1);
   b.group_row = a.take<int32_t>(n);
@@ -789,13 +737,7 @@ int run_adaptive(const AdaptiveArgs& f, void* ws, size_t ws_bytes, const QuerySh
     return FKNN_OK;
   }
   int nl = 0;
-  cudaError_t e = cudaMemsetAsync(b.tslots[0], 0xff, sizeof(Slot) * b.cap, s);
-  if (e == cudaSuccess) e = cudaMemsetAsync(b.tslots[1], 0xff, sizeof(Slot) * b.cap, s);
-  if (e == cudaSuccess) e = cudaMemsetAsync(b.group_flag, 0, static_cast<size_t>(n), s);
-  if (e != cudaSuccess) {
-    note_cuda_error(e);
-    return FKNN_ERR_CUDA;
-  }
+  cudaError_t e;
   ka_init<<<64, 256, 0, s>>>(b.meta, b.box, b.totals, kSortMaxPasses * 256);
   ka_box<<<blocks_for(n, kTile), 256, 0, s>>>(f.grid, f.batch, n, b.box, b.meta);
   ka_meta<<<1, 1024, 0, s>>>(b.box, f.max_shift, b.meta);
@@ -813,41 +755,28 @@ int run_adaptive(const AdaptiveArgs& f, void* ws, size_t ws_bytes, const QuerySh
   const int tiles = blocks_for(n, kTile);
   const int min_count = f.min_factor * f.k, max_count = f.max_factor * f.k;
   const int top_host = f.max_shift >= 0 ? f.max_shift : kMaxLevel;
-  const Table tab[2] = {{b.tslots[0], static_cast<uint32_t>(b.cap - 1)},
-                        {b.tslots[1], static_cast<uint32_t>(b.cap - 1)}};
-  {
-    const LevelArgs la{sp, key_bits, b.meta, n, 0};
-    ka_heads_all<<<tiles, 256, 0, s>>>(la, tiles, b.tile_counts);
-    ka_scan_all<<<kMaxLevel + 1, 1024, 0, s>>>(b.tile_counts, tiles, b.level_nodes);
-    nl += 2;
-  }
-  for (int lv = top_host; lv >= 0; --lv) {
-    const LevelArgs la{sp, key_bits, b.meta, n, lv};
-    int* nodes = b.level_nodes + lv;
-    const int* stale = b.level_nodes + (lv + 2 <= kMaxLevel ? lv + 2 : kMaxLevel);
-    const int h = lv & 1, up = (lv + 1) & 1;
-    ka_nodes<<<tiles, 256, 0, s>>>(la, b.tile_counts + static_cast<int64_t>(lv) * tiles, nodes,
-                                   b.node_of, b.node_start, stale, b.slot_of[h], b.tslots[h]);
-    ka_insert<<<capped_blocks(n), 256, 0, s>>>(la, nodes, b.node_start, tab[h], b.slot_of[h]);
-    ka_counts<<<capped_blocks(n * 32), 256, 0, s>>>(la, nodes, b.node_start, tab[h],
-                                                     b.active[up], b.cand);
-    const SelectArgs sa{b.node_of, b.cand, min_count, max_count, b.sel[up], b.active[up],
-                        b.sel[h], b.active[h], tab[up], b.group_flag, b.runs};
-    ka_select<<<capped_blocks(n), 256, 0, s>>>(la, sa);
-    nl += 4;
-  }
-  {
-    const LevelArgs la{sp, key_bits, b.meta, n, 0};
-    ka_finalize<<<capped_blocks(n), 256, 0, s>>>(la, 0, tab[0], b.sel[0], b.group_flag, b.runs);
-    ka_group_tiles<<<tiles, 256, 0, s>>>(n, b.group_flag, b.tile_counts);
-    k_scan_tiles<<<1, 1024, 0, s>>>(b.tile_counts, tiles, &b.meta->n_groups);
-    ka_groups<<<tiles, 256, 0, s>>>(n, b.group_flag, b.tile_counts, &b.meta->n_groups,
-                                    b.group_start, b.group_row);
-    nl += 4;
-    if (f.level_out) {
-      ka_levels_out<<<blocks_for(n, 256), 256, 0, s>>>(n, b.rec, b.sel[0], f.level_out);
-      ++nl;
-    }
+  const LevelArgs la{sp, key_bits, b.meta, n, 0};
+  const int64_t node_bound = static_cast<int64_t>(top_host + 1) * (n + 1);
+  ka_heads_all<<<tiles, 256, 0, s>>>(la, tiles, b.tile_counts);
+  ka_scan_all<<<kMaxLevel + 1, 1024, 0, s>>>(b.tile_counts, tiles, b.level_nodes);
+  ka_level_bases<<<1, 32, 0, s>>>(b.level_nodes, b.meta, b.level_base, b.cap);
+  ka_table_clear<<<capped_blocks(2 * node_bound), 256, 0, s>>>(b.slots, b.meta);
+  ka_nodes_all<<<tiles, 256, 0, s>>>(la, tiles, b.tile_counts, b.level_nodes, b.level_base,
+                                     b.node_start);
+  ka_insert_all<<<capped_blocks(node_bound), 256, 0, s>>>(la, b.level_base, b.node_start,
+                                                          b.slots, b.slot_of_node);
+  ka_counts_all<<<capped_blocks(node_bound * 32), 256, 0, s>>>(
+      la, b.level_base, b.node_start, b.slots, b.slot_of_node, b.cand_slot);
+  ka_select_all<<<capped_blocks(n), 256, 0, s>>>(la, b.slots, b.cand_slot, min_count, max_count,
+                                                 b.sel, b.group_flag, b.runs);
+  ka_group_tiles<<<tiles, 256, 0, s>>>(n, b.group_flag, b.tile_counts);
+  k_scan_tiles<<<1, 1024, 0, s>>>(b.tile_counts, tiles, &b.meta->n_groups);
+  ka_groups<<<tiles, 256, 0, s>>>(n, b.group_flag, b.tile_counts, &b.meta->n_groups,
+                                  b.group_start, b.group_row);
+  nl += 11;
+  if (f.level_out) {
+    ka_levels_out<<<blocks_for(n, 256), 256, 0, s>>>(n, b.rec, b.sel, f.level_out);
+    ++nl;
   }
   nl += launch_items(b.runs, b.group_start, b.group_row, &b.meta->n_groups, n, shape.tile_records,
                      b.cands, b.seg_counts, &b.meta->n_items, b.items, s, &b.meta->status, n,
