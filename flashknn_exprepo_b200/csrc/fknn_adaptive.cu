@@ -359,21 +359,25 @@ struct LTable {
   const int* mask_word;  // capacity - 1, set on the device
 };
 
-__device__ __forceinline__ int level_find(const Slot* slots, uint32_t mask, uint64_t v) {
+// Run of the node with level key v: one 16-byte load per probe; (0, 0)
+// when absent.
+__device__ __forceinline__ int2 level_find(const Slot* slots, uint32_t mask, uint64_t v) {
   uint32_t h = slot_of_key(v, mask);
   for (uint32_t probe = 0; probe <= mask; ++probe) {
-    const uint64_t k = __ldcg(&slots[h].key);
-    if (k == v) return static_cast<int>(h);
-    if (k == 0ull) break;
+    const ulonglong2 e = __ldcg(reinterpret_cast<const ulonglong2*>(slots + h));
+    if (e.x == v)
+      return make_int2(static_cast<int>(static_cast<uint32_t>(e.y)),
+                       static_cast<int>(static_cast<uint32_t>(e.y >> 32)));
+    if (e.x == 0ull) break;
     h = (h + 1) & mask;
   }
-  return -1;
+  return make_int2(0, 0);
 }
 
-// Run of neighbour j of the level-s node with node key nk (table slot), or
-// (0, 0) when the neighbour is outside the grid or empty.
-__device__ __forceinline__ int level_neighbour_slot(const Slot* slots, uint32_t mask, uint64_t nk,
-                                                   int s, int bpa, int j) {
+// Run of neighbour j of the level-s node with node key nk, or (0, 0) when
+// the neighbour is outside the grid or empty.
+__device__ __forceinline__ int2 level_neighbour_run(const Slot* slots, uint32_t mask, uint64_t nk,
+                                                    int s, int bpa, int j) {
   const int sb = 3 * (bpa - s);  // spatial bits of a level-s node key
   const uint64_t batch = nk >> sb;
   const uint64_t m = sb ? (nk & ((1ull << sb) - 1)) : 0ull;
@@ -382,7 +386,7 @@ __device__ __forceinline__ int level_neighbour_slot(const Slot* slots, uint32_t 
   const int jy = (j / 3) % 3, jz = j % 3;
   const int y = static_cast<int>(compact3(m >> 1)) + (jy == 0 ? 0 : (jy == 1 ? -1 : 1));
   const int z = static_cast<int>(compact3(m)) + (jz == 0 ? 0 : (jz == 1 ? -1 : 1));
-  if (x < 0 || y < 0 || z < 0 || x >= lim || y >= lim || z >= lim) return -1;
+  if (x < 0 || y < 0 || z < 0 || x >= lim || y >= lim || z >= lim) return make_int2(0, 0);
   const uint64_t key = (batch << sb) | morton3(static_cast<uint32_t>(x), static_cast<uint32_t>(y),
                                                static_cast<uint32_t>(z));
   return level_find(slots, mask, key | (1ull << (63 - 3 * s)));
@@ -399,7 +403,8 @@ __device__ __forceinline__ int level_of_node(const int* base, int top, int64_t g
 __device__ __forceinline__ int* level_mask_word(Meta* m) { return &m->reserved[2]; }
 
 // One warp: base[s] for s = 0..top+1 and the table mask (capacity = next
-// power of two >= 2 x all nodes).
+// power of two >= 4 x all nodes: most neighbour lookups miss, and misses end
+// at the first empty slot).
 __global__ void ka_level_bases(const int* __restrict__ level_nodes, Meta* meta,
                                int* __restrict__ base, int64_t max_cap) {
   if (threadIdx.x != 0) return;
@@ -411,7 +416,7 @@ __global__ void ka_level_bases(const int* __restrict__ level_nodes, Meta* meta,
   }
   base[top + 1] = b;
   int64_t cap = 16;
-  while (cap < 2 * static_cast<int64_t>(b)) cap <<= 1;
+  while (cap < 4 * static_cast<int64_t>(b)) cap <<= 1;
   if (cap > max_cap) {  // cannot happen: b <= (top + 1) * (n + 1)
     raise_status(&meta->status, kStatusTable);
     cap = max_cap;
@@ -436,12 +441,13 @@ __device__ __forceinline__ int head_level(const uint64_t* key, int64_t p) {
   return min((63 - __clzll(static_cast<long long>(x))) / 3, kMaxLevel);
 }
 
-// Node starts of every level: tile of 2048 positions, 8 per thread, one
+// Node starts of every level, and node_of[s * n + p] = the global node of
+// sorted position p at level s: tile of 2048 positions, 8 per thread, one
 // block scan per level over the precomputed per-level tile offsets.
 __global__ void __launch_bounds__(256)
     ka_nodes_all(LevelArgs a, int n_tiles, const uint32_t* __restrict__ tile_offsets,
                  const int* __restrict__ level_nodes, const int* __restrict__ base,
-                 int32_t* __restrict__ node_start) {
+                 int32_t* __restrict__ node_start, int32_t* __restrict__ node_of) {
   __shared__ uint32_t warp_sums[32];
   const int top = top_level(a.meta);
   const uint64_t* key = sorted_keys(a.sp, a.bits);
@@ -455,20 +461,24 @@ __global__ void __launch_bounds__(256)
     for (int r = 0; r < 8; ++r) heads += hl[r] >= s ? 1u : 0u;
     const uint32_t incl = block_inclusive_scan(heads, warp_sums, nullptr);
     int64_t g = base[s] + static_cast<int64_t>(tile_offsets[static_cast<int64_t>(s) * n_tiles +
-                                                            blockIdx.x]) + incl - heads;
+                                                            blockIdx.x]) + incl - heads - 1;
+    int32_t* nof = node_of + static_cast<int64_t>(s) * a.n;
 #pragma unroll
-    for (int r = 0; r < 8; ++r)
-      if (hl[r] >= s) node_start[g++] = static_cast<int32_t>(p0 + r);
+    for (int r = 0; r < 8; ++r) {
+      if (p0 + r >= a.n) break;
+      if (hl[r] >= s) node_start[++g] = static_cast<int32_t>(p0 + r);
+      nof[p0 + r] = static_cast<int32_t>(g);
+    }
     if (p0 <= a.n - 1 && a.n - 1 < p0 + 8)  // the sentinel after the level's last node
       node_start[base[s] + level_nodes[s]] = static_cast<int32_t>(a.n);
   }
 }
 
 // Every node of every level into the table: (start, count) under its level
-// key; slot_of_node[g] = its slot.  One thread per global node.
+// key.  One thread per global node.
 __global__ void __launch_bounds__(256)
     ka_insert_all(LevelArgs a, const int* __restrict__ base, const int32_t* __restrict__ node_start,
-                  Slot* __restrict__ slots, int32_t* __restrict__ slot_of_node) {
+                  Slot* __restrict__ slots) {
   const int top = top_level(a.meta);
   const uint32_t mask = static_cast<uint32_t>(a.meta->reserved[2]);
   const uint64_t* key = sorted_keys(a.sp, a.bits);
@@ -485,7 +495,6 @@ __global__ void __launch_bounds__(256)
           atomicCAS(reinterpret_cast<unsigned long long*>(&slots[h].key), 0ull, v);
       if (prev == 0ull) {
         slots[h].run = make_int2(st, node_start[g + 1] - st);
-        slot_of_node[g] = static_cast<int32_t>(h);
         break;
       }
       h = (h + 1) & mask;
@@ -493,12 +502,12 @@ __global__ void __launch_bounds__(256)
   }
 }
 
-// cand_slot[slot of node] = points in the 27 same-level nodes around it.
-// One warp per node, one lookup per lane.
+// cand[g] = points in the 27 same-level nodes around global node g.  One
+// warp per node, one lookup per lane.
 __global__ void __launch_bounds__(256)
     ka_counts_all(LevelArgs a, const int* __restrict__ base,
                   const int32_t* __restrict__ node_start, const Slot* __restrict__ slots,
-                  const int32_t* __restrict__ slot_of_node, int32_t* __restrict__ cand_slot) {
+                  int32_t* __restrict__ cand) {
   const int top = top_level(a.meta);
   const uint32_t mask = static_cast<uint32_t>(a.meta->reserved[2]);
   const int bpa = a.meta->bpa;
@@ -511,33 +520,36 @@ __global__ void __launch_bounds__(256)
     const int s = level_of_node(base, top, g);
     if (g == base[s + 1] - 1) continue;  // sentinel (warp-uniform)
     const uint64_t nk = key[node_start[g]] >> (3 * s);
-    int len = 0;
-    if (lane < kNeighbours) {
-      const int h = level_neighbour_slot(slots, mask, nk, s, bpa, lane);
-      if (h >= 0) len = __ldcg(&slots[h].run.y);
-    }
+    const int len = lane < kNeighbours ? level_neighbour_run(slots, mask, nk, s, bpa, lane).y : 0;
     const int t = __reduce_add_sync(kFull, len);
-    if (lane == 0) cand_slot[slot_of_node[g]] = t;
+    if (lane == 0) cand[g] = t;
   }
 }
 
 // Selected level of sorted position q: from the top level down, an active
 // point moves to level s when its level-s count is >= min_count and stays
-// active while it is > max_count (adaptive_octree.py:312-351).
-__device__ __forceinline__ int select_level(const uint64_t* key, int64_t q, int top,
-                                            const Slot* slots, uint32_t mask,
-                                            const int32_t* cand_slot, int min_count,
+// active while it is > max_count (adaptive_octree.py:312-351).  The counts
+// of all levels are loaded first (independent loads), then walked.
+__device__ __forceinline__ int select_level(int64_t q, int64_t n, int top,
+                                            const int32_t* __restrict__ node_of,
+                                            const int32_t* __restrict__ cand, int min_count,
                                             int max_count) {
-  const uint64_t k = key[q];
+  int cnt[kMaxLevel + 1];
+#pragma unroll
+  for (int s = 0; s <= kMaxLevel; ++s)
+    cnt[s] = s <= top ? __ldcg(cand + __ldcg(node_of + static_cast<int64_t>(s) * n + q)) : 0;
   int sel = top;
-  int h = level_find(slots, mask, level_key(k, top));
-  bool act = h >= 0 && __ldcg(cand_slot + h) > max_count;
-  for (int s = top - 1; s >= 0 && act; --s) {
-    h = level_find(slots, mask, level_key(k, s));
-    const int cnt = h >= 0 ? __ldcg(cand_slot + h) : 0;
-    const bool use = cnt >= min_count;
-    if (use) sel = s;
-    act = use && cnt > max_count;
+  bool act = false;
+#pragma unroll
+  for (int s = kMaxLevel; s >= 0; --s) {
+    if (s > top) continue;
+    if (s == top) {
+      act = cnt[s] > max_count;
+    } else if (act) {
+      const bool use = cnt[s] >= min_count;
+      if (use) sel = s;
+      act = use && cnt[s] > max_count;
+    }
   }
   return sel;
 }
@@ -547,8 +559,8 @@ __device__ __forceinline__ int select_level(const uint64_t* key, int64_t q, int 
 // same level-L node; its start writes group_flag and the 27 runs (row p).
 // One warp per 32 positions; lane 0 recomputes its predecessor's level.
 __global__ void __launch_bounds__(256)
-    ka_select_all(LevelArgs a, const Slot* __restrict__ slots,
-                  const int32_t* __restrict__ cand_slot, int min_count, int max_count,
+    ka_select_all(LevelArgs a, const Slot* __restrict__ slots, const int32_t* __restrict__ node_of,
+                  const int32_t* __restrict__ cand, int min_count, int max_count,
                   uint8_t* __restrict__ sel_out, uint8_t* __restrict__ group_flag,
                   int2* __restrict__ runs) {
   const int top = top_level(a.meta);
@@ -562,12 +574,12 @@ __global__ void __launch_bounds__(256)
     const int64_t p = base + lane;
     int L = -1;
     if (p < a.n) {
-      L = select_level(key, p, top, slots, mask, cand_slot, min_count, max_count);
+      L = select_level(p, a.n, top, node_of, cand, min_count, max_count);
       sel_out[p] = static_cast<uint8_t>(L);
     }
     int prev = __shfl_up_sync(kFull, L, 1);
     if (lane == 0 && p > 0 && p < a.n)
-      prev = select_level(key, p - 1, top, slots, mask, cand_slot, min_count, max_count);
+      prev = select_level(p - 1, a.n, top, node_of, cand, min_count, max_count);
     bool start = false;
     if (p < a.n) {
       start = p == 0 || prev != L || node_head(key, p, 3 * L);
@@ -579,15 +591,9 @@ __global__ void __launch_bounds__(256)
       starts &= starts - 1;
       const int64_t ps = base + src;
       const int Ls = __shfl_sync(kFull, L, src);
-      if (lane < kNeighbours) {
-        const int h = level_neighbour_slot(slots, mask, key[ps] >> (3 * Ls), Ls, bpa, lane);
-        int2 run = make_int2(0, 0);
-        if (h >= 0) {
-          run.x = __ldcg(&slots[h].run.x);
-          run.y = __ldcg(&slots[h].run.y);
-        }
-        runs[ps * kNeighbours + lane] = run;
-      }
+      if (lane < kNeighbours)
+        runs[ps * kNeighbours + lane] =
+            level_neighbour_run(slots, mask, key[ps] >> (3 * Ls), Ls, bpa, lane);
     }
   }
 }
@@ -659,9 +665,9 @@ struct ABufs {
   int* level_nodes;        // [kMaxLevel + 1]
   int* level_base;         // [kMaxLevel + 2]
   int32_t* node_start;     // nodes of every level, one sentinel per level
-  int32_t* slot_of_node;
+  int32_t* node_of;        // [kMaxLevel + 1][n] global node of each sorted position
   Slot* slots;             // node table of every level
-  int32_t* cand_slot;      // 27-node count per slot
+  int32_t* cand;           // 27-node count per global node
   int64_t cap;             // table capacity for the largest possible node count
   uint8_t* sel;
   uint8_t* group_flag;
@@ -692,11 +698,11 @@ ABufs alayout(void* ws, int64_t n, size_t* bytes) {
   // at most n nodes (+ a sentinel) on each of the kMaxLevel + 1 levels
   const int64_t max_nodes = static_cast<int64_t>(kMaxLevel + 1) * (n + 1);
   b.node_start = a.take<int32_t>(max_nodes);
-  b.slot_of_node = a.take<int32_t>(max_nodes);
+  b.node_of = a.take<int32_t>(static_cast<size_t>(kMaxLevel + 1) * static_cast<size_t>(n));
   b.cap = 16;
-  while (b.cap < 2 * max_nodes) b.cap <<= 1;
+  while (b.cap < 4 * max_nodes) b.cap <<= 1;
   b.slots = a.take<Slot>(b.cap);
-  b.cand_slot = a.take<int32_t>(b.cap);
+  b.cand = a.take<int32_t>(max_nodes);
   b.sel = a.take<uint8_t>(n);
   b.group_flag = a.take<uint8_t>(n);
   b.runs = a.take<int2>(static_cast<size_t>(n) * kNeighbours);
@@ -760,15 +766,15 @@ int run_adaptive(const AdaptiveArgs& f, void* ws, size_t ws_bytes, const QuerySh
   ka_heads_all<<<tiles, 256, 0, s>>>(la, tiles, b.tile_counts);
   ka_scan_all<<<kMaxLevel + 1, 1024, 0, s>>>(b.tile_counts, tiles, b.level_nodes);
   ka_level_bases<<<1, 32, 0, s>>>(b.level_nodes, b.meta, b.level_base, b.cap);
-  ka_table_clear<<<capped_blocks(2 * node_bound), 256, 0, s>>>(b.slots, b.meta);
+  ka_table_clear<<<capped_blocks(4 * node_bound), 256, 0, s>>>(b.slots, b.meta);
   ka_nodes_all<<<tiles, 256, 0, s>>>(la, tiles, b.tile_counts, b.level_nodes, b.level_base,
-                                     b.node_start);
+                                     b.node_start, b.node_of);
   ka_insert_all<<<capped_blocks(node_bound), 256, 0, s>>>(la, b.level_base, b.node_start,
-                                                          b.slots, b.slot_of_node);
-  ka_counts_all<<<capped_blocks(node_bound * 32), 256, 0, s>>>(
-      la, b.level_base, b.node_start, b.slots, b.slot_of_node, b.cand_slot);
-  ka_select_all<<<capped_blocks(n), 256, 0, s>>>(la, b.slots, b.cand_slot, min_count, max_count,
-                                                 b.sel, b.group_flag, b.runs);
+                                                          b.slots);
+  ka_counts_all<<<capped_blocks(node_bound * 32), 256, 0, s>>>(la, b.level_base, b.node_start,
+                                                               b.slots, b.cand);
+  ka_select_all<<<capped_blocks(n), 256, 0, s>>>(la, b.slots, b.node_of, b.cand, min_count,
+                                                 max_count, b.sel, b.group_flag, b.runs);
   ka_group_tiles<<<tiles, 256, 0, s>>>(n, b.group_flag, b.tile_counts);
   k_scan_tiles<<<1, 1024, 0, s>>>(b.tile_counts, tiles, &b.meta->n_groups);
   ka_groups<<<tiles, 256, 0, s>>>(n, b.group_flag, b.tile_counts, &b.meta->n_groups,
