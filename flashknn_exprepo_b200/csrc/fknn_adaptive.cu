@@ -402,9 +402,10 @@ __device__ __forceinline__ int level_of_node(const int* base, int top, int64_t g
 // Meta words of the all-levels pipeline.
 __device__ __forceinline__ int* level_mask_word(Meta* m) { return &m->reserved[2]; }
 
-// One warp: base[s] for s = 0..top+1 and the table mask (capacity = next
-// power of two >= 4 x all nodes: most neighbour lookups miss, and misses end
-// at the first empty slot).
+// One warp: base[s] for s = 0..top+1 and the table mask: capacity = next
+// power of two >= 4 x all nodes (most neighbour lookups miss, and misses end
+// at the first empty slot), at most the allocated capacity, which holds
+// twice the largest possible node count.
 __global__ void ka_level_bases(const int* __restrict__ level_nodes, Meta* meta,
                                int* __restrict__ base, int64_t max_cap) {
   if (threadIdx.x != 0) return;
@@ -417,10 +418,7 @@ __global__ void ka_level_bases(const int* __restrict__ level_nodes, Meta* meta,
   base[top + 1] = b;
   int64_t cap = 16;
   while (cap < 4 * static_cast<int64_t>(b)) cap <<= 1;
-  if (cap > max_cap) {  // cannot happen: b <= (top + 1) * (n + 1)
-    raise_status(&meta->status, kStatusTable);
-    cap = max_cap;
-  }
+  if (cap > max_cap) cap = max_cap;
   *level_mask_word(meta) = static_cast<int>(cap - 1);
 }
 
@@ -668,7 +666,7 @@ struct ABufs {
   int32_t* node_of;        // [kMaxLevel + 1][n] global node of each sorted position
   Slot* slots;             // node table of every level
   int32_t* cand;           // 27-node count per global node
-  int64_t cap;             // table capacity for the largest possible node count
+  int64_t cap;             // table allocation: twice the largest possible node count
   uint8_t* sel;
   uint8_t* group_flag;
   int2* runs;
@@ -700,7 +698,7 @@ ABufs alayout(void* ws, int64_t n, size_t* bytes) {
   b.node_start = a.take<int32_t>(max_nodes);
   b.node_of = a.take<int32_t>(static_cast<size_t>(kMaxLevel + 1) * static_cast<size_t>(n));
   b.cap = 16;
-  while (b.cap < 4 * max_nodes) b.cap <<= 1;
+  while (b.cap < 2 * max_nodes) b.cap <<= 1;
   b.slots = a.take<Slot>(b.cap);
   b.cand = a.take<int32_t>(max_nodes);
   b.sel = a.take<uint8_t>(n);
@@ -766,7 +764,7 @@ int run_adaptive(const AdaptiveArgs& f, void* ws, size_t ws_bytes, const QuerySh
   ka_heads_all<<<tiles, 256, 0, s>>>(la, tiles, b.tile_counts);
   ka_scan_all<<<kMaxLevel + 1, 1024, 0, s>>>(b.tile_counts, tiles, b.level_nodes);
   ka_level_bases<<<1, 32, 0, s>>>(b.level_nodes, b.meta, b.level_base, b.cap);
-  ka_table_clear<<<capped_blocks(4 * node_bound), 256, 0, s>>>(b.slots, b.meta);
+  ka_table_clear<<<capped_blocks(b.cap), 256, 0, s>>>(b.slots, b.meta);
   ka_nodes_all<<<tiles, 256, 0, s>>>(la, tiles, b.tile_counts, b.level_nodes, b.level_base,
                                      b.node_start, b.node_of);
   ka_insert_all<<<capped_blocks(node_bound), 256, 0, s>>>(la, b.level_base, b.node_start,
