@@ -126,3 +126,16 @@ def test_adaptive_errors(fk):
     idx = knn.query(g, b)                            # one voxel: everything ties at 0
     assert idx.shape == (10, 4)
 
+
+
+def test_sparse_points_distinct_at_most_levels(fk):
+    """Points spread over almost the whole coordinate range: nearly every
+    point is a node of its own up to high octree levels, so the node count
+    of all levels approaches its bound (n per level) and the node table runs
+    at its highest load."""
+    rng = np.random.default_rng(31)
+    grid = rng.integers(0, 60000, (3000, 3)).astype(np.int64)
+    xyz = grid.astype(np.float32) * np.float32(0.01)
+    check_vs_oracle(fk, grid, None, 8, xyz)
+    batch = rng.integers(0, 3, len(grid)).astype(np.int64)
+    check_vs_oracle(fk, grid, batch, 4, xyz, min_factor=1, max_factor=2)
