@@ -316,6 +316,15 @@ __global__ void __maxnreg__(query_max_regs<KCAP>())
 
     if (chunked) {
       // ------------------------------------------------ chunked item
+      // One group with more candidates than a tile, up to 32 of its queries,
+      // G lanes per query.  Phase A scans the first runs (the group's own
+      // cell first) until they hold 2K candidates; the G partial lists of a
+      // query are then merged, so every query knows its K-th distance over
+      // those candidates, an upper bound of its final K-th.  A later
+      // candidate can only enter the top-K of some query q if its distance to
+      // the queries' centroid c is at most |q - c| + K-th(q) <= R + D (R, D:
+      // the item's largest), so phase B scans, tile by tile, only the
+      // candidates inside that sphere (with a margin for FP32 rounding).
       const int row = a.group_row ? a.group_row[g0] : g0;
       const int2 run = load_run(a, row, lane);
       const int incl = warp_inclusive_scan(run.y);
@@ -329,40 +338,88 @@ __global__ void __maxnreg__(query_max_regs<KCAP>())
       const bool takes = active && cut_accepts_any(a.cut_r2);
       float4 q = make_float4(0.f, 0.f, 0.f, 0.f);
       if (active) q = a.qrec[q0 + qi];
+      // phase A: whole runs until 2K candidates (all of them when fewer)
+      const uint32_t long_enough = __ballot_sync(kFull, lane < kNeighbours && incl >= 2 * KCAP);
+      const int a_end = long_enough ? __shfl_sync(kFull, incl, __ffs(long_enough) - 1) : total;
+      // centroid of the item's queries and their largest distance to it
+      const bool head = active && sub == 0;
+      const float inv_qn = 1.f / static_cast<float>(qn);
+      const float cx = warp_sum(head ? q.x : 0.f) * inv_qn;
+      const float cy = warp_sum(head ? q.y : 0.f) * inv_qn;
+      const float cz = warp_sum(head ? q.z : 0.f) * inv_qn;
+      const float qx = q.x - cx, qy = q.y - cy, qz = q.z - cz;
+      const float rq = sqrtf(warp_max(head ? qx * qx + qy * qy + qz * qz : 0.f));
       uint64_t L[KCAP];
 #pragma unroll
       for (int j = 0; j < KCAP; ++j) L[j] = kEmpty;
       const uint32_t cut_lim = cut_limit(a.cut_r2);
-      uint32_t thr = cut_lim;
+      uint32_t thr = cut_lim, qthr = cut_lim;
       bool timed_out = false;
-      for (int c0 = 0; c0 < total; c0 += T) {
-        const int c1 = min(total, c0 + T);
-        __syncwarp();
-        fence_proxy_async_smem();  // earlier generic reads of the tile precede the copies
-        if (lane == 0) mbar_arrive_expect_tx(bar, static_cast<uint32_t>(c1 - c0) * 16u);
-        __syncwarp();
-        const int lo = max(run_off, c0), hi = min(run_off + run.y, c1);
-        if (hi > lo)
-          bulk_copy_g2s(tile + (lo - c0), a.srec + run.x + (lo - run_off),
-                        static_cast<uint32_t>(hi - lo) * 16u, bar);
-        if (!mbar_wait_bounded(bar, phase, kWaitLimit)) {
-          timed_out = true;
-          break;
-        }
-        phase ^= 1u;
-        const int cnt = c1 - c0;
-        for (int i0 = 0; i0 < cnt; i0 += G) {
-          const int i = i0 + sub;
-          const bool ok = takes && i < cnt;
-          const float4 c = ok ? tile[i] : q;
-          const float d = sq_dist(c.x, c.y, c.z, q.x, q.y, q.z);
-          const uint32_t db = __float_as_uint(d);
-          const bool acc = ok && db <= thr;
-          if (__any_sync(kFull, acc)) {
-            list_insert<KCAP>(L, acc ? make_key(d, c.w) : kEmpty);
-            thr = kth_limit(L[KCAP - 1], cut_lim);
+      float rad2 = 0.f;
+      // Stage the candidates [lo, hi) of the concatenated runs tile by tile;
+      // with `filter`, keep those within sqrt(rad2) of the centroid.
+      auto scan_range = [&](int lo_c, int hi_c, bool filter) {
+        for (int c0 = lo_c; c0 < hi_c && !timed_out; c0 += T) {
+          const int c1 = min(hi_c, c0 + T);
+          __syncwarp();
+          fence_proxy_async_smem();  // earlier generic reads of the tile precede the copies
+          if (lane == 0) mbar_arrive_expect_tx(bar, static_cast<uint32_t>(c1 - c0) * 16u);
+          __syncwarp();
+          const int lo = max(run_off, c0), hi = min(run_off + run.y, c1);
+          if (hi > lo)
+            bulk_copy_g2s(tile + (lo - c0), a.srec + run.x + (lo - run_off),
+                          static_cast<uint32_t>(hi - lo) * 16u, bar);
+          if (!mbar_wait_bounded(bar, phase, kWaitLimit)) {
+            timed_out = true;
+            break;
+          }
+          phase ^= 1u;
+          int cnt = c1 - c0;
+          if (filter) {  // compact the tile to the candidates inside the sphere
+            int m = 0;
+            for (int t0 = 0; t0 < cnt; t0 += 32) {
+              const int t = t0 + lane;
+              bool keep = false;
+              if (t < cnt) {
+                const float4 c = tile[t];
+                const float dx = c.x - cx, dy = c.y - cy, dz = c.z - cz;
+                keep = dx * dx + dy * dy + dz * dz <= rad2;
+              }
+              const uint32_t b = __ballot_sync(kFull, keep);
+              if (keep) srt16[m + __popc(b & lanemask_lt())] = static_cast<uint16_t>(t);
+              m += __popc(b);
+            }
+            __syncwarp();
+            cnt = m;
+          }
+          for (int i0 = 0; i0 < cnt; i0 += G) {
+            const int i = i0 + sub;
+            const bool ok = takes && i < cnt;
+            const float4 c = ok ? tile[filter ? srt16[i] : i] : q;
+            const float d = sq_dist(c.x, c.y, c.z, q.x, q.y, q.z);
+            const uint32_t db = __float_as_uint(d);
+            const bool acc = ok && db <= thr;
+            if (__any_sync(kFull, acc)) {
+              list_insert<KCAP>(L, acc ? make_key(d, c.w) : kEmpty);
+              thr = min(kth_limit(L[KCAP - 1], cut_lim), qthr);
+            }
           }
         }
+      };
+      scan_range(0, a_end, false);
+      if (!timed_out && a_end < total) {
+        for (int m = 1; m < G; m <<= 1) merge_with_lane<KCAP>(L, m);
+        qthr = kth_limit(L[KCAP - 1], cut_lim);  // the query's bound (same in its G lanes)
+        thr = qthr;
+        if (sub != 0) {  // its candidates now live in lane sub == 0 only
+#pragma unroll
+          for (int j = 0; j < KCAP; ++j) L[j] = kEmpty;
+        }
+        const float d2 = warp_max(active ? __uint_as_float(qthr) : 0.f);
+        const float mag = fmaxf(fabsf(cx), fmaxf(fabsf(cy), fabsf(cz))) + rq;
+        const float rad = (rq + sqrtf(d2)) * 1.00001f + mag * 4e-6f + 1e-30f;
+        rad2 = rad * rad * 1.00001f;
+        scan_range(a_end, total, rad2 <= 3.0e38f);
       }
       if (timed_out) {
         if (lane == 0) raise_status(&meta->status, kStatusTimeout);
