@@ -36,6 +36,7 @@ namespace fknn {
 constexpr uint64_t kEmpty = ~0ull;
 constexpr uint32_t kWaitLimit = 1u << 22;
 constexpr int kBuckets = 32;
+constexpr int kMaxOrderedGroup = 4096;  // queries: larger chunked groups keep record order
 
 // Per-group scratch of the current packed item (shared memory, per warp).
 struct GroupSlot {
@@ -269,14 +270,204 @@ __device__ __forceinline__ int2 load_run(const QueryLaunch& a, int row, int lane
 // one, ptxas holds the 16-entry kernels to 64 registers and spills; 96 still
 // fits the 20 resident warps per SM that the default tile's shared memory
 // allows.  Lists of up to 8 entries fit in 72 without spilling.
+// Record of query qi of a chunked item (queries q0 .. q0+qn-1 of group g0):
+// the group's queries taken in octant-major order around their centroid
+// (item j of the group = positions 32j .. 32j+31 of that order), so every
+// query belongs to exactly one item and an item's queries are close
+// together.  Groups of at most 32 or more than kMaxOrderedGroup queries, and
+// items not cut at multiples of 32, keep record order.  qlist: 32 ints of
+// scratch; hist: 8 counters.  Kept out of line so its registers do not add
+// to the packed path's.
+__device__ __noinline__ int ordered_query_row(const float4* __restrict__ qrec,
+                                              const int32_t* __restrict__ group_start, int g0,
+                                              int q0, int qn, int qi, bool active, int* qlist,
+                                              uint32_t* hist) {
+  const int lane = threadIdx.x & 31;
+  const int gq0 = group_start[g0], gq1 = group_start[g0 + 1];
+  const int nqg = gq1 - gq0;
+  if (!(nqg > 32 && nqg <= kMaxOrderedGroup && q0 >= gq0 && q0 + qn <= gq1 &&
+        (q0 - gq0) % 32 == 0))
+    return q0 + qi;
+  float gx = 0.f, gy = 0.f, gz = 0.f;
+  for (int t = lane; t < nqg; t += 32) {
+    const float4 v = qrec[gq0 + t];
+    gx += v.x;
+    gy += v.y;
+    gz += v.z;
+  }
+  const float inv = 1.f / static_cast<float>(nqg);
+  gx = warp_sum(gx) * inv;
+  gy = warp_sum(gy) * inv;
+  gz = warp_sum(gz) * inv;
+  auto octant = [&](int t) {
+    const float4 v = qrec[gq0 + t];
+    return (v.x > gx ? 1 : 0) | (v.y > gy ? 2 : 0) | (v.z > gz ? 4 : 0);
+  };
+  if (lane < 8) hist[lane] = 0u;
+  __syncwarp();
+  for (int t = lane; t < nqg; t += 32) atomicAdd(&hist[octant(t)], 1u);
+  __syncwarp();
+  const uint32_t h = lane < 8 ? hist[lane] : 0u;
+  const uint32_t off = static_cast<uint32_t>(warp_inclusive_scan(static_cast<int>(h))) - h;
+  __syncwarp();
+  if (lane < 8) hist[lane] = off;  // running position of each octant
+  __syncwarp();
+  const int first = q0 - gq0;
+  for (int t0 = 0; t0 < nqg; t0 += 32) {
+    const int t = t0 + lane;
+    const int o = t < nqg ? octant(t) : 8;
+    const uint32_t peers = __match_any_sync(kFull, o);
+    int pos = -1;
+    if (o < 8) pos = static_cast<int>(hist[o]) + __popc(peers & lanemask_lt());
+    __syncwarp();
+    if (o < 8 && lane == __ffs(peers) - 1) hist[o] += __popc(peers);
+    if (pos >= first && pos < first + qn) qlist[pos - first] = gq0 + t;
+    __syncwarp();
+  }
+  const int row = active ? qlist[qi] : q0 + qi;
+  __syncwarp();
+  return row;
+}
+
 template <int KCAP>
 constexpr int query_max_regs() {
   return KCAP <= 8 ? 72 : (KCAP <= 16 ? 96 : (KCAP <= 32 ? 128 : 224));
 }
 
+// A chunked item: one group with more candidates than a tile.  Out of line,
+// so its registers do not add to the packed path's.  Returns the mbarrier's
+// next phase, or -1 after a bounded wait gave up (status raised, the warp's
+// copies waited for).
+template <int KCAP, bool EXACT, typename IdxT>
+__device__ __noinline__ int chunked_item(const QueryLaunch& a, int T, int min_cands_per_lane,
+                                         int q0, int qn, int g0, int k, float4* tile,
+                                         uint16_t* srt16, uint32_t* hist, uint64_t* bar,
+                                         uint32_t phase) {
+  const int lane = threadIdx.x & 31;
+  // One group with more candidates than a tile, up to 32 of its queries,
+  // G lanes per query.  Phase A scans the first runs (the group's own
+  // cell first) until they hold 2K candidates; the G partial lists of a
+  // query are then merged, so every query knows its K-th distance over
+  // those candidates, an upper bound of its final K-th.  A later
+  // candidate can only enter the top-K of some query q if its distance to
+  // the queries' centroid c is at most |q - c| + K-th(q) <= R + D (R, D:
+  // the item's largest), so phase B scans, tile by tile, only the
+  // candidates inside that sphere (with a margin for FP32 rounding).
+  const int row = a.group_row ? a.group_row[g0] : g0;
+  const int2 run = load_run(a, row, lane);
+  const int incl = warp_inclusive_scan(run.y);
+  const int total = __shfl_sync(kFull, incl, 31);
+  const int run_off = incl - run.y;
+  int lg = 5 - ceil_log2(qn);
+  while (lg > 0 && (total >> lg) < min_cands_per_lane) --lg;
+  const int G = 1 << lg;
+  const int qi = lane >> lg, sub = lane & (G - 1);
+  const bool active = qi < qn;
+  const bool takes = active && cut_accepts_any(a.cut_r2);
+  // The packer cuts the group's queries into items of 32 in record order
+  // (item j = positions 32j..): take them instead in octant-major order
+  // (ordered_query_row), so an item's queries are close together and the
+  // phase-B sphere below stays small.
+  const int qrow = ordered_query_row(a.qrec, a.group_start, g0, q0, qn, qi, active,
+                                     reinterpret_cast<int*>(tile), hist);
+  float4 q = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (active) q = a.qrec[qrow];
+  // phase A: whole runs until 2K candidates (all of them when fewer)
+  const uint32_t long_enough = __ballot_sync(kFull, lane < kNeighbours && incl >= 2 * KCAP);
+  const int a_end = long_enough ? __shfl_sync(kFull, incl, __ffs(long_enough) - 1) : total;
+  // centroid of the item's queries and their largest distance to it
+  const bool head = active && sub == 0;
+  const float inv_qn = 1.f / static_cast<float>(qn);
+  const float cx = warp_sum(head ? q.x : 0.f) * inv_qn;
+  const float cy = warp_sum(head ? q.y : 0.f) * inv_qn;
+  const float cz = warp_sum(head ? q.z : 0.f) * inv_qn;
+  const float qx = q.x - cx, qy = q.y - cy, qz = q.z - cz;
+  const float rq = sqrtf(warp_max(head ? qx * qx + qy * qy + qz * qz : 0.f));
+  uint64_t L[KCAP];
+#pragma unroll
+  for (int j = 0; j < KCAP; ++j) L[j] = kEmpty;
+  const uint32_t cut_lim = cut_limit(a.cut_r2);
+  uint32_t thr = cut_lim, qthr = cut_lim;
+  bool timed_out = false;
+  float rad2 = 0.f;
+  // Stage the candidates [lo, hi) of the concatenated runs tile by tile;
+  // with `filter`, keep those within sqrt(rad2) of the centroid.
+  auto scan_range = [&](int lo_c, int hi_c, bool filter) {
+    for (int c0 = lo_c; c0 < hi_c && !timed_out; c0 += T) {
+      const int c1 = min(hi_c, c0 + T);
+      __syncwarp();
+      fence_proxy_async_smem();  // earlier generic reads of the tile precede the copies
+      if (lane == 0) mbar_arrive_expect_tx(bar, static_cast<uint32_t>(c1 - c0) * 16u);
+      __syncwarp();
+      const int lo = max(run_off, c0), hi = min(run_off + run.y, c1);
+      if (hi > lo)
+        bulk_copy_g2s(tile + (lo - c0), a.srec + run.x + (lo - run_off),
+                      static_cast<uint32_t>(hi - lo) * 16u, bar);
+      if (!mbar_wait_bounded(bar, phase, kWaitLimit)) {
+        timed_out = true;
+        break;
+      }
+      phase ^= 1u;
+      int cnt = c1 - c0;
+      if (filter) {  // compact the tile to the candidates inside the sphere
+        int m = 0;
+        for (int t0 = 0; t0 < cnt; t0 += 32) {
+          const int t = t0 + lane;
+          bool keep = false;
+          if (t < cnt) {
+            const float4 c = tile[t];
+            const float dx = c.x - cx, dy = c.y - cy, dz = c.z - cz;
+            keep = dx * dx + dy * dy + dz * dz <= rad2;
+          }
+          const uint32_t b = __ballot_sync(kFull, keep);
+          if (keep) srt16[m + __popc(b & lanemask_lt())] = static_cast<uint16_t>(t);
+          m += __popc(b);
+        }
+        __syncwarp();
+        cnt = m;
+      }
+      for (int i0 = 0; i0 < cnt; i0 += G) {
+        const int i = i0 + sub;
+        const bool ok = takes && i < cnt;
+        const float4 c = ok ? tile[filter ? srt16[i] : i] : q;
+        const float d = sq_dist(c.x, c.y, c.z, q.x, q.y, q.z);
+        const uint32_t db = __float_as_uint(d);
+        const bool acc = ok && db <= thr;
+        if (__any_sync(kFull, acc)) {
+          list_insert<KCAP>(L, acc ? make_key(d, c.w) : kEmpty);
+          thr = min(kth_limit(L[KCAP - 1], cut_lim), qthr);
+        }
+      }
+    }
+  };
+  scan_range(0, a_end, false);
+  if (!timed_out && a_end < total) {
+    for (int m = 1; m < G; m <<= 1) merge_with_lane<KCAP>(L, m);
+    qthr = kth_limit(L[KCAP - 1], cut_lim);  // the query's bound (same in its G lanes)
+    thr = qthr;
+    if (sub != 0) {  // its candidates now live in lane sub == 0 only
+#pragma unroll
+      for (int j = 0; j < KCAP; ++j) L[j] = kEmpty;
+    }
+    const float d2 = warp_max(active ? __uint_as_float(qthr) : 0.f);
+    const float mag = fmaxf(fabsf(cx), fmaxf(fabsf(cy), fabsf(cz))) + rq;
+    const float rad = (rq + sqrtf(d2)) * 1.00001f + mag * 4e-6f + 1e-30f;
+    rad2 = rad * rad * 1.00001f;
+    scan_range(a_end, total, rad2 <= 3.0e38f);
+  }
+  if (timed_out) {
+    if (lane == 0) raise_status(&a.meta->status, kStatusTimeout);
+    mbar_wait_bounded(bar, phase, kWaitLimit);  // let this warp's copies land
+    return -1;
+  }
+  for (int m = 1; m < G; m <<= 1) merge_with_lane<KCAP>(L, m);
+  if (active && sub == 0) write_row<IdxT, KCAP, EXACT>(a, L, __float_as_int(q.w), k);
+  return static_cast<int>(phase);
+}
+
 template <int KCAP, bool EXACT, typename IdxT>
 __global__ void __maxnreg__(query_max_regs<KCAP>())
-    k_query(QueryLaunch a, int T, int min_cands_per_lane) {
+    k_query(const __grid_constant__ QueryLaunch a, int T, int min_cands_per_lane) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw) + warp;
@@ -315,119 +506,10 @@ __global__ void __maxnreg__(query_max_regs<KCAP>())
     }
 
     if (chunked) {
-      // ------------------------------------------------ chunked item
-      // One group with more candidates than a tile, up to 32 of its queries,
-      // G lanes per query.  Phase A scans the first runs (the group's own
-      // cell first) until they hold 2K candidates; the G partial lists of a
-      // query are then merged, so every query knows its K-th distance over
-      // those candidates, an upper bound of its final K-th.  A later
-      // candidate can only enter the top-K of some query q if its distance to
-      // the queries' centroid c is at most |q - c| + K-th(q) <= R + D (R, D:
-      // the item's largest), so phase B scans, tile by tile, only the
-      // candidates inside that sphere (with a margin for FP32 rounding).
-      const int row = a.group_row ? a.group_row[g0] : g0;
-      const int2 run = load_run(a, row, lane);
-      const int incl = warp_inclusive_scan(run.y);
-      const int total = __shfl_sync(kFull, incl, 31);
-      const int run_off = incl - run.y;
-      int lg = 5 - ceil_log2(qn);
-      while (lg > 0 && (total >> lg) < min_cands_per_lane) --lg;
-      const int G = 1 << lg;
-      const int qi = lane >> lg, sub = lane & (G - 1);
-      const bool active = qi < qn;
-      const bool takes = active && cut_accepts_any(a.cut_r2);
-      float4 q = make_float4(0.f, 0.f, 0.f, 0.f);
-      if (active) q = a.qrec[q0 + qi];
-      // phase A: whole runs until 2K candidates (all of them when fewer)
-      const uint32_t long_enough = __ballot_sync(kFull, lane < kNeighbours && incl >= 2 * KCAP);
-      const int a_end = long_enough ? __shfl_sync(kFull, incl, __ffs(long_enough) - 1) : total;
-      // centroid of the item's queries and their largest distance to it
-      const bool head = active && sub == 0;
-      const float inv_qn = 1.f / static_cast<float>(qn);
-      const float cx = warp_sum(head ? q.x : 0.f) * inv_qn;
-      const float cy = warp_sum(head ? q.y : 0.f) * inv_qn;
-      const float cz = warp_sum(head ? q.z : 0.f) * inv_qn;
-      const float qx = q.x - cx, qy = q.y - cy, qz = q.z - cz;
-      const float rq = sqrtf(warp_max(head ? qx * qx + qy * qy + qz * qz : 0.f));
-      uint64_t L[KCAP];
-#pragma unroll
-      for (int j = 0; j < KCAP; ++j) L[j] = kEmpty;
-      const uint32_t cut_lim = cut_limit(a.cut_r2);
-      uint32_t thr = cut_lim, qthr = cut_lim;
-      bool timed_out = false;
-      float rad2 = 0.f;
-      // Stage the candidates [lo, hi) of the concatenated runs tile by tile;
-      // with `filter`, keep those within sqrt(rad2) of the centroid.
-      auto scan_range = [&](int lo_c, int hi_c, bool filter) {
-        for (int c0 = lo_c; c0 < hi_c && !timed_out; c0 += T) {
-          const int c1 = min(hi_c, c0 + T);
-          __syncwarp();
-          fence_proxy_async_smem();  // earlier generic reads of the tile precede the copies
-          if (lane == 0) mbar_arrive_expect_tx(bar, static_cast<uint32_t>(c1 - c0) * 16u);
-          __syncwarp();
-          const int lo = max(run_off, c0), hi = min(run_off + run.y, c1);
-          if (hi > lo)
-            bulk_copy_g2s(tile + (lo - c0), a.srec + run.x + (lo - run_off),
-                          static_cast<uint32_t>(hi - lo) * 16u, bar);
-          if (!mbar_wait_bounded(bar, phase, kWaitLimit)) {
-            timed_out = true;
-            break;
-          }
-          phase ^= 1u;
-          int cnt = c1 - c0;
-          if (filter) {  // compact the tile to the candidates inside the sphere
-            int m = 0;
-            for (int t0 = 0; t0 < cnt; t0 += 32) {
-              const int t = t0 + lane;
-              bool keep = false;
-              if (t < cnt) {
-                const float4 c = tile[t];
-                const float dx = c.x - cx, dy = c.y - cy, dz = c.z - cz;
-                keep = dx * dx + dy * dy + dz * dz <= rad2;
-              }
-              const uint32_t b = __ballot_sync(kFull, keep);
-              if (keep) srt16[m + __popc(b & lanemask_lt())] = static_cast<uint16_t>(t);
-              m += __popc(b);
-            }
-            __syncwarp();
-            cnt = m;
-          }
-          for (int i0 = 0; i0 < cnt; i0 += G) {
-            const int i = i0 + sub;
-            const bool ok = takes && i < cnt;
-            const float4 c = ok ? tile[filter ? srt16[i] : i] : q;
-            const float d = sq_dist(c.x, c.y, c.z, q.x, q.y, q.z);
-            const uint32_t db = __float_as_uint(d);
-            const bool acc = ok && db <= thr;
-            if (__any_sync(kFull, acc)) {
-              list_insert<KCAP>(L, acc ? make_key(d, c.w) : kEmpty);
-              thr = min(kth_limit(L[KCAP - 1], cut_lim), qthr);
-            }
-          }
-        }
-      };
-      scan_range(0, a_end, false);
-      if (!timed_out && a_end < total) {
-        for (int m = 1; m < G; m <<= 1) merge_with_lane<KCAP>(L, m);
-        qthr = kth_limit(L[KCAP - 1], cut_lim);  // the query's bound (same in its G lanes)
-        thr = qthr;
-        if (sub != 0) {  // its candidates now live in lane sub == 0 only
-#pragma unroll
-          for (int j = 0; j < KCAP; ++j) L[j] = kEmpty;
-        }
-        const float d2 = warp_max(active ? __uint_as_float(qthr) : 0.f);
-        const float mag = fmaxf(fabsf(cx), fmaxf(fabsf(cy), fabsf(cz))) + rq;
-        const float rad = (rq + sqrtf(d2)) * 1.00001f + mag * 4e-6f + 1e-30f;
-        rad2 = rad * rad * 1.00001f;
-        scan_range(a_end, total, rad2 <= 3.0e38f);
-      }
-      if (timed_out) {
-        if (lane == 0) raise_status(&meta->status, kStatusTimeout);
-        mbar_wait_bounded(bar, phase, kWaitLimit);  // let this warp's copies land
-        return;
-      }
-      for (int m = 1; m < G; m <<= 1) merge_with_lane<KCAP>(L, m);
-      if (active && sub == 0) write_row<IdxT, KCAP, EXACT>(a, L, __float_as_int(q.w), k);
+      const int next = chunked_item<KCAP, EXACT, IdxT>(a, T, min_cands_per_lane, q0, qn, g0, k,
+                                                       tile, srt16, hist, bar, phase);
+      if (next < 0) return;
+      phase = static_cast<uint32_t>(next);
       continue;
     }
 
