@@ -266,10 +266,6 @@ __device__ __forceinline__ int2 load_run(const QueryLaunch& a, int row, int lane
   return run;
 }
 
-// Register budget per list length (CTAs have at most 256 threads).  Without
-// one, ptxas holds the 16-entry kernels to 64 registers and spills; 96 still
-// fits the 20 resident warps per SM that the default tile's shared memory
-// allows.  Lists of up to 8 entries fit in 72 without spilling.
 // Record of query qi of a chunked item (queries q0 .. q0+qn-1 of group g0):
 // the group's queries taken in octant-major order around their centroid
 // (item j of the group = positions 32j .. 32j+31 of that order), so every
@@ -329,9 +325,13 @@ __device__ __noinline__ int ordered_query_row(const float4* __restrict__ qrec,
   return row;
 }
 
+// Register budget per list length (CTAs have at most 256 threads).  Without
+// one, ptxas holds the 16-entry kernels to 64 registers and spills; 96 still
+// fits the 20 resident warps per SM that the default tile's shared memory
+// allows.  Lists of up to 8 entries fit in 80 without spilling.
 template <int KCAP>
 constexpr int query_max_regs() {
-  return KCAP <= 8 ? 72 : (KCAP <= 16 ? 96 : (KCAP <= 32 ? 128 : 224));
+  return KCAP <= 8 ? 80 : (KCAP <= 16 ? 96 : (KCAP <= 32 ? 128 : 224));
 }
 
 // A chunked item: one group with more candidates than a tile.  Out of line,
