@@ -160,24 +160,32 @@ def stream_handle(device=None) -> int:
 
 
 class Workspace:
-    """Per-(device, stream) scratch buffer, grown on demand (256-byte aligned)."""
+    """Scratch buffer per (host thread, device, stream), grown on demand
+    (256-byte aligned).  Every host thread has its own buffers: two threads
+    enqueueing on one stream at the same time would otherwise interleave
+    their launches over one buffer.  A thread's buffers go with the thread."""
 
     def __init__(self):
-        self._bufs = {}
-        self._lock = threading.Lock()
+        self._local = threading.local()
+
+    def _bufs(self) -> dict:
+        bufs = getattr(self._local, "bufs", None)
+        if bufs is None:
+            bufs = self._local.bufs = {}
+        return bufs
 
     def get(self, nbytes: int, device: torch.device) -> torch.Tensor:
         key = (device.index, torch.cuda.current_stream(device).cuda_stream)
-        with self._lock:
-            buf = self._bufs.get(key)
-            if buf is None or buf.numel() < nbytes:
-                buf = torch.empty(max(int(nbytes), 256), dtype=torch.uint8, device=device)
-                self._bufs[key] = buf
-            return buf
+        bufs = self._bufs()
+        buf = bufs.get(key)
+        if buf is None or buf.numel() < nbytes:
+            buf = torch.empty(max(int(nbytes), 256), dtype=torch.uint8, device=device)
+            bufs[key] = buf
+        return buf
 
     def clear(self):
-        with self._lock:
-            self._bufs.clear()
+        """Drop the calling thread's buffers."""
+        self._bufs().clear()
 
 
 WORKSPACE = Workspace()

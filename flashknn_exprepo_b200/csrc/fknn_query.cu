@@ -27,6 +27,10 @@
 //   * lists hold packed u64 keys (distance bits << 32 | index), so ordering
 //     is exact including ties; rows are written straight to the caller's
 //     row / index space.
+#include <algorithm>
+#include <mutex>
+#include <vector>
+
 #include "fknn_common.cuh"
 #include "fknn_networks.cuh"
 #include "fknn_internal.h"
@@ -746,34 +750,50 @@ int launch_t(const QueryLaunch& q, const QueryShape& shape, cudaStream_t s) {
       128 + static_cast<size_t>(shape.warps_per_cta) * warp_smem_bytes(shape.tile_records);
   // Device properties and occupancy are resolved once per (device, shape) and
   // cached, so a launch inside a CUDA graph capture issues nothing but the
-  // kernel itself.
+  // kernel itself.  The cache is shared by all host threads under a mutex,
+  // and the kernel's dynamic shared-memory limit is raised once per device
+  // to the device's opt-in maximum, so a launch with one shape never lowers
+  // the limit under a concurrent launch with a larger one.
   struct Cached {
-    int dev = -1, threads = 0, per_sm = 0, sms = 0;
-    size_t smem = 0;
+    int dev, threads, per_sm, sms;
+    size_t smem;
   };
-  static Cached cache;
+  static std::mutex mu;
+  static std::vector<Cached> cache;
+  static std::vector<int> raised;  // devices whose limit is raised
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
-  if (cache.dev != dev || cache.threads != threads || cache.smem != smem) {
-    Cached c;
-    c.dev = dev;
-    c.threads = threads;
-    c.smem = smem;
-    e = cudaDeviceGetAttribute(&c.sms, cudaDevAttrMultiProcessorCount, dev);
-    if (e != cudaSuccess) return e;
-    if (smem > 48 * 1024) {
-      e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               static_cast<int>(smem));
+  Cached use{};
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    bool found = false;
+    for (const Cached& c : cache)
+      if (c.dev == dev && c.threads == threads && c.smem == smem) {
+        use = c;
+        found = true;
+      }
+    if (!found) {
+      Cached c{dev, threads, 0, 0, smem};
+      e = cudaDeviceGetAttribute(&c.sms, cudaDevAttrMultiProcessorCount, dev);
       if (e != cudaSuccess) return e;
+      if (std::find(raised.begin(), raised.end(), dev) == raised.end()) {
+        int optin = 0;
+        e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+        if (e != cudaSuccess) return e;
+        e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
+        if (e != cudaSuccess) return e;
+        raised.push_back(dev);
+      }
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c.per_sm, kern, threads, smem);
+      if (e != cudaSuccess) return e;
+      if (c.per_sm < 1) c.per_sm = 1;
+      cache.push_back(c);
+      use = c;
     }
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c.per_sm, kern, threads, smem);
-    if (e != cudaSuccess) return e;
-    if (c.per_sm < 1) c.per_sm = 1;
-    cache = c;
   }
-  const int per_sm = shape.ctas_per_sm > 0 ? shape.ctas_per_sm : cache.per_sm;
-  const int grid = cache.sms * per_sm;
+  const int per_sm = shape.ctas_per_sm > 0 ? shape.ctas_per_sm : use.per_sm;
+  const int grid = use.sms * per_sm;
   const int slot = profile_start(s);
   kern<<<grid, threads, smem, s>>>(q, shape.tile_records, shape.min_candidates_per_lane);
   e = cudaGetLastError();

@@ -62,3 +62,40 @@ def test_tune_caches_and_reloads(fk, tmp_path, monkeypatch):
     i1, d1 = fk.ops.knn_offsets(xyz, off, 16, S.C3_VOXEL, 2, config=cfg)
     i0, d0 = fk.ops.knn_offsets(xyz, off, 16, S.C3_VOXEL, 2)
     assert torch.equal(i0, i1) and torch.equal(d0, d1)
+
+
+def test_concurrent_threads_with_different_shapes(fk):
+    """Host threads querying one device at once, each with its own launch
+    shape (different shared-memory sizes), on the same stream: every result
+    equals the single-threaded one (per-thread workspaces, a launch cache
+    shared under a lock)."""
+    import threading
+
+    from flashknn_exprepo_b200 import _lib
+    from flashknn_exprepo_b200 import synthetic as S
+    b = S.first_clouds(S.uneven_batch(), 3)
+    xyz = torch.from_numpy(b.xyz).to(DEV)
+    off = torch.from_numpy(b.offsets).to(DEV)
+    base = fk.ops.knn_offsets(xyz, off, 16, S.C4_VOXEL, 2)
+    torch.cuda.synchronize()
+    shapes = [(4, 448, 8, 0), (8, 1024, 8, 0), (2, 256, 4, 0), (4, 640, 16, 0)]
+    errors = []
+
+    def worker(shape):
+        try:
+            cfg = _lib.FknnConfig(*shape)
+            for _ in range(6):
+                i, d = fk.ops.knn_offsets(xyz, off, 16, S.C4_VOXEL, 2, config=cfg)
+                torch.cuda.current_stream().synchronize()
+                if not (torch.equal(i, base[0]) and torch.equal(d, base[1])):
+                    errors.append(f"shape {shape}: result differs")
+        except Exception as exc:  # reported below, on the main thread
+            errors.append(f"shape {shape}: {exc}")
+
+    threads = [threading.Thread(target=worker, args=(s,)) for s in shapes]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join(timeout=300)
+    assert not any(t.is_alive() for t in threads)
+    assert not errors, errors
