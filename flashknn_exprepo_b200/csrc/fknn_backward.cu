@@ -6,10 +6,11 @@
 //   grad_p[n] = sum_{idx_ij = n} -2 g_ij (q_i - p_n)     (segmented reduction)
 // The reference-side sum is a segmented reduction over the entries sorted by
 // neighbour index: a counting sort by idx (integer atomics count each
-// segment, a scan places the segments, a scatter fills them), then one
-// thread per support point orders its segment by entry number e = i*K+j
-// (a register sorting network; a warp-cooperative selection for segments
-// longer than 32) and sums it sequentially in ascending e.  Every FP32
+// segment, a scan places the segments, a scatter fills them with entry
+// numbers e = i*K+j), then one thread per support point orders its segment
+// by e (a register sorting network; a warp-cooperative selection for
+// segments longer than 32) and sums it sequentially in ascending e, reading
+// g_e and q_i where it adds them.  Every FP32
 // operation therefore happens in an order fixed by the inputs alone: the
 // gradients are bitwise reproducible, and no floating-point atomics are used.
 #include "fknn_common.cuh"
@@ -23,7 +24,7 @@ namespace fknn {
 namespace {
 
 constexpr int kScanTile = 1024;
-constexpr uint64_t kNoPair = ~0ull;
+constexpr uint32_t kNoEntry = ~0u;
 
 __device__ __forceinline__ bool entry_valid(int32_t t, int64_t n, float d) {
   return t >= 0 && t < n && !isinf(d);
@@ -109,35 +110,33 @@ __global__ void __launch_bounds__(kScanTile)
   }
 }
 
-// One thread per entry: scatter (e << 32 | bits of -2 g_e) into the
-// segment of its neighbour.  The slot order inside a segment depends on the
-// scheduling; the reduction below orders each segment by e.
+// One thread per entry: scatter the entry number e into the segment of its
+// neighbour (4 bytes per entry).  The slot order inside a segment depends on
+// the scheduling; the reduction below orders each segment by e.
 __global__ void __launch_bounds__(256)
     k_bwd_scatter(int64_t total, int64_t n, const int32_t* __restrict__ idx,
-                  const float* __restrict__ dist, const float* __restrict__ grad,
-                  uint32_t* __restrict__ cursor, uint64_t* __restrict__ pairs, int vec4) {
+                  const float* __restrict__ dist, uint32_t* __restrict__ cursor,
+                  uint32_t* __restrict__ seg, int vec4) {
   const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
-  auto put = [&](int64_t e, int32_t t, float d, float g) {
+  auto put = [&](int64_t e, int32_t t, float d) {
     if (!entry_valid(t, n, d)) return;
-    const uint32_t slot = atomicSub(&cursor[t], 1u) - 1u;
-    pairs[slot] = (static_cast<uint64_t>(e) << 32) | __float_as_uint(-2.f * g);
+    seg[atomicSub(&cursor[t], 1u) - 1u] = static_cast<uint32_t>(e);
   };
   if (vec4) {  // total % 4 == 0, 16-byte aligned: four entries (and atomics) in flight
     for (int64_t w = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
          w < (total >> 2); w += stride) {
       const int4 t = reinterpret_cast<const int4*>(idx)[w];
       const float4 d = reinterpret_cast<const float4*>(dist)[w];
-      const float4 g = reinterpret_cast<const float4*>(grad)[w];
-      put(4 * w, t.x, d.x, g.x);
-      put(4 * w + 1, t.y, d.y, g.y);
-      put(4 * w + 2, t.z, d.z, g.z);
-      put(4 * w + 3, t.w, d.w, g.w);
+      put(4 * w, t.x, d.x);
+      put(4 * w + 1, t.y, d.y);
+      put(4 * w + 2, t.z, d.z);
+      put(4 * w + 3, t.w, d.w);
     }
     return;
   }
   for (int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; e < total;
        e += stride)
-    put(e, idx[e], dist[e], grad[e]);
+    put(e, idx[e], dist[e]);
 }
 
 namespace {
@@ -146,39 +145,56 @@ struct Acc {
   float x = 0.f, y = 0.f, z = 0.f;
 };
 
-// One term of the reference-side sum, in the order the caller fixes.
-__device__ __forceinline__ void add_pair(Acc& a, uint64_t pr, const float* __restrict__ q_xyz,
-                                         int k, float px, float py, float pz) {
-  const int64_t i = static_cast<int64_t>(pr >> 32) / k;
-  const float g2 = __uint_as_float(static_cast<uint32_t>(pr));
+// Query row i = e / K of an entry number e < 2^31 without a division
+// instruction: Granlund and Montgomery's method for an invariant unsigned
+// divisor ("Division by invariant integers using multiplication", PLDI
+// 1994): with l = ceil(log2 K) and mul = floor(2^32 (2^l - K) / K) + 1,
+// t = umulhi(mul, e) and e / K = (t + ((e - t) >> min(l, 1))) >> max(l - 1, 0).
+struct DivK {
+  uint32_t mul;
+  int s1, s2;
+};
+
+DivK make_divk(uint32_t d) {
+  int l = 0;
+  while ((1ull << l) < d) ++l;
+  DivK r;
+  r.mul = static_cast<uint32_t>(((1ull << 32) * ((1ull << l) - d)) / d + 1);
+  r.s1 = l < 1 ? l : 1;
+  r.s2 = l > 1 ? l - 1 : 0;
+  return r;
+}
+
+__device__ __forceinline__ uint32_t div_k(uint32_t e, const DivK& dk) {
+  const uint32_t t = __umulhi(dk.mul, e);
+  return (t + ((e - t) >> dk.s1)) >> dk.s2;
+}
+
+// One term of the reference-side sum, in the order the caller fixes:
+// entry e = i*K+j adds -2 g_e (q_i - p).
+__device__ __forceinline__ void add_entry(Acc& a, uint32_t e, const float* __restrict__ q_xyz,
+                                          const float* __restrict__ grad, const DivK& k, float px,
+                                          float py, float pz) {
+  const int64_t i = div_k(e, k);
+  const float g2 = __fmul_rn(-2.f, grad[e]);
   a.x = __fmaf_rn(g2, __fsub_rn(q_xyz[3 * i], px), a.x);
   a.y = __fmaf_rn(g2, __fsub_rn(q_xyz[3 * i + 1], py), a.y);
   a.z = __fmaf_rn(g2, __fsub_rn(q_xyz[3 * i + 2], pz), a.z);
 }
 
-// Sorts a segment of at most CAP pairs in registers and sums it.
+// Sorts a segment of at most CAP entries in registers and sums it.
 template <int CAP>
-__device__ __forceinline__ void sum_short(Acc& a, const uint64_t* __restrict__ seg, uint32_t len,
-                                          const float* __restrict__ q_xyz, int k, float px,
+__device__ __forceinline__ void sum_short(Acc& a, const uint32_t* __restrict__ seg, uint32_t len,
+                                          const float* __restrict__ q_xyz,
+                                          const float* __restrict__ grad, const DivK& k, float px,
                                           float py, float pz) {
-  uint64_t L[CAP];
+  uint32_t L[CAP];
 #pragma unroll
-  for (int c = 0; c < CAP; ++c) L[c] = c < static_cast<int>(len) ? seg[c] : kNoPair;
+  for (int c = 0; c < CAP; ++c) L[c] = c < static_cast<int>(len) ? seg[c] : kNoEntry;
   sort_network<CAP, 0, CAP>(L);
 #pragma unroll
   for (int c = 0; c < CAP; ++c)
-    if (c < static_cast<int>(len)) add_pair(a, L[c], q_xyz, k, px, py, pz);
-}
-
-__device__ __forceinline__ uint64_t warp_min_u64(uint64_t v) {
-#pragma unroll
-  for (int s = 16; s > 0; s >>= 1) {
-    const uint64_t o = (static_cast<uint64_t>(__shfl_xor_sync(kFull, static_cast<uint32_t>(v >> 32), s))
-                        << 32) |
-                       __shfl_xor_sync(kFull, static_cast<uint32_t>(v), s);
-    v = o < v ? o : v;
-  }
-  return v;
+    if (c < static_cast<int>(len)) add_entry(a, L[c], q_xyz, grad, k, px, py, pz);
 }
 
 }  // namespace
@@ -188,10 +204,10 @@ __device__ __forceinline__ uint64_t warp_min_u64(uint64_t v) {
 // them as a neighbour) are taken by the whole warp, one at a time: every
 // round the warp selects the smallest remaining e (entries are distinct),
 // so the order and the arithmetic are those of the short path.
-__global__ void __launch_bounds__(128)
+__global__ void __maxnreg__(96)
     k_bwd_support(const float* __restrict__ q_xyz, const float* __restrict__ p_xyz, int64_t n,
-                  int k, const uint32_t* __restrict__ start, const uint64_t* __restrict__ pairs,
-                  float* __restrict__ grad_p, int accumulate) {
+                  DivK k, const uint32_t* __restrict__ start, const uint32_t* __restrict__ seg,
+                  const float* __restrict__ grad, float* __restrict__ grad_p, int accumulate) {
   const int64_t p0 = static_cast<int64_t>(blockIdx.x) * blockDim.x;
   if (p0 >= n) return;  // whole warps leave together: n is the same for all
   const int64_t p = p0 + threadIdx.x;
@@ -209,9 +225,9 @@ __global__ void __launch_bounds__(128)
   Acc a;
   const bool long_seg = len > 32;
   if (__any_sync(kFull, !long_seg && len > 16)) {
-    if (!long_seg) sum_short<32>(a, pairs + s, len, q_xyz, k, px, py, pz);
+    if (!long_seg) sum_short<32>(a, seg + s, len, q_xyz, grad, k, px, py, pz);
   } else if (!long_seg && len > 0) {
-    sum_short<16>(a, pairs + s, len, q_xyz, k, px, py, pz);
+    sum_short<16>(a, seg + s, len, q_xyz, grad, k, px, py, pz);
   }
   uint32_t todo = __ballot_sync(kFull, long_seg);
   while (todo) {
@@ -223,15 +239,15 @@ __global__ void __launch_bounds__(128)
     const float ly = __shfl_sync(kFull, py, leader);
     const float lz = __shfl_sync(kFull, pz, leader);
     Acc b;
-    uint64_t last = 0;
+    uint32_t last = 0;
     for (uint32_t r = 0; r < ll; ++r) {
-      uint64_t best = kNoPair;
+      uint32_t best = kNoEntry;
       for (uint32_t t = lane; t < ll; t += 32) {
-        const uint64_t v = pairs[ls + t];
+        const uint32_t v = seg[ls + t];
         if ((r == 0 || v > last) && v < best) best = v;
       }
-      best = warp_min_u64(best);
-      add_pair(b, best, q_xyz, k, lx, ly, lz);
+      best = __reduce_min_sync(kFull, best);
+      add_entry(b, best, q_xyz, grad, k, lx, ly, lz);
       last = best;
     }
     if (lane == leader) a = b;
@@ -258,7 +274,7 @@ struct BwdBufs {
   uint32_t* start;    // [n + 1]
   uint32_t* cursor;   // [n]
   uint32_t* tiles;    // [n_tiles]
-  uint64_t* pairs;    // [m * k]
+  uint32_t* seg;      // [m * k] entry numbers grouped by neighbour
   int* total;         // valid entries (written by the tile scan)
 };
 
@@ -270,7 +286,7 @@ BwdBufs bwd_layout(void* ws, int64_t m, int64_t n, int k, size_t* bytes) {
   b.start = a.take<uint32_t>(n + 1);
   b.cursor = a.take<uint32_t>(n);
   b.tiles = a.take<uint32_t>(ceil_div(n > 0 ? n : 1, kScanTile));
-  b.pairs = a.take<uint64_t>(m * k);
+  b.seg = a.take<uint32_t>(m * k);
   if (bytes) *bytes = a.used + 256;
   return b;
 }
@@ -321,11 +337,12 @@ int run_backward(const BackwardArgs& a, void* ws, size_t ws_bytes, cudaStream_t 
     if (total > 0) {
       const int64_t sb = ceil_div(total, 256);
       k_bwd_scatter<<<static_cast<int>(sb < 8192 ? sb : 8192), 256, 0, s>>>(
-          total, a.n, a.idx, a.dist, a.grad, b.cursor, b.pairs, vec4 ? 1 : 0);
+          total, a.n, a.idx, a.dist, b.cursor, b.seg, vec4 ? 1 : 0);
       ++nl;
     }
-    k_bwd_support<<<blocks_for(a.n, 128), 128, 0, s>>>(a.q_xyz, a.p_xyz, a.n, a.k, b.start,
-                                                       b.pairs, a.grad_p, a.accumulate);
+    k_bwd_support<<<blocks_for(a.n, 128), 128, 0, s>>>(a.q_xyz, a.p_xyz, a.n,
+                                                       make_divk(static_cast<uint32_t>(a.k)), b.start,
+                                                       b.seg, a.grad, a.grad_p, a.accumulate);
     ++nl;
   }
   e = cudaGetLastError();

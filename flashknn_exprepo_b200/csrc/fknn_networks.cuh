@@ -1,4 +1,4 @@
-// Ascending sorting networks over a register array of uint64 keys.
+// Ascending sorting networks over a register array of unsigned keys.
 #pragma once
 
 #include <cstdint>
@@ -11,16 +11,16 @@ namespace fknn {
 // odd-even merge.  Each network was checked with the 0-1 principle (all
 // 2^n binary inputs for n <= 16, all pairs of sorted binary halves for the
 // merges).
-template <int KCAP>
-__device__ __forceinline__ void cas_up(uint64_t (&L)[KCAP], int i, int j) {
-  const uint64_t a = L[i], b = L[j];
+template <int KCAP, typename T>
+__device__ __forceinline__ void cas_up(T (&L)[KCAP], int i, int j) {
+  const T a = L[i], b = L[j];
   const bool sw = b < a;
   L[i] = sw ? b : a;
   L[j] = sw ? a : b;
 }
 
-template <int KCAP, int LO, int N, int R>
-__device__ __forceinline__ void odd_even_merge(uint64_t (&L)[KCAP]) {
+template <int KCAP, int LO, int N, int R, typename T>
+__device__ __forceinline__ void odd_even_merge(T (&L)[KCAP]) {
   constexpr int M = R * 2;
   if constexpr (M < N) {
     odd_even_merge<KCAP, LO, N, M>(L);
@@ -32,8 +32,8 @@ __device__ __forceinline__ void odd_even_merge(uint64_t (&L)[KCAP]) {
   }
 }
 
-template <int KCAP, int OFF, int N>
-__device__ __forceinline__ void sort_network(uint64_t (&L)[KCAP]) {
+template <int KCAP, int OFF, int N, typename T>
+__device__ __forceinline__ void sort_network(T (&L)[KCAP]) {
   if constexpr (N == 2) {
     cas_up<KCAP>(L, OFF, OFF + 1);
   } else if constexpr (N == 4) {
