@@ -350,7 +350,7 @@ def run_ours(args, rank, world, local_rank, dist):
                   "h2d_bytes_per_step": int(xyz_pin.numel() * 4 + off_pin.numel() * 8),
                   "d2h_bytes_per_step": int(n * k * 8),
                   "call": "knn_query_host: pinned host in/out, copies overlapped with the "
-                          "query in 4 whole-cloud runs",
+                          "query in 8 whole-cloud runs",
                   "single_call": {"value": n * args.steps / (single_total / 1e3),
                                   "unit": "queries/s",
                                   "call": "H2D, knn_query, D2H of idx and dist, one after "

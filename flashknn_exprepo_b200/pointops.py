@@ -181,12 +181,15 @@ def ball_query_and_group(feat, xyz, offset=None, new_xyz=None, new_offset=None, 
 
 
 def knn_query_host(nsample, xyz, offset, idx_out=None, dist_out=None, *, voxel_size,
-                   num_down=2, chunks=4, device=None, config=None):
+                   num_down=2, chunks=8, device=None, config=None):
     """Self query of an offset batch held in host memory, answers written to
     host memory: the call for a caller whose points arrive from and whose
     neighbours go back to the CPU.
 
-    The batch is cut into ``chunks`` runs of whole clouds of about equal size.
+    The batch is cut into ``chunks`` runs of whole clouds of about equal size
+    (8 by default: fewer runs leave more of the first run's upload and query
+    outside the overlap, more runs cost more host-side launch work than they
+    hide).
     Each run's upload, query and index shift run on the current stream, and
     its download starts on a second stream as soon as the run is done, so the
     device-to-host copy of one run overlaps the upload and query of the next
@@ -214,6 +217,12 @@ def knn_query_host(nsample, xyz, offset, idx_out=None, dist_out=None, *, voxel_s
         if e >= target * len(cuts) and c + 1 < len(ends) and len(cuts) < chunks:
             cuts.append(c + 1)
     cuts.append(len(ends))
+    # every run's cloud ends relative to its first point, uploaded once from
+    # pinned memory (a copy from pageable memory would wait for the stream)
+    local = offset.clone()
+    for a, b in zip(cuts[:-1], cuts[1:]):
+        local[a:b] -= ends[a - 1] if a else 0
+    local_dev = local.pin_memory().to(dev, non_blocking=True)
     compute = torch.cuda.current_stream(dev)
     copy = torch.cuda.Stream(dev)
     for a, b in zip(cuts[:-1], cuts[1:]):
@@ -222,8 +231,8 @@ def knn_query_host(nsample, xyz, offset, idx_out=None, dist_out=None, *, voxel_s
         start = ends[a - 1] if a else 0
         stop = ends[b - 1]
         x = xyz[start:stop].to(dev, non_blocking=True)
-        o = (offset[a:b] - start).to(dev, non_blocking=True)
-        idx, dist = ops.knn_offsets(x, o, nsample, voxel_size, num_down, config=config)
+        idx, dist = ops.knn_offsets(x, local_dev[a:b], nsample, voxel_size, num_down,
+                                    config=config)
         if start:
             idx += start                               # run-local -> batch indices
         done = torch.cuda.Event()
