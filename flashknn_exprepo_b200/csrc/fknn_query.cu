@@ -204,7 +204,9 @@ __device__ __forceinline__ int stop_position(const uint64_t (&L)[KCAP], const Gr
   const uint64_t last = L[KCAP - 1];
   if (last == kEmpty) return s.len;
   const float thr = __uint_as_float(static_cast<uint32_t>(last >> 32));
-  const float reach = rq + sqrtf(thr) * 1.0001f + s.eps;
+  // thr * rsqrt(thr) is within a few ulp of sqrt(thr), far inside the 1e-4
+  // margin; thr == 0 or +inf gives NaN, which skips no bucket
+  const float reach = rq + thr * rsqrtf(thr) * 1.0001f + s.eps;
   const float lim = reach * reach * s.inv_w2;
   if (!(lim < static_cast<float>(kBuckets - 1))) return s.len;
   return bstart[static_cast<int>(lim) + 1];
