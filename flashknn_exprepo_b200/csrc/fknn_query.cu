@@ -754,8 +754,9 @@ int launch_t(const QueryLaunch& q, const QueryShape& shape, cudaStream_t s) {
   // cached, so a launch inside a CUDA graph capture issues nothing but the
   // kernel itself.  The cache is shared by all host threads under a mutex,
   // and the kernel's dynamic shared-memory limit is raised once per device
-  // to the device's opt-in maximum, so a launch with one shape never lowers
-  // the limit under a concurrent launch with a larger one.
+  // to the device's opt-in maximum (less the kernel's static shared memory),
+  // so a launch with one shape never lowers the limit under a concurrent
+  // launch with a larger one.
   struct Cached {
     int dev, threads, per_sm, sms;
     size_t smem;
@@ -783,7 +784,11 @@ int launch_t(const QueryLaunch& q, const QueryShape& shape, cudaStream_t s) {
         int optin = 0;
         e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
         if (e != cudaSuccess) return e;
-        e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
+        cudaFuncAttributes fa{};
+        e = cudaFuncGetAttributes(&fa, kern);
+        if (e != cudaSuccess) return e;
+        e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 optin - static_cast<int>(fa.sharedSizeBytes));
         if (e != cudaSuccess) return e;
         raised.push_back(dev);
       }
