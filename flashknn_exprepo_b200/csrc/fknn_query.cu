@@ -28,6 +28,7 @@
 //     is exact including ties; rows are written straight to the caller's
 //     row / index space.
 #include <algorithm>
+#include <cfloat>
 #include <mutex>
 #include <vector>
 
@@ -203,10 +204,12 @@ __device__ __forceinline__ int stop_position(const uint64_t (&L)[KCAP], const Gr
                                              float rq, const uint16_t* bstart) {
   const uint64_t last = L[KCAP - 1];
   if (last == kEmpty) return s.len;
-  const float thr = __uint_as_float(static_cast<uint32_t>(last >> 32));
-  // thr * rsqrt(thr) is within a few ulp of sqrt(thr), far inside the 1e-4
-  // margin; thr == 0 or +inf gives NaN, which skips no bucket
-  const float reach = rq + thr * rsqrtf(thr) * 1.0001f + s.eps;
+  // m * rsqrt(m) is within a few ulp of sqrt(m), far inside the 1e-4 margin;
+  // m >= FLT_MIN keeps a K-th distance of 0 (a query on a support point) or
+  // a subnormal one bounded from above, and +inf gives NaN, which skips no
+  // bucket
+  const float m = fmaxf(__uint_as_float(static_cast<uint32_t>(last >> 32)), FLT_MIN);
+  const float reach = rq + m * rsqrtf(m) * 1.0001f + s.eps;
   const float lim = reach * reach * s.inv_w2;
   if (!(lim < static_cast<float>(kBuckets - 1))) return s.len;
   return bstart[static_cast<int>(lim) + 1];
