@@ -249,3 +249,31 @@ def test_hub_points_with_long_segments(fk):
                             g.cpu().numpy().astype(np.float64))
     assert _rel_max(outs[0][0], wq) <= 1e-5
     assert _rel_max(outs[0][1], wp) <= 1e-5
+
+
+@pytest.mark.parametrize("k", [1, 3, 7, 12, 24, 33, 64])
+def test_backward_list_lengths(fk, k):
+    """Every row length: entry e = i*K+j maps back to its query row by a
+    multiply-shift division (exact for every K, power of two or not), and
+    K not a multiple of 4 takes the scalar row loads.  Against the oracle's
+    FP64 backward, and bitwise identical run to run."""
+    rng = np.random.default_rng(100 + k)
+    xyz = rng.random((6000, 3), dtype=np.float32)
+    n = len(xyz)
+    x = torch.from_numpy(xyz).to(DEV)
+    offs = torch.tensor([n], device=DEV)
+    idx, dist = fk.ops.knn_offsets(x, offs, k, 0.02, 2)
+    g = torch.from_numpy(rng.standard_normal((n, k)).astype(np.float32)).to(DEV)
+    g = _masked(g, dist)
+    outs = []
+    for _ in range(2):
+        gq = torch.empty_like(x)
+        gp = torch.empty_like(x)
+        fk.ops.backward(x, x, idx, dist, g, grad_q=gq, grad_p=gp)
+        outs.append((gq.cpu().numpy(), gp.cpu().numpy()))
+    for a, b in zip(outs[0], outs[1]):
+        assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+    wq, wp = O.backward_f64(xyz, xyz, idx.cpu().numpy(), dist.cpu().numpy(),
+                            g.cpu().numpy().astype(np.float64))
+    assert _rel_max(outs[0][0], wq) <= 1e-5
+    assert _rel_max(outs[0][1], wp) <= 1e-5
