@@ -148,16 +148,41 @@ def measured_peak_hbm():
     return 6650.0, "fallback"
 
 
+def _query_profile(k):
+    path = os.path.join(ROOT, "profiles", f"k_query_uneven_batch_k{k}.txt")
+    if not os.path.exists(path):
+        return None, None
+    with open(path) as f:
+        return os.path.relpath(path, ROOT), f.read()
+
+
 def profiled_traffic(k):
     """DRAM bytes (read + write) of one query-kernel launch on this workload,
     from the committed ncu summary of that kernel; None when absent."""
-    path = os.path.join(ROOT, "profiles", f"k_query_uneven_batch_k{k}.txt")
-    if not os.path.exists(path):
-        return None
     import re
-    with open(path) as f:
-        m = re.search(r"dram_bytes_per_launch\s*=\s*([0-9]+)", f.read())
+    _, text = _query_profile(k)
+    m = re.search(r"dram_bytes_per_launch\s*=\s*([0-9]+)", text or "")
     return int(m.group(1)) if m else None
+
+
+def profiled_limiter(k):
+    """The unit that bounds the query kernel, from the same ncu summary: the
+    kernel is instruction-bound (ALU pipe), so the HBM fraction alone does
+    not describe it."""
+    import re
+    path, text = _query_profile(k)
+    if text is None:
+        return None
+    alu = re.search(r"sm__inst_executed_pipe_alu \(active\)\s+([0-9.]+) %", text)
+    issue = re.search(r"smsp__issue_active \(active\)\s+([0-9.]+) %", text)
+    per_q = re.search(r"~([0-9]+) warp instructions per query", text)
+    if not (alu and issue and per_q):
+        return None
+    return {"unit": "ALU pipe (integer compare/select)",
+            "alu_pipe_active_pct": float(alu.group(1)),
+            "issue_active_pct": float(issue.group(1)),
+            "warp_instructions_per_query": int(per_q.group(1)),
+            "source": path}
 
 
 def cpu_cores():
@@ -840,7 +865,8 @@ def main():
         achieved = algo_bytes / (avg * 1e-3) / 1e9
         roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                     "frac": achieved / peak, "traffic": profiled_traffic(k),
-                    "kernel": "fknn::k_query<16>", "kernel_ms": avg,
+                    "kernel": f"fknn::k_query<{1 << max(0, (k - 1).bit_length())}>",
+                    "kernel_ms": avg, "limiter": profiled_limiter(k),
                     "algorithmic_bytes_per_launch": algo_bytes,
                     "peak_source": f"{peak_kind} hbm_gbs"}
     line = {
