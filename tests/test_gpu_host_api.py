@@ -39,3 +39,17 @@ def test_host_query_into_caller_buffers(fk):
     assert out[0] is idx and out[1] is dist
     di, dd = fk.ops.knn_offsets(xyz.cuda(), off.cuda(), 8, 0.02, 2)
     assert torch.equal(idx, di.cpu()) and torch.equal(dist, dd.cpu())
+
+
+@pytest.mark.parametrize("chunks", [2, 4, 8])
+def test_host_query_with_empty_clouds(fk, chunks):
+    """Empty clouds (repeated ends) anywhere in the offsets, including whole
+    runs of them: every run is still answered and placed by its offsets."""
+    rng = np.random.default_rng(5)
+    xyz = torch.from_numpy(rng.random((4000, 3), dtype=np.float32)).pin_memory()
+    off = torch.tensor([0, 1000, 1000, 1000, 2500, 2500, 4000, 4000])
+    idx, dist = fk.knn_query_host(8, xyz, off, voxel_size=0.02, chunks=chunks)
+    torch.cuda.current_stream().synchronize()
+    di, dd = fk.ops.knn_offsets(xyz.cuda(), off.cuda(), 8, 0.02, 2)
+    assert torch.equal(idx, di.cpu())
+    assert torch.equal(dist.view(torch.int32), dd.cpu().view(torch.int32))
