@@ -230,7 +230,7 @@ def nanoflann_rate(batch, k, steps, warmup):
         _, _, tb, tq = ref_nanoflann.knn(batch.xyz, batch.offsets, k, nthreads=cores)
         secs.append(tb + tq)
     return {"value": n * len(secs) / sum(secs), "unit": "queries/s", "cores": cores,
-            "kind": "reference",
+            "kind": "reference", "ms_per_step": sum(secs) / len(secs) * 1e3,
             "sample": f"whole batch ({n} points, {len(batch.offsets)} clouds) x {steps} passes: "
                       f"nanoflann KD-tree build (leaf 20) + exact K={k} query, OpenMP x{cores}"}
 
@@ -421,6 +421,22 @@ def extras_single_gpu(args, fk, torch, dev, batch, voxel, flush):
     res["per_cloud"] = {"value": n * reps / (sum(ms) / 1e3), "unit": "queries/s",
                         "ms_per_step": sum(ms) / reps,
                         "what": "loop of 16 plain fknn_knn_offsets calls, one per cloud, eager"}
+    # the same loop captured in one CUDA graph: no host launch overhead, so
+    # the comparison with the batched step is launch model against launch model
+    stream = torch.cuda.Stream(dev)
+    stream.wait_stream(torch.cuda.current_stream(dev))
+    with torch.cuda.stream(stream):
+        per_cloud()  # workspace of this stream sized for the largest cloud
+        torch.cuda.synchronize(dev)
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph, stream=stream):
+            per_cloud()
+    torch.cuda.current_stream(dev).wait_stream(stream)
+    torch.cuda.synchronize(dev)
+    gms = _event_ms(torch, graph.replay, flush, reps=reps)
+    del graph
+    res["per_cloud_graph"] = {"value": n / (gms * 1e-3), "unit": "queries/s", "ms_per_step": gms,
+                              "what": "the same 16 per-cloud calls replayed from one CUDA graph"}
 
     # forward + backward (loss = sum(w * d), w ~ N(0,1))
     xyz = torch.from_numpy(batch.xyz).to(dev)
@@ -591,6 +607,20 @@ def rows_single_gpu(fk, torch, dev, flush, peak_gbs):
                                      "ms": ms, "build_tables_ms": bms,
                                      "what": "reference table ABI (FlashKNN_Query_Dynamic_Load "
                                              "boundary): query on caller-built tables"}
+    # the largest cloud of the uneven batch through the table ABI at K=16
+    # (tables from fknn_build_tables, equal to the reference's own; the
+    # reference arm times FlashKNN_Query_Dynamic_Load on them)
+    c = int(np.argmax(b.counts))
+    lx_ = T(b.xyz[int(b.offsets[c] - b.counts[c]):int(b.offsets[c])])
+    lgrid = torch.floor(lx_ * (1.0 / synthetic.C4_VOXEL)).long()
+    ltb = fk.ops.build_tables(lgrid, None, 2)
+    lxs = lx_[ltb["order"]].contiguous()
+    ms = _event_ms(torch, lambda: fk.ops.query_tables(lxs, ltb["steps"], ltb["neigh"],
+                                                      ltb["cnt"], 16), flush)
+    rows["query_tables_largest_cloud_k16"] = {
+        "value": lx_.shape[0] / (ms * 1e-3), "unit": "queries/s", "ms": ms,
+        "n_points": int(lx_.shape[0]),
+        "what": "reference table ABI on the largest cloud of the uneven batch"}
     # the same stride-4 queries through the selected-query table ABI: qindex =
     # their sorted positions grouped by parent, steps_query = per-parent offsets
     inv = torch.empty_like(tb["order"])
@@ -774,6 +804,7 @@ def run_reference(args):
                                            "construction + query)",
             "value": value, "unit": "queries/s", "higher_is_better": True,
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": n / value * 1e3,
             "dtype": "f32", "data": "synthetic (seeded, stands in for S3DIS/SemanticKITTI)",
             "config": {"workload": "uneven_batch_16clouds_k16", "n_points": n,
                        "k": k, "voxel_m": voxel, "num_down": 2},
@@ -785,7 +816,53 @@ def run_reference(args):
         line["reference_gpu_per_cloud"] = reference_gpu_per_cloud(batch, k, voxel)
     except Exception as exc:  # context only: never fails the CPU arm
         line["reference_gpu_per_cloud"] = {"unavailable": f"{type(exc).__name__}: {exc}"[:200]}
+    try:
+        line["reference_kernel"] = reference_kernel_rows(batch)
+    except Exception as exc:  # context only
+        line["reference_kernel"] = {"unavailable": f"{type(exc).__name__}: {exc}"[:200]}
     return line
+
+
+def reference_kernel_rows(batch):
+    """The reference's production kernel alone (FlashKNN_Query_Dynamic_Load
+    built for sm_100a) on the tables its own construction builds, timed with
+    CUDA events around each call, L2 flushed before each: the room at K=32
+    and the largest cloud of the uneven batch at K=16.  Our arm's rows
+    query_tables_room_k32 / query_tables_largest_cloud_k16 time
+    fknn_query_tables on the same tables (the tables are equal bit for bit:
+    tests/test_gpu_reference_parity.py).  The reference launcher ends with a
+    cudaDeviceSynchronize, so its closing event is recorded only after the
+    host wakes up: `sync_gap_ms` is that gap measured alone (two events
+    around a synchronise of an idle stream), an upper bound of what the
+    events add to the kernel time."""
+    import torch
+    from flashknn_exprepo_b200 import synthetic
+    from oracle import ref_kernels, ref_pipeline
+    if not torch.cuda.is_available():
+        return {"unavailable": "no CUDA device"}
+    if not ref_kernels.available():
+        return {"unavailable": "reference kernels not built (oracle/build_ref.py)"}
+    cufun = ref_kernels.load()
+    dev = torch.device("cuda", 0)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
+    c = int(np.argmax(batch.counts))
+    cases = [("room_k32", synthetic.room(), synthetic.C2_VOXEL, 32),
+             ("largest_cloud_k16",
+              batch.xyz[int(batch.offsets[c] - batch.counts[c]):int(batch.offsets[c])],
+              synthetic.C4_VOXEL, 16)]
+    out = {}
+    for name, xyz, voxel, k in cases:
+        x = torch.from_numpy(np.ascontiguousarray(xyz)).to(dev)
+        grid = torch.floor(x * (1.0 / voxel)).long()
+        t = ref_pipeline.reference_tables(cufun, grid, torch.zeros_like(grid[:, 0]), x, 2)
+        ri = torch.zeros((len(xyz), k), dtype=torch.int32, device=dev)
+        rd = torch.zeros((len(xyz), k), dtype=torch.float32, device=dev)
+        ms = _event_ms(torch, lambda: cufun.FlashKNN_Query_Dynamic_Load(
+            t["xyz_sorted"], t["steps"], t["neigh"], t["cnt"], k, ri, rd, 1, math.inf), flush)
+        out[name] = {"value": len(xyz) / (ms * 1e-3), "unit": "queries/s", "ms": ms,
+                     "n_points": int(len(xyz))}
+    out["sync_gap_ms"] = _event_ms(torch, torch.cuda.synchronize, flush)
+    return out
 
 
 def reference_gpu_per_cloud(batch, k, voxel):
@@ -888,6 +965,9 @@ def main():
     if "per_cloud" in out:
         line["per_cloud"] = out["per_cloud"]
         line["batched_vs_per_cloud"] = out["value"] / out["per_cloud"]["value"]
+    if "per_cloud_graph" in out:
+        line["per_cloud_graph"] = out["per_cloud_graph"]
+        line["batched_vs_per_cloud_graph"] = out["value"] / out["per_cloud_graph"]["value"]
     if "fwd_bwd_ms" in out:
         line["fwd_bwd_ms"] = out["fwd_bwd_ms"]
     if "fd_check" in out:

@@ -66,6 +66,7 @@ _SIGNATURES = {
     "fknn_error_string": (ctypes.c_char_p, [ctypes.c_int]),
     "fknn_last_cuda_error": (ctypes.c_int, []),
     "fknn_read_status": (ctypes.c_int, [_P, _P, _P]),
+    "fknn_read_candidate_stats": (ctypes.c_int, [_P, _P, _P, _P]),
     "fknn_last_launch_count": (ctypes.c_int, []),
     "fknn_profile_enable": (ctypes.c_int, [ctypes.c_int]),
     "fknn_profile_read": (ctypes.c_int, [_P, ctypes.c_int]),
@@ -82,6 +83,7 @@ _SIGNATURES = {
                                          _P, _P]),
     "fknn_query_tables_noalloc": (ctypes.c_int, [_P, _I64, _P, _P, _P, _I64, _I32, _F32, _P, _P,
                                                  _P]),
+    "fknn_query_tables_noalloc_read_status": (ctypes.c_int, [_P, _P]),
     "fknn_selected_query_tables": (ctypes.c_int, [_P, _I64, _P, _I64, _P, _P, _P, _P, _I64, _I32,
                                                   _F32, _P, _P, _P, _SZ, _P, _P]),
     "fknn_morton_encode": (ctypes.c_int, [_P, _P, _I64, _P, _P]),
@@ -197,6 +199,16 @@ def read_status(ws: torch.Tensor) -> int:
     check(lib.fknn_read_status(ptr(ws), ctypes.byref(out), stream_handle(ws.device)),
           "fknn_read_status")
     return out.value
+
+
+def candidate_stats(ws: torch.Tensor) -> tuple[int, int]:
+    """(candidate total, groups) of the last self / general query that used
+    ``ws`` (fknn_read_candidate_stats; synchronises the stream)."""
+    lib = load()
+    total, groups = ctypes.c_int64(0), ctypes.c_int64(0)
+    check(lib.fknn_read_candidate_stats(ptr(ws), ctypes.byref(total), ctypes.byref(groups),
+                                        stream_handle(ws.device)), "fknn_read_candidate_stats")
+    return total.value, groups.value
 
 
 def raise_on_status(ws: torch.Tensor, what: str, ignore: int = DEVICE_NO_CANDIDATES) -> None:

@@ -185,6 +185,24 @@ int fknn_read_status(const void* workspace, int* status, void* stream) {
   return FKNN_OK;
 }
 
+int fknn_read_candidate_stats(const void* workspace, int64_t* total, int64_t* groups,
+                              void* stream) {
+  if (!workspace || !total || !groups) return FKNN_ERR_ARG;
+  fknn::Meta meta{};
+  cudaError_t e = cudaMemcpyAsync(&meta, workspace, sizeof(meta), cudaMemcpyDeviceToHost,
+                                  as_stream(stream));
+  if (e == cudaSuccess) e = cudaStreamSynchronize(as_stream(stream));
+  if (e != cudaSuccess) {
+    fknn::note_cuda_error(e);
+    return FKNN_ERR_CUDA;
+  }
+  *total = static_cast<int64_t>(meta.cand_total);
+  // self queries group by support cell (n_groups stays 0), general queries
+  // by query cell
+  *groups = meta.n_groups > 0 ? meta.n_groups : meta.n_cells;
+  return FKNN_OK;
+}
+
 size_t fknn_workspace_bytes(int64_t n_support, int64_t n_query, int64_t n_clouds,
                             int32_t query_kind) {
   if (n_support < 0 || n_query < 0 || n_clouds < 1 || query_kind < 0 || query_kind > 2) return 0;

@@ -463,12 +463,17 @@ __device__ __forceinline__ int2 hash_find(const HashSlot* table, uint32_t mask, 
 // key in the support key space; runs[g*27 + j] = (start, count) of the
 // support cell at offset j, or (0, 0) when that cell is empty.  With cands,
 // cands[g] = the group's candidate total (the work-item packer's input; a
-// group without candidates sets kStatusNoCandidates in *status).
+// group without candidates sets kStatusNoCandidates in *status) and
+// meta->cand_total receives the sum of the totals (one atomic per block).
 __global__ void __launch_bounds__(256)
     k_runs(const uint64_t* __restrict__ group_key, const int* group_count_ptr,
            const HashSlot* __restrict__ table, uint32_t hmask, const int* cell_count_ptr,
-           const Meta* meta, int2* __restrict__ runs, int32_t* __restrict__ cands,
+           Meta* meta, int2* __restrict__ runs, int32_t* __restrict__ cands,
            int* status) {
+  __shared__ unsigned long long block_total;
+  if (threadIdx.x == 0) block_total = 0ull;
+  __syncthreads();
+  unsigned long long my_total = 0ull;
   const int groups = *group_count_ptr;
   const int bpa = meta->bpa;
   const int cells = *cell_count_ptr;
@@ -498,9 +503,15 @@ __global__ void __launch_bounds__(256)
       const int total = __reduce_add_sync(kFull, run.y);
       if (j == 0) {
         cands[g] = total;
+        my_total += static_cast<unsigned long long>(total);
         if (total == 0) raise_status(status, kStatusNoCandidates);
       }
     }
+  }
+  if (cands) {
+    if (my_total) atomicAdd(&block_total, my_total);
+    __syncthreads();
+    if (threadIdx.x == 0 && block_total) atomicAdd(&meta->cand_total, block_total);
   }
 }
 

@@ -23,9 +23,13 @@ struct Meta {
   int batch_bits;   // bits of the largest batch id
   int max_extent;   // largest per-cloud parent-coordinate extent
   int n_points_scanned;  // total of a scan over per-cell point counts (= n)
-  int reserved[5];
+  int reserved[3];  // per-path scratch words (the adaptive octree's)
+  // sum over the query groups of their 27-cell candidate totals (self and
+  // general queries; read back for FlashKNN.query's traverse_info)
+  unsigned long long cand_total;
 };
 static_assert(sizeof(Meta) == 64, "Meta layout");
+static_assert(offsetof(Meta, cand_total) == 56, "Meta layout");
 
 // Work items (int4): (q_start, q_count, g_first, g_count | flags) -- the
 // queries [q_start, q_start + q_count) of the query-record array, which

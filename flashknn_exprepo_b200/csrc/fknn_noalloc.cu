@@ -21,6 +21,13 @@
 // The first call on each device looks up the array's device address
 // (cudaGetSymbolAddress) with that device current; make that first call
 // before any stream capture.  Later calls only launch work on the stream.
+// The address is kept for the life of the process: calls after a device
+// reset (cudaDeviceReset, which unloads the array) are not supported.
+//
+// Problems only the device can see (tables naming rows outside the point
+// array, a bounded wait that gave up) are OR-ed into a status word at the
+// start of the array, as fknn_query_tables does in its workspace; each call
+// clears it first.  fknn_query_tables_noalloc_read_status copies it out.
 #include <cstdint>
 #include <mutex>
 
@@ -90,4 +97,13 @@ extern "C" int fknn_query_tables_noalloc(const float* xyz_sorted, int64_t n,
                                    static_cast<cudaStream_t>(stream), &launches);
   if (out == FKNN_OK) fknn::note_launches(launches);
   return out;
+}
+
+extern "C" int fknn_query_tables_noalloc_read_status(int* status, void* stream) {
+  if (!status) return FKNN_ERR_ARG;
+  void* scratch = nullptr;
+  const int rc = scratch_address(&scratch);
+  if (rc != FKNN_OK) return rc;
+  // the status word is the first int of the scratch, as in every workspace
+  return fknn_read_status(scratch, status, stream);
 }

@@ -89,10 +89,12 @@ def _offsets_call(entry, xyz, offset, k, voxel, num_down, new_xyz, new_offset, l
 
 
 def knn_grid(xyz, grid_coord, batch_idx, k, num_down=2, cut_r2=math.inf, query_indices=None,
-             idx_dtype=torch.int64, config=None, validate=False):
+             idx_dtype=torch.int64, config=None, validate=False, candidate_stats=None):
     """FlashKNN.query / selected_query on caller-voxelised grid coordinates.
 
     Returns (idx [m,k] of ``idx_dtype`` in original point numbering, dist2 f32).
+    With ``candidate_stats`` (a list) a self query appends (candidate total,
+    parent cells) read back from the device (one synchronisation).
     """
     lib = _lib.load()
     grid_coord = _require(grid_coord, "grid_coord", torch.int64, 2, 3)
@@ -123,6 +125,8 @@ def knn_grid(xyz, grid_coord, batch_idx, k, num_down=2, cut_r2=math.inf, query_i
     check(rc, "fknn_knn_grid")
     if validate:
         _lib.raise_on_status(ws, "knn_grid")
+    if candidate_stats is not None:
+        candidate_stats.append(_lib.candidate_stats(ws))
     return idx, dist
 
 

@@ -19,6 +19,7 @@ from __future__ import annotations
 import math
 import time
 
+import numpy as np
 import torch
 
 from . import ops
@@ -90,19 +91,25 @@ class FlashKNN:
         num_down).  Returns int64 [N, K] original indices; with
         ``return_distances`` returns (int32 indices, f32 squared distances).
         ``batch_for_prune`` and ``dynamic_load`` are accepted and unused, as in
-        the reference kernel.
+        the reference kernel.  ``traverse_info[0]`` receives the mean number
+        of candidates per parent cell (the points of its 27 neighbour cells),
+        as FlashKnnWrapper.py:351-352 writes it: summed exactly on the device
+        and rounded to FP32 (the reference takes an FP32 mean).
         """
         self._check_modes(memory_mode, sorting_mode, candidate_mode, enable_skip,
                           thread_group_size)
         t0 = time.perf_counter() if self.debug else 0.0
         coords = xyz if xyz is not None else grid_coord.float()
+        stats = [] if traverse_info is not None else None
         idx, dist = ops.knn_grid(
             coords, grid_coord, batch_idx, self.num_nbr, self.num_down,
             cut_r2=float(cut_radius) * float(cut_radius),
             idx_dtype=torch.int32 if return_distances else torch.int64,
-            config=self.config, validate=validate)
+            config=self.config, validate=validate, candidate_stats=stats)
         if traverse_info is not None:
-            traverse_info[0] = float("nan")
+            total, cells = stats[0]
+            mean = total / cells if cells else float("nan")
+            traverse_info[0] = float(np.float32(mean))
         self._record("query", t0, {"memory_mode": memory_mode, "sorting_mode": sorting_mode})
         return (idx, dist) if return_distances else idx
 

@@ -75,6 +75,14 @@ FKNN_API int fknn_last_cuda_error(void);
 /* Copies the workspace's device status word to *status (synchronises
  * `stream`).  0 means no device-side problem was seen. */
 FKNN_API int fknn_read_status(const void* workspace, int* status, void* stream);
+/* Candidate statistics of the last fused self or general query that used
+ * `workspace` (fknn_knn_grid / fknn_knn_offsets / fknn_ball_query):
+ * *total = the sum over query groups (parent cells) of the number of points
+ * in their 27-cell neighbourhoods, *groups = the number of groups.  The
+ * reference's FlashKNN.query reports total / groups as traverse_info[0]
+ * (FlashKNN/functions/FlashKnnWrapper.py:351-352).  Synchronises `stream`. */
+FKNN_API int fknn_read_candidate_stats(const void* workspace, int64_t* total, int64_t* groups,
+                                       void* stream);
 /* Number of kernels the last successful fused call launched. */
 FKNN_API int fknn_last_launch_count(void);
 /* Kernel timing for benchmarks (no reference counterpart).  With slots > 0
@@ -243,11 +251,19 @@ FKNN_API int fknn_query_tables(const float* xyz_sorted, int64_t n, const int32_t
  * each; larger problems return FKNN_ERR_SCRATCH_LIMIT.  All calls on a device
  * share that array: calls that overlap on the GPU race, so order them on one
  * stream.  The first call on a device looks up the array's address with that
- * device current; make it before any stream capture. */
+ * device current; make it before any stream capture.  The address is kept
+ * until exit: calls after a device reset are not supported.  Device-side
+ * problems are reported by fknn_query_tables_noalloc_read_status. */
 FKNN_API int fknn_query_tables_noalloc(const float* xyz_sorted, int64_t n, const int32_t* steps,
                                        const int32_t* neigh, const int32_t* cnt, int64_t p,
                                        int32_t k, float cut_r2, int32_t* idx_out,
                                        float* dist_out, void* stream);
+/* No counterpart in the reference.  The device status word of the last
+ * fknn_query_tables_noalloc call on the current device (the FKNN_DEVICE_*
+ * bits that fknn_read_status reports for a workspace; each call clears it
+ * first), copied to *status after `stream` is synchronised.  Order it after
+ * that call on the same stream.  Allocates nothing. */
+FKNN_API int fknn_query_tables_noalloc_read_status(int* status, void* stream);
 
 /* Replaces FlashKNN_Selected_Query_DL (FlashKNN/csrc/flash_knn_query.h:206-218):
  * qindex int32 [m] (sorted support index of each query, grouped by parent

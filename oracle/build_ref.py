@@ -1,7 +1,8 @@
 """Compile the reference's own CUDA kernels for sm_100a into oracle/_ref/.
 
 TEST INFRASTRUCTURE ONLY.  Run it in a container that has the reference
-checkout (default /root/reference, override with FKNN_REFERENCE); the built
+checkout (``reference_root()``: $FKNN_REFERENCE, else the build container's
+mount point of the checkout); the built
 module (oracle/_ref/fknn_ref_cufun*.so) is git-ignored and travels to the
 GPU machine with the working tree.  It compiles the reference sources where
 they lie -- FlashKNN/csrc/flash_knn_query_dynamic_load.cu (production SMPS
@@ -27,10 +28,19 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "_ref")
 NAME = "fknn_ref_cufun"
+# where the build container mounts the reference checkout (read-only)
+REFERENCE_MOUNT = "/root/reference"
+
+
+def reference_root() -> str:
+    """The reference checkout every recipe that reads the reference's
+    sources uses: $FKNN_REFERENCE when set, else the build container's
+    mount point.  The GPU machine has neither; nothing there calls this."""
+    return os.environ.get("FKNN_REFERENCE") or REFERENCE_MOUNT
 
 
 def build(reference: str | None = None, verbose: bool = False) -> str:
-    reference = reference or os.environ.get("FKNN_REFERENCE", "/root/reference")
+    reference = reference or reference_root()
     csrc = os.path.join(reference, "FlashKNN", "csrc")
     if not os.path.isdir(csrc):
         raise FileNotFoundError(f"reference sources not found under {csrc}")
@@ -54,7 +64,7 @@ def build(reference: str | None = None, verbose: bool = False) -> str:
 
 
 def build_nanoflann(reference: str | None = None) -> str:
-    reference = reference or os.environ.get("FKNN_REFERENCE", "/root/reference")
+    reference = reference or reference_root()
     inc = os.path.join(reference, "Query", "ThirdParty", "nanoflannkdtree", "csrcs")
     if not os.path.isfile(os.path.join(inc, "nanoflann.hpp")):
         raise FileNotFoundError(f"nanoflann.hpp not found under {inc}")

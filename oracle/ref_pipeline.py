@@ -19,6 +19,21 @@ import torch.nn.functional as F
 def reference_query(cufun, grid_coord, batch_idx, xyz, k, num_down=2, cut_radius=math.inf):
     """Returns (int64 [N,K] original indices, f32 [N,K] distances in sorted
     order remapped like the indices)."""
+    t = reference_tables(cufun, grid_coord, batch_idx, xyz, num_down)
+    out_indices = torch.zeros((len(grid_coord), k), device=grid_coord.device, dtype=torch.int32)
+    out_dis = torch.zeros((len(grid_coord), k), device=grid_coord.device, dtype=torch.float32)
+    cufun.FlashKNN_Query_Dynamic_Load(t["xyz_sorted"], t["steps"], t["neigh"], t["cnt"], k,
+                                      out_indices, out_dis, 1, cut_radius * cut_radius)
+    order, inverse_order = t["order"], t["inverse_order"]
+    out = order[out_indices.long()[inverse_order]]
+    torch.cuda.synchronize()
+    return out, out_dis[inverse_order]
+
+
+def reference_tables(cufun, grid_coord, batch_idx, xyz, num_down=2):
+    """The tables FlashKNN.query hands its kernel (FlashKnnWrapper.py:220-365):
+    xyz_sorted f32 [N,3], steps / neigh / cnt int32, plus order and
+    inverse_order (int64) for the remap."""
     device = grid_coord.device
     key = cufun.FlashKNN_Morton_Encode(grid_coord.contiguous(), batch_idx.contiguous())
     order = torch.argsort(key)
@@ -39,14 +54,9 @@ def reference_query(cufun, grid_coord, batch_idx, xyz, k, num_down=2, cut_radius
     present = (positions < len(parent_keys)) & (parent_keys[safe_positions] == key_down_nbr)
     neigh = torch.where(present, safe_positions, -1).reshape(-1, 27)
     cnt_in_neigh = F.pad(torch.cumsum(F.pad(count, (0, 1))[neigh], dim=1), [1, 0])
-    out_indices = torch.zeros((len(grid_coord), k), device=device, dtype=torch.int32)
-    out_dis = torch.zeros((len(grid_coord), k), device=device, dtype=torch.float32)
     xyz_sorted = xyz[order].float().contiguous()
-    cufun.FlashKNN_Query_Dynamic_Load(xyz_sorted, steps.int(), neigh.int(), cnt_in_neigh.int(), k,
-                                      out_indices, out_dis, 1, cut_radius * cut_radius)
-    out = order[out_indices.long()[inverse_order]]
-    torch.cuda.synchronize()
-    return out, out_dis[inverse_order]
+    return {"xyz_sorted": xyz_sorted, "steps": steps.int(), "neigh": neigh.int(),
+            "cnt": cnt_in_neigh.int(), "order": order, "inverse_order": inverse_order}
 
 
 def reference_back_query(cufun, xyz, sel_indices, query_grid_size, batch_idx, k):

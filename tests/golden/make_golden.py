@@ -1,7 +1,7 @@
 """Generate the golden fixtures in this directory from the reference's own code.
 
-Run this in a container that has the reference checkout (default
-``/root/reference``; override with ``FKNN_REFERENCE``).  It never runs on a
+Run this in a container that has the reference checkout (``oracle.build_ref.reference_root()``:
+``FKNN_REFERENCE``, else the build container's mount point).  It never runs on a
 GPU machine and the tests only read its outputs (``*.npz``).
 
 How the fixtures are made
@@ -19,9 +19,10 @@ How the fixtures are made
   (sorted xyz, steps, neigh, cnt, query index, query steps), so the fixture
   holds exactly what the reference kernel would receive.
 
-The kNN outputs of the reference kernel itself on these tables are produced
-on a GPU machine by ``tests/golden/make_golden_gpu.py`` from the reference
-kernel compiled for sm_100a (``oracle/build_ref.py``).
+The reference kernel itself runs on these tables on the GPU in
+``tests/test_gpu_parity.py`` (``test_reference_kernel_agrees_with_oracle``),
+compiled for sm_100a by ``oracle/build_ref.py``; nothing kernel-made is
+stored here.
 """
 from __future__ import annotations
 
@@ -34,7 +35,10 @@ import numpy as np
 import torch
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = os.environ.get("FKNN_REFERENCE", "/root/reference")
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+from oracle import build_ref  # noqa: E402
+
+REF = build_ref.reference_root()
 SEED = 47
 
 CASES = {

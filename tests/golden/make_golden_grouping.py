@@ -2,8 +2,8 @@
 ``pointops.grouping`` (``Pointcept/libs/pointops/functions/grouping.py:36-60``)
 as shipped in the reference tree, on CPU tensors.
 
-Run this in a container that has the reference checkout (default
-``/root/reference``; override with ``FKNN_REFERENCE``).  The tests only read
+Run this in a container that has the reference checkout (``oracle.build_ref.reference_root()``:
+``FKNN_REFERENCE``, else the build container's mount point).  The tests only read
 its outputs (``grouping_<case>.npz``).
 
 ``grouping`` is plain torch indexing; only the module's import of the
@@ -22,7 +22,10 @@ import numpy as np
 import torch
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = os.environ.get("FKNN_REFERENCE", "/root/reference")
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+from oracle import build_ref  # noqa: E402
+
+REF = build_ref.reference_root()
 SEED = 47
 
 # name: (n, m, k, c, with_xyz, separate queries)

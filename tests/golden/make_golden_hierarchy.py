@@ -1,8 +1,8 @@
 """Golden fixtures of voxel-first subsampling and the DeLA hierarchy builder,
 made by the reference's own ``Networks/hierarchy.py`` on CPU tensors.
 
-Run this in a container that has the reference checkout (default
-``/root/reference``; override with ``FKNN_REFERENCE``) after building the
+Run this in a container that has the reference checkout (``oracle.build_ref.reference_root()``:
+``FKNN_REFERENCE``, else the build container's mount point) after building the
 oracle (``make -C oracle``).  The tests only read its outputs
 (``hierarchy_<case>.npz``).
 

@@ -53,3 +53,20 @@ def test_host_query_with_empty_clouds(fk, chunks):
     di, dd = fk.ops.knn_offsets(xyz.cuda(), off.cuda(), 8, 0.02, 2)
     assert torch.equal(idx, di.cpu())
     assert torch.equal(dist.view(torch.int32), dd.cpu().view(torch.int32))
+
+
+@pytest.mark.parametrize("case", ["uniform_k16", "dense_multibatch_k64", "duplicate_voxels_k32"])
+def test_traverse_info_is_the_mean_candidate_count(fk, case):
+    """FlashKNN.query(traverse_info=...) writes the mean over parent cells of
+    the points in their 27 neighbour cells, as the reference computes it from
+    its tables (cnt_in_neigh[:, -1].float().mean(), FlashKnnWrapper.py:351-352)."""
+    import os
+
+    from tests.conftest import GOLDEN
+    z = np.load(os.path.join(GOLDEN, f"tables_{case}.npz"))
+    want = np.float32(z["ref_cnt"][:, 27].astype(np.float64).mean())
+    info = [None]
+    f = fk.FlashKNN(num_nbr=int(z["k"]), num_down=int(z["num_down"]))
+    f.query(torch.from_numpy(z["grid"]).cuda(), torch.from_numpy(z["batch"]).cuda(),
+            torch.from_numpy(z["xyz"]).cuda(), traverse_info=info)
+    assert info[0] == pytest.approx(float(want), rel=1e-6)

@@ -255,11 +255,12 @@ def test_general_queries_outside_support(fk):
     assert (oi == -1).any()  # some far queries see no candidates
 
 
-def test_c4_batched_full_size_properties_and_sampled_rows(fk):
+@pytest.mark.parametrize("k", [16, 32])
+def test_c4_batched_full_size_properties_and_sampled_rows(fk, k):
     from flashknn_exprepo_b200 import synthetic as S
     b = S.uneven_batch()
     n = len(b.xyz)
-    gi, gd = fk.ops.knn_offsets(T(b.xyz), T(b.offsets), 16, S.C4_VOXEL, 2, validate=True)
+    gi, gd = fk.ops.knn_offsets(T(b.xyz), T(b.offsets), k, S.C4_VOXEL, 2, validate=True)
     gi, gd = H(gi), H(gd)
     # size-independent properties
     assert np.all(gd[:, 1:] >= gd[:, :-1])           # ascending (+inf padding last)
@@ -275,7 +276,7 @@ def test_c4_batched_full_size_properties_and_sampled_rows(fk):
     rows = np.sort(rng.choice(n, 20000, replace=False))
     # knn_offsets voxelises as floor(x * (1 / voxel)) in FP32
     grid = np.floor(b.xyz * (np.float32(1) / np.float32(S.C4_VOXEL))).astype(np.int64)
-    oi, od = O.knn_general(b.xyz, grid, cloud, b.xyz[rows], grid[rows], cloud[rows], 2, 16,
+    oi, od = O.knn_general(b.xyz, grid, cloud, b.xyz[rows], grid[rows], cloud[rows], 2, k,
                            pad=rows)
     assert np.array_equal(gi[rows], oi)
     assert np.array_equal(gd[rows].view(np.uint32), od.view(np.uint32))
