@@ -325,6 +325,7 @@ def run_ours(args, rank, world, local_rank, dist):
            "launch_shape": None if cfg is None else {
                "warps_per_cta": cfg.warps_per_cta, "tile_records": cfg.tile_records,
                "min_candidates_per_lane": cfg.min_candidates_per_lane,
+               "staging_depth": cfg.staging_depth,
                "tuned": next(iter(tuned.values()), None)}}
     del graph
 

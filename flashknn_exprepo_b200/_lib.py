@@ -28,6 +28,7 @@ DEVICE_BAD_TABLE = 2
 DEVICE_TIMEOUT = 4
 DEVICE_BATCH_RANGE = 8
 DEVICE_NO_CANDIDATES = 16  # informational: general / back queries pad such rows
+DEVICE_COPY_IN_FLIGHT = 32
 
 QUERY_SELF = 0
 QUERY_SELECTED = 1
@@ -39,6 +40,7 @@ _STATUS_TEXT = {
     DEVICE_TIMEOUT: "a bounded wait on a shared-memory bulk copy gave up",
     DEVICE_BATCH_RANGE: "a batch id lies outside [0, number of clouds)",
     DEVICE_NO_CANDIDATES: "a query has no candidate in its 27-cell neighbourhood",
+    DEVICE_COPY_IN_FLIGHT: "a warp stopped while its bulk copies may still have been in flight",
 }
 
 
@@ -48,11 +50,12 @@ class FknnError(RuntimeError):
 
 class FknnConfig(ctypes.Structure):
     _fields_ = [("warps_per_cta", ctypes.c_int32), ("tile_records", ctypes.c_int32),
-                ("min_candidates_per_lane", ctypes.c_int32), ("ctas_per_sm", ctypes.c_int32)]
+                ("min_candidates_per_lane", ctypes.c_int32), ("ctas_per_sm", ctypes.c_int32),
+                ("staging_depth", ctypes.c_int32)]
 
     def as_tuple(self):
         return (self.warps_per_cta, self.tile_records, self.min_candidates_per_lane,
-                self.ctas_per_sm)
+                self.ctas_per_sm, self.staging_depth)
 
 
 _P = ctypes.c_void_p

@@ -1,10 +1,13 @@
 """Autotuner of the query kernel's launch shape.
 
-The top-K kernel has three shape knobs (``fknn_config``): warps per CTA
+The top-K kernel has four shape knobs (``fknn_config``): warps per CTA
 (queries per CTA, 32 per warp), the candidate tile staged in shared memory
 per warp (``tile_records``; groups with more candidates stream tile by
-tile), and how many lanes may share one query when a group is larger than a
-tile (``min_candidates_per_lane``).  The best shape depends on K (register
+tile), how many lanes may share one query when a group is larger than a
+tile (``min_candidates_per_lane``), and the shared-memory staging depth (1:
+a warp stages a work item's candidates and then scans them; 2: two tiles
+per warp, the next item's bulk copies in flight during the scan, at twice
+the tile memory, hence fewer resident warps).  The best shape depends on K (register
 list length, hence occupancy) and on point density (candidates per query,
 hence tile fill and the chunked path).  ``tune_offsets`` times a
 coarse-to-fine grid of shapes on the caller's own workload with CUDA events
@@ -26,7 +29,8 @@ from . import _lib, ops
 WARPS = (2, 4, 8)
 TILES = (256, 384, 448, 512, 640, 768, 1024)
 LANE_SHARES = (4, 8, 16)
-DEFAULT = (4, 448, 8, 0)
+DEPTHS = (1, 2)
+DEFAULT = (4, 448, 8, 0, 1)
 
 _cache: dict = {}
 _lock = threading.Lock()
@@ -100,9 +104,9 @@ def _time(fn, reps: int) -> float:
 def tune_offsets(xyz, offset, k, voxel, num_down=2, reps=3, force=False):
     """Fastest launch shape for this self-query workload (and its class).
 
-    Times every (warps, tile) pair with 8 lanes per query share, then the
-    lane shares for the best pair; returns the FknnConfig and records it for
-    (GPU, K bucket, density bucket).  Results are identical for every shape
+    Times every (warps, tile, depth) triple with 8 lanes per query share,
+    then the lane shares for the best triple; returns the FknnConfig and
+    records it for (GPU, K bucket, density bucket).  Results are identical for every shape
     (the shape changes the schedule, never the answer)."""
     dev = xyz.device
     density = density_bucket(xyz, offset, voxel, num_down)
@@ -123,12 +127,13 @@ def tune_offsets(xyz, offset, k, voxel, num_down=2, reps=3, force=False):
 
     for w in WARPS:
         for t in TILES:
-            ms = run((w, t, 8, 0))
-            if ms is not None:
-                times[(w, t, 8, 0)] = ms
+            for depth in DEPTHS:
+                ms = run((w, t, 8, 0, depth))
+                if ms is not None:
+                    times[(w, t, 8, 0, depth)] = ms
     best = min(times, key=times.get)
     for share in LANE_SHARES:
-        cfg = (best[0], best[1], share, 0)
+        cfg = (best[0], best[1], share, 0, best[4])
         if cfg not in times:
             ms = run(cfg)
             if ms is not None:

@@ -18,6 +18,7 @@ constexpr int kStatusTable = FKNN_DEVICE_BAD_TABLE;
 constexpr int kStatusTimeout = FKNN_DEVICE_TIMEOUT;
 constexpr int kStatusBatch = FKNN_DEVICE_BATCH_RANGE;
 constexpr int kStatusNoCandidates = FKNN_DEVICE_NO_CANDIDATES;
+constexpr int kStatusCopyInFlight = FKNN_DEVICE_COPY_IN_FLIGHT;
 
 __host__ __device__ inline int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
 

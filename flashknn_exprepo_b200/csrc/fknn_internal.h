@@ -44,6 +44,7 @@ struct QueryShape {
   int tile_records;
   int min_candidates_per_lane;
   int ctas_per_sm;
+  int staging_depth;  // 1: stage an item, then scan it; 2: stage the next during the scan
 };
 
 QueryShape resolve_shape(const fknn_config* cfg);

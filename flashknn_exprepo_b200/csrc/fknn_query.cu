@@ -55,10 +55,16 @@ struct GroupSlot {
 };
 static_assert(sizeof(GroupSlot) == 48, "GroupSlot layout");
 
-// Bytes of one warp's shared-memory region for a tile of T records.
-__host__ __device__ constexpr size_t warp_smem_bytes(int T) {
-  return ((static_cast<size_t>(T) * 20 + 16 + kMaxGroupsPerItem * sizeof(GroupSlot) +
-           kMaxGroupsPerItem * (kBuckets + 1) * 2 + 32 + kBuckets * 4 + 127) /
+// Staging buffers per warp (the autotuner's depth axis: 1 or 2).
+constexpr int kMaxStaging = 2;
+
+// Bytes of one warp's shared-memory region: `depth` staging buffers of T
+// records (tile, group slots, flag) and one set of sort scratch.
+__host__ __device__ constexpr size_t warp_smem_bytes(int T, int depth) {
+  return ((static_cast<size_t>(depth) *
+               (static_cast<size_t>(T) * 16 + kMaxGroupsPerItem * sizeof(GroupSlot) + 16) +
+           static_cast<size_t>(T) * 4 + kMaxGroupsPerItem * (kBuckets + 1) * 2 + 32 +
+           kBuckets * 4 + 127) /
           128) *
          128;
 }
@@ -345,8 +351,9 @@ constexpr int query_max_regs() {
 
 // A chunked item: one group with more candidates than a tile.  Out of line,
 // so its registers do not add to the packed path's.  Returns the mbarrier's
-// next phase, or -1 after a bounded wait gave up (status raised, the warp's
-// copies waited for).
+// next phase, or -1 after a bounded wait gave up (status raised; the warp
+// waited once more, bounded, for its copies, and raised kStatusCopyInFlight
+// if they still had not landed).
 template <int KCAP, bool EXACT, typename IdxT>
 __device__ __noinline__ int chunked_item(const QueryLaunch& a, int T, int min_cands_per_lane,
                                          int q0, int qn, int g0, int k, float4* tile,
@@ -464,9 +471,11 @@ __device__ __noinline__ int chunked_item(const QueryLaunch& a, int T, int min_ca
     rad2 = rad * rad * 1.00001f;
     scan_range(a_end, total, rad2 <= 3.0e38f);
   }
-  if (timed_out) {
+  if (timed_out) {  // no copy was issued after the wait that gave up
     if (lane == 0) raise_status(&a.meta->status, kStatusTimeout);
-    mbar_wait_bounded(bar, phase, kWaitLimit);  // let this warp's copies land
+    const bool landed = mbar_wait_bounded(bar, phase, kWaitLimit);  // let them land
+    if (!__all_sync(kFull, landed) && lane == 0)
+      raise_status(&a.meta->status, kStatusCopyInFlight);
     return -1;
   }
   for (int m = 1; m < G; m <<= 1) merge_with_lane<KCAP>(L, m);
@@ -474,250 +483,370 @@ __device__ __noinline__ int chunked_item(const QueryLaunch& a, int T, int min_ca
   return static_cast<int>(phase);
 }
 
-template <int KCAP, bool EXACT, typename IdxT>
-__global__ void __maxnreg__(query_max_regs<KCAP>())
-    k_query(const __grid_constant__ QueryLaunch a, int T, int min_cands_per_lane) {
-  extern __shared__ __align__(128) unsigned char smem_raw[];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw) + warp;
-  unsigned char* wb = smem_raw + 128 + static_cast<size_t>(warp) * warp_smem_bytes(T);
-  float4* tile = reinterpret_cast<float4*>(wb);
-  uint16_t* tmp16 = reinterpret_cast<uint16_t*>(wb + static_cast<size_t>(T) * 16);
-  uint16_t* srt16 = tmp16 + T;
-  GroupSlot* slots =
-      reinterpret_cast<GroupSlot*>(wb + ((static_cast<size_t>(T) * 20 + 15) & ~size_t{15}));
-  uint16_t* bstart = reinterpret_cast<uint16_t*>(slots + kMaxGroupsPerItem);
-  uint8_t* qgroup = reinterpret_cast<uint8_t*>(bstart + kMaxGroupsPerItem * (kBuckets + 1));
-  uint32_t* hist = reinterpret_cast<uint32_t*>(qgroup + 32);
-  Meta* meta = a.meta;
-  if (lane == 0) {
-    mbar_init(bar, 1);
-    mbar_init_fence();
+// Shared memory of one staging buffer of a warp: the candidate tile, the
+// item's group slots and a flag word (1 = the item's groups overflowed the
+// tile, which only a malformed item can cause).
+__host__ __device__ constexpr size_t buffer_bytes(int T) {
+  return static_cast<size_t>(T) * 16 + kMaxGroupsPerItem * sizeof(GroupSlot) + 16;
+}
+
+// One warp's shared memory: `depth` staging buffers (at buf0 + b * stride)
+// and their mbarriers, then the sort scratch shared by the buffers.
+struct WarpSmem {
+  unsigned char* buf0;
+  size_t stride;
+  int T;
+  uint64_t* bars;
+  uint16_t* tmp16;
+  uint16_t* srt16;
+  uint16_t* bstart;
+  uint8_t* qgroup;
+  uint32_t* hist;
+  __device__ __forceinline__ float4* tile(int b) const {
+    return reinterpret_cast<float4*>(buf0 + b * stride);
+  }
+  __device__ __forceinline__ GroupSlot* slots(int b) const {
+    return reinterpret_cast<GroupSlot*>(buf0 + b * stride + static_cast<size_t>(T) * 16);
+  }
+  __device__ __forceinline__ int* flags(int b) const {
+    return reinterpret_cast<int*>(slots(b) + kMaxGroupsPerItem);
+  }
+  __device__ __forceinline__ uint64_t* bar(int b) const { return bars + b; }
+};
+
+__device__ __forceinline__ WarpSmem warp_smem(unsigned char* smem_raw, int T, int depth) {
+  const int warp = threadIdx.x >> 5;
+  WarpSmem w;
+  w.buf0 = smem_raw + 128 + static_cast<size_t>(warp) * warp_smem_bytes(T, depth);
+  w.stride = buffer_bytes(T);
+  w.T = T;
+  w.bars = reinterpret_cast<uint64_t*>(smem_raw) + warp * kMaxStaging;
+  w.tmp16 = reinterpret_cast<uint16_t*>(w.buf0 + static_cast<size_t>(depth) * buffer_bytes(T));
+  w.srt16 = w.tmp16 + T;
+  w.bstart = w.srt16 + T;
+  w.qgroup = reinterpret_cast<uint8_t*>(w.bstart + kMaxGroupsPerItem * (kBuckets + 1));
+  w.hist = reinterpret_cast<uint32_t*>(w.qgroup + 32);
+  return w;
+}
+
+__device__ __forceinline__ int pop_item(Meta* meta) {
+  int item = 0;
+  if ((threadIdx.x & 31) == 0) item = atomicAdd(&meta->queue_head, 1);
+  return __shfl_sync(kFull, item, 0);
+}
+
+// Checks item `item` and, for a packed item, issues the bulk copies of its
+// groups' candidate runs into buffer b (completing on the buffer's
+// mbarrier) and records the groups in the buffer's slots.  Returns 1 when
+// copies were armed (the caller waits on the buffer's barrier), 0 for a
+// chunked item (it streams its own tiles), -1 for a malformed item (status
+// raised, nothing to do).
+__device__ __forceinline__ int stage_item(const QueryLaunch& a, int item, int n_groups, int T,
+                                          const WarpSmem& w, int b) {
+  const int lane = threadIdx.x & 31;
+  const int4 it = a.items[item];
+  const int q0 = it.x, qn = it.y, g0 = it.z, gn = it.w & 0xffff;
+  const bool chunked = (it.w & kItemChunked) != 0;
+  if (q0 < 0 || qn < 1 || qn > 32 || static_cast<int64_t>(q0) + qn > a.n_qrec || g0 < 0 ||
+      gn < 1 || gn > kMaxGroupsPerItem || g0 + gn > n_groups || (chunked && gn != 1)) {
+    if (lane == 0) raise_status(&a.meta->status, kStatusTable);
+    return -1;
+  }
+  if (chunked) return 0;
+  int ga = 0, gb = 0, grow = 0;
+  if (lane < gn) {
+    const int g = g0 + lane;
+    const int gs = a.group_start[g], ge = a.group_start[g + 1];
+    ga = max(gs, q0);
+    gb = max(ga, min(ge, q0 + qn));
+    grow = a.group_row ? a.group_row[g] : g;
   }
   __syncwarp();
-  uint32_t phase = 0;
-  const int n_items = meta->n_items;
-  const int n_groups = *a.group_count_ptr;
+  fence_proxy_async_smem();  // earlier generic accesses of the tile precede the copies
+  __syncwarp();
+  float4* tile = w.tile(b);
+  uint64_t* bar = w.bar(b);
+  int seg = 0;
+  bool overflow = false;
+  for (int gi = 0; gi < gn; ++gi) {
+    const int ga_ = __shfl_sync(kFull, ga, gi), gb_ = __shfl_sync(kFull, gb, gi);
+    const int row = __shfl_sync(kFull, grow, gi);
+    int len = 0;
+    if (gb_ > ga_ && !overflow) {
+      const int2 run = load_run(a, row, lane);
+      const int incl = warp_inclusive_scan(run.y);
+      len = __shfl_sync(kFull, incl, 31);
+      if (seg + len > T) {
+        overflow = true;
+        len = 0;
+      } else if (len > 0) {
+        if (lane == 0) mbar_expect_tx(bar, static_cast<uint32_t>(len) * 16u);
+        __syncwarp();
+        if (run.y > 0)
+          bulk_copy_g2s(tile + seg + (incl - run.y), a.srec + run.x,
+                        static_cast<uint32_t>(run.y) * 16u, bar);
+      }
+    }
+    if (lane == 0) {
+      GroupSlot s{};
+      s.seg = seg;
+      s.len = len;
+      s.a = ga_;
+      s.b = overflow ? ga_ : gb_;
+      w.slots(b)[gi] = s;
+    }
+    seg += len;
+  }
+  if (lane == 0) {
+    *w.flags(b) = overflow ? 1 : 0;
+    mbar_arrive(bar);
+  }
+  return 1;
+}
+
+// A packed item whose copies into buffer b have landed: up to 32 queries of
+// up to 16 groups, one query per lane (see the file comment).
+template <int KCAP, bool EXACT, typename IdxT>
+__device__ __forceinline__ void packed_item(const QueryLaunch& a, int item, const WarpSmem& w,
+                                            int b) {
+  const int lane = threadIdx.x & 31;
+  Meta* meta = a.meta;
+  const int4 it = a.items[item];
+  const int q0 = it.x, qn = it.y, gn = it.w & 0xffff;
+  const float4* tile = w.tile(b);
+  GroupSlot* slots = w.slots(b);
+  uint16_t* tmp16 = w.tmp16;
+  uint16_t* srt16 = w.srt16;
+  uint16_t* bstart = w.bstart;
+  uint8_t* qgroup = w.qgroup;
+  uint32_t* hist = w.hist;
   const int k = a.k;
+  if (*w.flags(b)) {  // the packer bounds every item by the tile; report a broken item
+    if (lane == 0) raise_status(&meta->status, kStatusTable);
+    return;
+  }
+  // query -> group map (0xff: a query no group of the item covers)
+  qgroup[lane] = 0xffu;
+  __syncwarp();
+  if (lane < gn) {
+    const GroupSlot s = slots[lane];
+    for (int p = s.a; p < s.b; ++p) qgroup[p - q0] = static_cast<uint8_t>(lane);
+  }
+  __syncwarp();
 
-  for (;;) {
-    int item = 0;
-    if (lane == 0) item = atomicAdd(&meta->queue_head, 1);
-    item = __shfl_sync(kFull, item, 0);
-    if (item >= n_items) break;
-    const int4 it = a.items[item];
-    const int q0 = it.x, qn = it.y, g0 = it.z, gn = it.w & 0xffff;
-    const bool chunked = (it.w & kItemChunked) != 0;
-    if (q0 < 0 || qn < 1 || qn > 32 || static_cast<int64_t>(q0) + qn > a.n_qrec || g0 < 0 ||
-        gn < 1 || gn > kMaxGroupsPerItem || g0 + gn > n_groups || (chunked && gn != 1)) {
-      if (lane == 0) raise_status(&meta->status, kStatusTable);
-      continue;
-    }
-
-    if (chunked) {
-      const int next = chunked_item<KCAP, EXACT, IdxT>(a, T, min_cands_per_lane, q0, qn, g0, k,
-                                                       tile, srt16, hist, bar, phase);
-      if (next < 0) return;
-      phase = static_cast<uint32_t>(next);
-      continue;
-    }
-
-    // -------------------------------------------------- packed item
-    int ga = 0, gb = 0, grow = 0;
-    if (lane < gn) {
-      const int g = g0 + lane;
-      const int gs = a.group_start[g], ge = a.group_start[g + 1];
-      ga = max(gs, q0);
-      gb = max(ga, min(ge, q0 + qn));
-      grow = a.group_row ? a.group_row[g] : g;
-    }
-    __syncwarp();
-    fence_proxy_async_smem();  // earlier generic accesses of the tile precede the copies
-    __syncwarp();
-    int seg = 0;
-    bool overflow = false;
-    for (int gi = 0; gi < gn; ++gi) {
-      const int ga_ = __shfl_sync(kFull, ga, gi), gb_ = __shfl_sync(kFull, gb, gi);
-      const int row = __shfl_sync(kFull, grow, gi);
-      int len = 0;
-      if (gb_ > ga_ && !overflow) {
-        const int2 run = load_run(a, row, lane);
-        const int incl = warp_inclusive_scan(run.y);
-        len = __shfl_sync(kFull, incl, 31);
-        if (seg + len > T) {
-          overflow = true;
-          len = 0;
-        } else if (len > 0) {
-          if (lane == 0) mbar_expect_tx(bar, static_cast<uint32_t>(len) * 16u);
-          __syncwarp();
-          if (run.y > 0)
-            bulk_copy_g2s(tile + seg + (incl - run.y), a.srec + run.x,
-                          static_cast<uint32_t>(run.y) * 16u, bar);
-        }
-      }
-      if (lane == 0) {
-        GroupSlot s{};
-        s.seg = seg;
-        s.len = len;
-        s.a = ga_;
-        s.b = overflow ? ga_ : gb_;
-        slots[gi] = s;
-      }
-      seg += len;
-    }
-    if (lane == 0) mbar_arrive(bar);
-    if (!mbar_wait_bounded(bar, phase, kWaitLimit)) {
-      if (lane == 0) raise_status(&meta->status, kStatusTimeout);
-      mbar_wait_bounded(bar, phase, kWaitLimit);
-      return;
-    }
-    phase ^= 1u;
-    if (overflow) {  // the packer bounds every item by the tile; report a broken item
-      if (lane == 0) raise_status(&meta->status, kStatusTable);
-      continue;
-    }
-    // query -> group map (0xff: a query no group of the item covers)
-    qgroup[lane] = 0xffu;
-    __syncwarp();
-    if (lane < gn)
-      for (int p = ga; p < gb; ++p) qgroup[p - q0] = static_cast<uint8_t>(lane);
-    __syncwarp();
-
-    // Per group: centroid of its queries, distance buckets, counting sort.
-    for (int gi = 0; gi < gn; ++gi) {
-      const GroupSlot s = slots[gi];
-      if (s.b <= s.a) continue;
-      const int nq = s.b - s.a;
-      float4 qv = make_float4(0.f, 0.f, 0.f, 0.f);
-      if (lane < nq) qv = a.qrec[s.a + lane];
-      const float inv_nq = 1.f / static_cast<float>(nq);
-      const float cx = warp_sum(qv.x) * inv_nq;
-      const float cy = warp_sum(qv.y) * inv_nq;
-      const float cz = warp_sum(qv.z) * inv_nq;
-      float d2max = 0.f;
-      for (int t = lane; t < s.len; t += 32) {
-        const float4 c = tile[s.seg + t];
-        const float dx = c.x - cx, dy = c.y - cy, dz = c.z - cz;
-        d2max = fmaxf(d2max, dx * dx + dy * dy + dz * dz);
-      }
-      d2max = warp_max(d2max);
-      const float w2 = d2max > 0.f ? d2max * (1.0f / kBuckets) * 1.0001f : 1.f;
-      const float inv_w2 = 1.f / w2;
-      hist[lane] = 0u;  // kBuckets == 32: one bucket per lane
-      __syncwarp();
-      // Bucket of every candidate and its rank inside the bucket.
-      for (int t = lane; t < s.len; t += 32) {
-        const float4 c = tile[s.seg + t];
-        const float dx = c.x - cx, dy = c.y - cy, dz = c.z - cz;
-        const int bkt = min(static_cast<int>((dx * dx + dy * dy + dz * dz) * inv_w2), kBuckets - 1);
-        const uint32_t r = atomicAdd(&hist[bkt], 1u);
-        tmp16[s.seg + t] = static_cast<uint16_t>((bkt << 10) | r);
-      }
-      __syncwarp();
-      const uint32_t h = hist[lane];
-      const uint32_t hi = static_cast<uint32_t>(warp_inclusive_scan(static_cast<int>(h)));
-      uint16_t* bs = bstart + gi * (kBuckets + 1);
-      bs[lane] = static_cast<uint16_t>(hi - h);
-      if (lane == 31) bs[kBuckets] = static_cast<uint16_t>(hi);
-      __syncwarp();
-      hist[lane] = hi - h;
-      __syncwarp();
-      for (int t = lane; t < s.len; t += 32) {
-        const uint16_t v = tmp16[s.seg + t];
-        const int bkt = v >> 10;
-        srt16[s.seg + hist[bkt] + (v & 1023)] = static_cast<uint16_t>(s.seg + t);
-      }
-      if (lane == 0) {
-        const float mag = fmaxf(fabsf(cx), fmaxf(fabsf(cy), fabsf(cz))) + sqrtf(d2max);
-        slots[gi].cx = cx;
-        slots[gi].cy = cy;
-        slots[gi].cz = cz;
-        slots[gi].inv_w2 = inv_w2;
-        slots[gi].eps = mag * 4e-6f + 1e-30f;
-      }
-      __syncwarp();
-    }
-
-    // One query per lane.
-    const int mapped = lane < qn ? qgroup[lane] : 0;
-    if (lane < qn && mapped >= gn) raise_status(&meta->status, kStatusTable);
-    const bool active = lane < qn && mapped < gn;
-    const int gi = active ? mapped : 0;
+  // Per group: centroid of its queries, distance buckets, counting sort.
+  for (int gi = 0; gi < gn; ++gi) {
     const GroupSlot s = slots[gi];
-    const uint16_t* bs = bstart + gi * (kBuckets + 1);
-    float4 q = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (active) q = a.qrec[q0 + lane];
-    const float rdx = q.x - s.cx, rdy = q.y - s.cy, rdz = q.z - s.cz;
-    const float rq = sqrtf(rdx * rdx + rdy * rdy + rdz * rdz);
-    const int len = active && cut_accepts_any(a.cut_r2) ? s.len : 0;
-    const uint32_t cut_lim = cut_limit(a.cut_r2);
-
-    uint64_t L[KCAP];
-#pragma unroll
-    for (int j = 0; j < KCAP; ++j) {
-      uint64_t key = kEmpty;
-      if (j < len) {
-        const float4 c = tile[srt16[s.seg + j]];
-        const float d = sq_dist(c.x, c.y, c.z, q.x, q.y, q.z);
-        if (__float_as_uint(d) <= cut_lim) key = make_key(d, c.w);
-      }
-      L[j] = key;
+    if (s.b <= s.a) continue;
+    const int nq = s.b - s.a;
+    float4 qv = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (lane < nq) qv = a.qrec[s.a + lane];
+    const float inv_nq = 1.f / static_cast<float>(nq);
+    const float cx = warp_sum(qv.x) * inv_nq;
+    const float cy = warp_sum(qv.y) * inv_nq;
+    const float cz = warp_sum(qv.z) * inv_nq;
+    float d2max = 0.f;
+    for (int t = lane; t < s.len; t += 32) {
+      const float4 c = tile[s.seg + t];
+      const float dx = c.x - cx, dy = c.y - cy, dz = c.z - cz;
+      d2max = fmaxf(d2max, dx * dx + dy * dy + dz * dz);
     }
-    sort_network<KCAP, 0, KCAP>(L);
-    uint32_t thr = kth_limit(L[KCAP - 1], cut_lim);
-    int stop = len > 0 ? stop_position<KCAP>(L, s, rq, bs) : 0;
-    // Candidate t of the lane's scan: accepted when it beats the K-th.
-    auto test = [&](int t, uint64_t& x) {
-      const float4 c = tile[srt16[s.seg + t]];
+    d2max = warp_max(d2max);
+    const float w2 = d2max > 0.f ? d2max * (1.0f / kBuckets) * 1.0001f : 1.f;
+    const float inv_w2 = 1.f / w2;
+    hist[lane] = 0u;  // kBuckets == 32: one bucket per lane
+    __syncwarp();
+    // Bucket of every candidate and its rank inside the bucket.
+    for (int t = lane; t < s.len; t += 32) {
+      const float4 c = tile[s.seg + t];
+      const float dx = c.x - cx, dy = c.y - cy, dz = c.z - cz;
+      const int bkt = min(static_cast<int>((dx * dx + dy * dy + dz * dz) * inv_w2), kBuckets - 1);
+      const uint32_t r = atomicAdd(&hist[bkt], 1u);
+      tmp16[s.seg + t] = static_cast<uint16_t>((bkt << 10) | r);
+    }
+    __syncwarp();
+    const uint32_t h = hist[lane];
+    const uint32_t hi = static_cast<uint32_t>(warp_inclusive_scan(static_cast<int>(h)));
+    uint16_t* bs = bstart + gi * (kBuckets + 1);
+    bs[lane] = static_cast<uint16_t>(hi - h);
+    if (lane == 31) bs[kBuckets] = static_cast<uint16_t>(hi);
+    __syncwarp();
+    hist[lane] = hi - h;
+    __syncwarp();
+    for (int t = lane; t < s.len; t += 32) {
+      const uint16_t v = tmp16[s.seg + t];
+      const int bkt = v >> 10;
+      srt16[s.seg + hist[bkt] + (v & 1023)] = static_cast<uint16_t>(s.seg + t);
+    }
+    if (lane == 0) {
+      const float mag = fmaxf(fabsf(cx), fmaxf(fabsf(cy), fabsf(cz))) + sqrtf(d2max);
+      slots[gi].cx = cx;
+      slots[gi].cy = cy;
+      slots[gi].cz = cz;
+      slots[gi].inv_w2 = inv_w2;
+      slots[gi].eps = mag * 4e-6f + 1e-30f;
+    }
+    __syncwarp();
+  }
+
+  // One query per lane.
+  const int mapped = lane < qn ? qgroup[lane] : 0;
+  if (lane < qn && mapped >= gn) raise_status(&meta->status, kStatusTable);
+  const bool active = lane < qn && mapped < gn;
+  const int gi = active ? mapped : 0;
+  const GroupSlot s = slots[gi];
+  const uint16_t* bs = bstart + gi * (kBuckets + 1);
+  float4 q = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (active) q = a.qrec[q0 + lane];
+  const float rdx = q.x - s.cx, rdy = q.y - s.cy, rdz = q.z - s.cz;
+  const float rq = sqrtf(rdx * rdx + rdy * rdy + rdz * rdz);
+  const int len = active && cut_accepts_any(a.cut_r2) ? s.len : 0;
+  const uint32_t cut_lim = cut_limit(a.cut_r2);
+
+  uint64_t L[KCAP];
+#pragma unroll
+  for (int j = 0; j < KCAP; ++j) {
+    uint64_t key = kEmpty;
+    if (j < len) {
+      const float4 c = tile[srt16[s.seg + j]];
       const float d = sq_dist(c.x, c.y, c.z, q.x, q.y, q.z);
-      const bool acc = __float_as_uint(d) <= thr;
-      if (acc) x = make_key(d, c.w);
-      return acc;
-    };
-    if constexpr (KCAP <= 16) {
-      // Two candidates per iteration, both tested against the same K-th
-      // distance: half the loop and vote overhead, and two independent loads
-      // and distance chains in flight.  (With a 32- or 64-entry list the
-      // extra registers cost more than this saves.)
-      for (int t = KCAP;; t += 2) {
-        const bool live0 = t < stop, live1 = t + 1 < stop;
-        if (!__any_sync(kFull, live0)) break;
-        uint64_t x0 = kEmpty, x1 = kEmpty;
-        const bool acc0 = live0 && test(t, x0);
-        const bool acc1 = live1 && test(t + 1, x1);
-        // A lane that took only its second candidate inserts it in the first
-        // step, so the second step runs only when some lane took both (the
-        // list keeps the K smallest of what it is given, in any order).
-        if (!acc0) {
-          x0 = x1;
-          x1 = kEmpty;
-        }
-        const bool any0 = __any_sync(kFull, acc0 || acc1);
-        const bool any1 = __any_sync(kFull, acc0 && acc1);
-        if (any0) insert_one<KCAP>(L, x0);
-        if (any1) insert_one<KCAP>(L, x1);
-        if (acc0 || acc1) {
+      if (__float_as_uint(d) <= cut_lim) key = make_key(d, c.w);
+    }
+    L[j] = key;
+  }
+  sort_network<KCAP, 0, KCAP>(L);
+  uint32_t thr = kth_limit(L[KCAP - 1], cut_lim);
+  int stop = len > 0 ? stop_position<KCAP>(L, s, rq, bs) : 0;
+  // Candidate t of the lane's scan: accepted when it beats the K-th.
+  auto test = [&](int t, uint64_t& x) {
+    const float4 c = tile[srt16[s.seg + t]];
+    const float d = sq_dist(c.x, c.y, c.z, q.x, q.y, q.z);
+    const bool acc = __float_as_uint(d) <= thr;
+    if (acc) x = make_key(d, c.w);
+    return acc;
+  };
+  if constexpr (KCAP <= 16) {
+    // Two candidates per iteration, both tested against the same K-th
+    // distance: half the loop and vote overhead, and two independent loads
+    // and distance chains in flight.  (With a 32- or 64-entry list the
+    // extra registers cost more than this saves.)
+    for (int t = KCAP;; t += 2) {
+      const bool live0 = t < stop, live1 = t + 1 < stop;
+      if (!__any_sync(kFull, live0)) break;
+      uint64_t x0 = kEmpty, x1 = kEmpty;
+      const bool acc0 = live0 && test(t, x0);
+      const bool acc1 = live1 && test(t + 1, x1);
+      // A lane that took only its second candidate inserts it in the first
+      // step, so the second step runs only when some lane took both (the
+      // list keeps the K smallest of what it is given, in any order).
+      if (!acc0) {
+        x0 = x1;
+        x1 = kEmpty;
+      }
+      const bool any0 = __any_sync(kFull, acc0 || acc1);
+      const bool any1 = __any_sync(kFull, acc0 && acc1);
+      if (any0) insert_one<KCAP>(L, x0);
+      if (any1) insert_one<KCAP>(L, x1);
+      if (acc0 || acc1) {
+        thr = kth_limit(L[KCAP - 1], cut_lim);
+        stop = min(stop, stop_position<KCAP>(L, s, rq, bs));
+      }
+    }
+  } else {
+    for (int t = KCAP;; ++t) {
+      const bool live = t < stop;
+      if (!__any_sync(kFull, live)) break;
+      uint64_t x = kEmpty;
+      const bool acc = live && test(t, x);
+      if (__any_sync(kFull, acc)) {
+        insert_one<KCAP>(L, x);
+        if (acc) {
           thr = kth_limit(L[KCAP - 1], cut_lim);
           stop = min(stop, stop_position<KCAP>(L, s, rq, bs));
         }
       }
-    } else {
-      for (int t = KCAP;; ++t) {
-        const bool live = t < stop;
-        if (!__any_sync(kFull, live)) break;
-        uint64_t x = kEmpty;
-        const bool acc = live && test(t, x);
-        if (__any_sync(kFull, acc)) {
-          insert_one<KCAP>(L, x);
-          if (acc) {
-            thr = kth_limit(L[KCAP - 1], cut_lim);
-            stop = min(stop, stop_position<KCAP>(L, s, rq, bs));
-          }
-        }
-      }
     }
-    if (active) write_row<IdxT, KCAP, EXACT>(a, L, __float_as_int(q.w), k);
-    __syncwarp();
+  }
+  if (active) write_row<IdxT, KCAP, EXACT>(a, L, __float_as_int(q.w), k);
+  __syncwarp();
+}
+
+// After a bounded wait gave up: waits once more (bounded) for every buffer
+// that still has bulk copies in flight, so the warp does not leave while the
+// copies write into its shared memory; if they still have not landed, says
+// so with kStatusCopyInFlight.  The warp then stops; the other warps of its
+// CTA (which keep the shared memory allocated) finish their own items.
+__device__ __noinline__ void drain_after_timeout(Meta* meta, const WarpSmem& w, uint32_t phase,
+                                                 uint32_t pending, int depth) {
+  const int lane = threadIdx.x & 31;
+  if (lane == 0) raise_status(&meta->status, kStatusTimeout);
+  bool landed = true;
+  for (int b = 0; b < depth; ++b)
+    if (((pending >> b) & 1u) && !mbar_wait_bounded(w.bar(b), (phase >> b) & 1u, kWaitLimit))
+      landed = false;
+  if (!__all_sync(kFull, landed) && lane == 0) raise_status(&meta->status, kStatusCopyInFlight);
+}
+
+// The persistent query kernel.  Each warp pulls items from the queue; with
+// `depth` 2 it stages the next item's candidate runs into its second buffer
+// before it scans the current one, so those copies are in flight while it
+// computes.
+template <int KCAP, bool EXACT, typename IdxT>
+__global__ void __maxnreg__(query_max_regs<KCAP>())
+    k_query(const __grid_constant__ QueryLaunch a, int T, int min_cands_per_lane, int depth) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  const int lane = threadIdx.x & 31;
+  const WarpSmem w = warp_smem(smem_raw, T, depth);
+  Meta* meta = a.meta;
+  if (lane == 0) {
+    for (int b = 0; b < depth; ++b) mbar_init(w.bar(b), 1);
+    mbar_init_fence();
+  }
+  __syncwarp();
+  // bit b: the parity to wait for on buffer b's barrier / copies armed there
+  uint32_t phase = 0u, pending = 0u;
+  const int n_items = meta->n_items;
+  const int n_groups = *a.group_count_ptr;
+
+  int buf = 0;
+  int item = pop_item(meta);
+  int staged = item < n_items ? stage_item(a, item, n_groups, T, w, buf) : -1;
+  if (staged == 1) pending |= 1u << buf;
+  while (item < n_items) {
+    int next = n_items, next_staged = -1;
+    if (depth > 1) {  // the next item's copies fly while this one is scanned
+      next = pop_item(meta);
+      if (next < n_items) next_staged = stage_item(a, next, n_groups, T, w, buf ^ 1);
+      if (next_staged == 1) pending |= 1u << (buf ^ 1);
+    }
+    if (staged == 1) {
+      if (!mbar_wait_bounded(w.bar(buf), (phase >> buf) & 1u, kWaitLimit)) {
+        drain_after_timeout(meta, w, phase, pending, depth);
+        return;
+      }
+      phase ^= 1u << buf;
+      pending &= ~(1u << buf);
+      packed_item<KCAP, EXACT, IdxT>(a, item, w, buf);
+    } else if (staged == 0) {
+      const int4 it = a.items[item];
+      const int nxt = chunked_item<KCAP, EXACT, IdxT>(a, T, min_cands_per_lane, it.x, it.y, it.z,
+                                                      a.k, w.tile(buf), w.srt16, w.hist,
+                                                      w.bar(buf), (phase >> buf) & 1u);
+      if (nxt < 0) {  // its own copies were waited for; the other buffer's may fly
+        drain_after_timeout(meta, w, phase, pending, depth);
+        return;
+      }
+      phase = (phase & ~(1u << buf)) | (static_cast<uint32_t>(nxt) << buf);
+    }
+    if (depth > 1) {
+      buf ^= 1;
+    } else {
+      next = pop_item(meta);
+      if (next < n_items) next_staged = stage_item(a, next, n_groups, T, w, buf);
+      if (next_staged == 1) pending |= 1u << buf;
+    }
+    item = next;
+    staged = next_staged;
   }
   __syncwarp();
 }
@@ -725,12 +854,13 @@ __global__ void __maxnreg__(query_max_regs<KCAP>())
 // ------------------------------------------------------------------ host
 
 QueryShape resolve_shape(const fknn_config* cfg) {
-  QueryShape s{4, 448, 8, 0};
+  QueryShape s{4, 448, 8, 0, 1};
   if (cfg) {
     if (cfg->warps_per_cta) s.warps_per_cta = cfg->warps_per_cta;
     if (cfg->tile_records) s.tile_records = cfg->tile_records;
     if (cfg->min_candidates_per_lane) s.min_candidates_per_lane = cfg->min_candidates_per_lane;
     s.ctas_per_sm = cfg->ctas_per_sm;
+    if (cfg->staging_depth) s.staging_depth = cfg->staging_depth;
   }
   return s;
 }
@@ -738,10 +868,12 @@ QueryShape resolve_shape(const fknn_config* cfg) {
 bool shape_valid(const QueryShape& s) {
   const bool warps_ok = s.warps_per_cta == 1 || s.warps_per_cta == 2 ||
                         s.warps_per_cta == 4 || s.warps_per_cta == 8;
-  return warps_ok && s.tile_records >= 64 && s.tile_records <= 1024 &&
+  const bool depth_ok = s.staging_depth >= 1 && s.staging_depth <= kMaxStaging;
+  return warps_ok && depth_ok && s.tile_records >= 64 && s.tile_records <= 1024 &&
          s.tile_records % 32 == 0 && s.min_candidates_per_lane >= 1 &&
          s.ctas_per_sm >= 0 && s.ctas_per_sm <= 32 &&
-         128 + static_cast<size_t>(s.warps_per_cta) * warp_smem_bytes(s.tile_records) <=
+         128 + static_cast<size_t>(s.warps_per_cta) *
+                   warp_smem_bytes(s.tile_records, s.staging_depth) <=
              227 * 1024;
 }
 
@@ -751,8 +883,8 @@ template <int KCAP, bool EXACT, typename IdxT>
 int launch_t(const QueryLaunch& q, const QueryShape& shape, cudaStream_t s) {
   auto kern = k_query<KCAP, EXACT, IdxT>;
   const int threads = shape.warps_per_cta * 32;
-  const size_t smem =
-      128 + static_cast<size_t>(shape.warps_per_cta) * warp_smem_bytes(shape.tile_records);
+  const size_t smem = 128 + static_cast<size_t>(shape.warps_per_cta) *
+                               warp_smem_bytes(shape.tile_records, shape.staging_depth);
   // Device properties and occupancy are resolved once per (device, shape) and
   // cached, so a launch inside a CUDA graph capture issues nothing but the
   // kernel itself.  The cache is shared by all host threads under a mutex,
@@ -805,7 +937,8 @@ int launch_t(const QueryLaunch& q, const QueryShape& shape, cudaStream_t s) {
   const int per_sm = shape.ctas_per_sm > 0 ? shape.ctas_per_sm : use.per_sm;
   const int grid = use.sms * per_sm;
   const int slot = profile_start(s);
-  kern<<<grid, threads, smem, s>>>(q, shape.tile_records, shape.min_candidates_per_lane);
+  kern<<<grid, threads, smem, s>>>(q, shape.tile_records, shape.min_candidates_per_lane,
+                                   shape.staging_depth);
   e = cudaGetLastError();
   profile_stop(slot, s);
   return e;

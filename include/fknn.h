@@ -53,18 +53,26 @@ extern "C" {
 #define FKNN_DEVICE_BATCH_RANGE 8 /* batch id outside [0, 2^15) */
 #define FKNN_DEVICE_NO_CANDIDATES 16 /* informational: a query saw no candidate
                                         (general / back queries pad it with -1) */
+#define FKNN_DEVICE_COPY_IN_FLIGHT 32 /* after FKNN_DEVICE_TIMEOUT, a second bounded
+                                         wait also gave up: a warp stopped while bulk
+                                         copies into its CTA's shared memory may still
+                                         have been in flight */
 
 /* Optional launch shape of the query kernel; NULL selects the defaults.
  * warps_per_cta in {1,2,4,8}; tile_records (candidate records staged per
  * warp) a multiple of 32 in [64, 1024] whose shared memory fits a CTA;
  * min_candidates_per_lane >= 1 caps how many lanes share one query;
- * ctas_per_sm 0 = occupancy maximum.  flashknn_exprepo_b200/autotune.py
- * picks these per K and point density by timing them. */
+ * ctas_per_sm 0 = occupancy maximum; staging_depth 1 (stage a work item's
+ * candidates, then scan them) or 2 (two tiles per warp: the next item's
+ * bulk copies are in flight while the current one is scanned).  Zero
+ * fields take the defaults.  flashknn_exprepo_b200/autotune.py picks these
+ * per K and point density by timing them. */
 typedef struct fknn_config {
   int32_t warps_per_cta;
   int32_t tile_records;
   int32_t min_candidates_per_lane;
   int32_t ctas_per_sm;
+  int32_t staging_depth;
 } fknn_config;
 
 /* ----------------------------------------------------------- utilities */

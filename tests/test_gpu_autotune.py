@@ -32,14 +32,15 @@ def test_every_shape_gives_identical_results(fk, k):
     for w in autotune.WARPS:
         for t in autotune.TILES[::2]:
             for share in autotune.LANE_SHARES:
-                try:
-                    got = fk.ops.knn_offsets(xyz, off, k, S.C4_VOXEL, 2,
-                                             config=_lib.FknnConfig(w, t, share, 0))
-                except _lib.FknnError:
-                    continue                      # shared memory beyond a CTA's
-                assert torch.equal(got[0], base[0]) and torch.equal(got[1], base[1])
-                seen += 1
-    assert seen >= 20
+                for depth in autotune.DEPTHS:
+                    try:
+                        got = fk.ops.knn_offsets(xyz, off, k, S.C4_VOXEL, 2,
+                                                 config=_lib.FknnConfig(w, t, share, 0, depth))
+                    except _lib.FknnError:
+                        continue                  # shared memory beyond a CTA's
+                    assert torch.equal(got[0], base[0]) and torch.equal(got[1], base[1])
+                    seen += 1
+    assert seen >= 40
 
 
 def test_tune_caches_and_reloads(fk, tmp_path, monkeypatch):
@@ -78,7 +79,7 @@ def test_concurrent_threads_with_different_shapes(fk):
     off = torch.from_numpy(b.offsets).to(DEV)
     base = fk.ops.knn_offsets(xyz, off, 16, S.C4_VOXEL, 2)
     torch.cuda.synchronize()
-    shapes = [(4, 448, 8, 0), (8, 1024, 8, 0), (2, 256, 4, 0), (4, 640, 16, 0)]
+    shapes = [(4, 448, 8, 0, 1), (8, 1024, 8, 0, 1), (2, 256, 4, 0, 2), (4, 640, 16, 0, 2)]
     errors = []
 
     def worker(shape):
