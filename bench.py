@@ -646,8 +646,13 @@ def rows_single_gpu(fk, torch, dev, flush, peak_gbs):
     cube = T(synthetic.uniform_cube())
     co = torch.tensor([cube.shape[0]], device=dev)
     ms = _event_ms(torch, lambda: fk.ops.knn_offsets(cube, co, 16, synthetic.C1_VOXEL, 2), flush)
+    gms = _event_ms(torch, lambda: fk.ops.knn_offsets(cube, co, 16, synthetic.C1_VOXEL, 2,
+                                                      graph=True), flush)
     rows["self_query_cube_k16"] = {"value": cube.shape[0] / (ms * 1e-3), "unit": "queries/s",
-                                   "ms": ms, "n_points": int(cube.shape[0])}
+                                   "ms": ms, "n_points": int(cube.shape[0]),
+                                   "graph_ms": gms,
+                                   "graph": "the same call with graph=True (a cached CUDA graph "
+                                            "of the pipeline replayed)"}
     # LiDAR scan (C3), K=16, alpha 4 and alpha 8 (num_down 2 and 3)
     lo_ = torch.tensor([lx.shape[0]], device=dev)
     for nd, alpha in ((2, 4), (3, 8)):

@@ -87,6 +87,8 @@ _SIGNATURES = {
     "fknn_query_tables_noalloc": (ctypes.c_int, [_P, _I64, _P, _P, _P, _I64, _I32, _F32, _P, _P,
                                                  _P]),
     "fknn_query_tables_noalloc_read_status": (ctypes.c_int, [_P, _P]),
+    "fknn_general_query_tables": (ctypes.c_int, [_P, _I64, _P, _I64, _P, _P, _P, _P, _P, _I64,
+                                                 _I32, _F32, _P, _P, _P, _SZ, _P, _P]),
     "fknn_selected_query_tables": (ctypes.c_int, [_P, _I64, _P, _I64, _P, _P, _P, _P, _I64, _I32,
                                                   _F32, _P, _P, _P, _SZ, _P, _P]),
     "fknn_morton_encode": (ctypes.c_int, [_P, _P, _I64, _P, _P]),

@@ -321,6 +321,29 @@ int fknn_knn_grid(const float* xyz, const int64_t* grid_coord, const int64_t* ba
   return finish(rc, launches);
 }
 
+int fknn_general_query_tables(const float* xyz_support, int64_t n, const float* xyz_query,
+                              int64_t m, const int32_t* pad_index, const int32_t* steps,
+                              const int32_t* steps_query, const int32_t* neigh,
+                              const int32_t* cnt, int64_t p, int32_t k, float cut_r2,
+                              int32_t* idx_out, float* dist_out, void* workspace,
+                              size_t workspace_bytes, const fknn_config* config, void* stream) {
+  int rc = check_k(k);
+  if (rc) return rc;
+  if (n < 0 || m < 0 || p < 0) return FKNN_ERR_ARG;
+  if (n > kMaxPoints || m > kMaxPoints || p > kMaxPoints / 28) return FKNN_ERR_SIZE;
+  if (!workspace || (n > 0 && !xyz_support) || (m > 0 && (!xyz_query || !idx_out || !dist_out)) ||
+      (p > 0 && (!steps || !steps_query || !neigh || !cnt)))
+    return FKNN_ERR_ARG;
+  if (!aligned(workspace, 256)) return FKNN_ERR_ARG;
+  QueryShape shape;
+  if ((rc = shape_from(config, &shape))) return rc;
+  fknn::TablesArgs t{xyz_support, n, steps, neigh, cnt, p, nullptr, steps_query, m, k, cut_r2,
+                     idx_out, dist_out, xyz_query, pad_index};
+  int launches = 0;
+  rc = fknn::run_tables(t, workspace, workspace_bytes, shape, as_stream(stream), &launches);
+  return finish(rc, launches);
+}
+
 size_t fknn_tables_workspace_bytes(int64_t n, int64_t m, int64_t p) {
   if (n < 0 || m < 0 || p < 0) return 0;
   return fknn::tables_workspace_bytes(n, m, p);

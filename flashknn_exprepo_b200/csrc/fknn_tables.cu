@@ -92,6 +92,15 @@ __global__ void k_tab_qrec(const float* __restrict__ xyz, int64_t n, const int32
                         __int_as_float(static_cast<int>(r)));
 }
 
+// Separate query points (FlashKNN_Query_GM, the back-query kernels): row r
+// is qxyz[r], already grouped by the caller's steps_query.
+__global__ void k_tab_qxyz(const float* __restrict__ qxyz, int64_t m, float4* __restrict__ qrec) {
+  const int64_t r = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (r >= m) return;
+  qrec[r] = make_float4(qxyz[3 * r], qxyz[3 * r + 1], qxyz[3 * r + 2],
+                        __int_as_float(static_cast<int>(r)));
+}
+
 namespace {
 
 inline int blocks_for(int64_t n, int per_block) {
@@ -132,7 +141,8 @@ size_t tables_workspace_bytes(int64_t n, int64_t m, int64_t p) {
 
 int run_tables(const TablesArgs& t, void* ws, size_t ws_bytes, const QueryShape& shape,
                cudaStream_t s, int* launches) {
-  const bool selected = t.qindex != nullptr;
+  const bool general = t.qxyz != nullptr;
+  const bool selected = t.qindex != nullptr || general;
   const int64_t m = selected ? t.m : t.n;
   size_t need = 0;
   TabBufs b = tab_layout(ws, t.n, m, t.p, &need);
@@ -149,7 +159,10 @@ int run_tables(const TablesArgs& t, void* ws, size_t ws_bytes, const QueryShape&
   }
   k_tab_runs<<<blocks_for(t.p * 27, 256), 256, 0, s>>>(t.steps, t.neigh, t.cnt, t.p, b.meta, b.runs);
   ++nl;
-  if (selected && m > 0) {
+  if (general && m > 0) {
+    k_tab_qxyz<<<blocks_for(m, 256), 256, 0, s>>>(t.qxyz, m, b.qrec);
+    ++nl;
+  } else if (selected && m > 0) {
     k_tab_qrec<<<blocks_for(m, 256), 256, 0, s>>>(t.xyz_sorted, t.n, t.qindex, m, b.meta, b.qrec);
     ++nl;
   }
@@ -180,8 +193,13 @@ int run_tables(const TablesArgs& t, void* ws, size_t ws_bytes, const QueryShape&
     q.idx_out = t.idx_out;
     q.dist_out = t.dist_out;
     q.n_rows = m;
-    q.pad = selected ? static_cast<const void*>(t.qindex) : nullptr;
-    q.pad_mode = selected ? kPadArray32 : kPadSelf;
+    if (general) {
+      q.pad = t.qpad;
+      q.pad_mode = t.qpad ? kPadArray32 : kPadMinusOne;
+    } else {
+      q.pad = selected ? static_cast<const void*>(t.qindex) : nullptr;
+      q.pad_mode = selected ? kPadArray32 : kPadSelf;
+    }
     q.vec_ok = (reinterpret_cast<uintptr_t>(t.idx_out) % 16 == 0) &&
                (reinterpret_cast<uintptr_t>(t.dist_out) % 16 == 0);
     const int rc = launch_query(q, shape, s);

@@ -23,6 +23,8 @@ struct TablesArgs {
   float cut_r2;
   int32_t* idx_out;
   float* dist_out;
+  const float* qxyz;           // separate query points [m,3] grouped by steps_query, or null
+  const int32_t* qpad;         // with qxyz: pad index per query row, or null (pad -1)
 };
 
 struct BuildTablesArgs {

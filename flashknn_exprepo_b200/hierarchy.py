@@ -2,11 +2,13 @@
 ``Networks/hierarchy.py``: ``_voxel_first_cuda`` / ``build_flash_hierarchy``).
 
 Per level: voxel-first subsampling of the previous level (one CUDA call,
-``fknn_voxel_first``), then the grid self query at that level's voxel size
+``fknn_voxel_first``, and one read-back of the level's size with its status
+word), then the grid self query at that level's voxel size
 (``fknn_knn_offsets``); at the end, for every level below the first, the
 nearest-point map from the full cloud to that level (``fknn_back_query``,
-K = 1).  Output order and types follow the reference: ``forward + backward``
-with int64 tensors.
+K = 1), whose status words are combined on the device and read once.
+Output order and types follow the reference: ``forward + backward`` with
+int64 tensors.
 """
 from __future__ import annotations
 
@@ -14,7 +16,7 @@ import math
 
 import torch
 
-from . import ops
+from . import _lib, ops
 
 
 def voxel_first(xyz: torch.Tensor, size: float, batch_idx: torch.Tensor | None = None
@@ -52,15 +54,20 @@ def build_flash_hierarchy(metric_xyz: torch.Tensor,
             cumulative = cumulative[local]
             forward.append(local)
             levels.append(cumulative)
-        offsets = torch.tensor([len(current)], dtype=torch.int64, device=dev)
+        offsets = torch.full((1,), len(current), dtype=torch.int64, device=dev)  # no host copy
         idx, _ = ops.knn_offsets(current, offsets, int(k), float(size), exponent)
         forward.append(idx.long())
     backward: list[torch.Tensor] = []
+    # the back queries' status words are OR-ed on the device and read once
+    status = torch.zeros(1, dtype=torch.int32, device=dev)
     for level in range(len(levels) - 1, -1, -1):
         size = voxel_sizes[level + 1]
-        idx, _, empty = ops.back_query(full_xyz, levels[level], size * 2, 1, validate=True)
-        if empty:
-            raise AssertionError("some query points have no support point in their "
-                                 "neighbourhood; consider a larger query_grid_size")
+        idx, _, _ = ops.back_query(full_xyz, levels[level], size * 2, 1, status_into=status)
         backward.append(idx[:, 0])
+    bits = int(status.item()) if levels else 0
+    if bits & ~_lib.DEVICE_NO_CANDIDATES:
+        raise _lib.FknnError(f"back_query: device reported {_lib.status_text(bits)}")
+    if bits & _lib.DEVICE_NO_CANDIDATES:
+        raise AssertionError("some query points have no support point in their "
+                             "neighbourhood; consider a larger query_grid_size")
     return forward + backward

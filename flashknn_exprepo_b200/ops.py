@@ -7,8 +7,10 @@ problem (coordinates outside the Morton range, bad tables, ...).
 """
 from __future__ import annotations
 
+import collections
 import ctypes
 import math
+import threading
 
 import torch
 
@@ -40,11 +42,68 @@ def _config_ptr(config):
     return c, ctypes.byref(c)
 
 
+class _GraphCache:
+    """Captured pipelines for ``graph=True`` calls, per host thread (LRU).
+
+    A small problem spends most of its time launching its dozen kernels;
+    replaying them from one CUDA graph removes the host-side launch cost.
+    An entry is keyed by everything the launches depend on -- the entry
+    point, the device, the input pointers and sizes, K, the grid parameters
+    and the launch shape -- and owns its workspace and output tensors: the
+    tensors a graph call returns are overwritten by the next call with the
+    same key (clone them to keep them).  Data-dependent sizes (cells, work
+    items) stay on the device, so one capture serves any point values."""
+
+    def __init__(self, capacity=16):
+        self._local = threading.local()
+        self.capacity = capacity
+
+    def _entries(self):
+        e = getattr(self._local, "entries", None)
+        if e is None:
+            e = self._local.entries = collections.OrderedDict()
+        return e
+
+    def run(self, key, dev, ws_bytes, make_outputs, launch):
+        entries = self._entries()
+        hit = entries.get(key)
+        if hit is None:
+            ws = torch.empty(max(int(ws_bytes), 256), dtype=torch.uint8, device=dev)
+            cur = torch.cuda.current_stream(dev)
+            side = torch.cuda.Stream(dev)
+            side.wait_stream(cur)
+            with torch.cuda.stream(side):
+                launch(ws, *make_outputs())  # loads the kernels, fills the launch cache
+                graph = torch.cuda.CUDAGraph()
+                with torch.cuda.graph(graph, stream=side):
+                    outs = make_outputs()
+                    launch(ws, *outs)
+            cur.wait_stream(side)
+            hit = (graph, outs, ws)
+            entries[key] = hit
+            while len(entries) > self.capacity:
+                entries.popitem(last=False)
+        else:
+            entries.move_to_end(key)
+        hit[0].replay()
+        return hit[1], hit[2]
+
+    def clear(self):
+        self._entries().clear()
+
+
+GRAPHS = _GraphCache()
+
+
 def knn_offsets(xyz, offset, k, voxel, num_down=2, new_xyz=None, new_offset=None,
-                cut_r2=math.inf, config=None, validate=False):
-    """Pointcept-style batched grid kNN.  Returns (idx int32 [m,k], dist2 f32 [m,k])."""
+                cut_r2=math.inf, config=None, validate=False, graph=False):
+    """Pointcept-style batched grid kNN.  Returns (idx int32 [m,k], dist2 f32 [m,k]).
+
+    ``graph=True`` replays a cached CUDA graph of the whole pipeline (captured
+    on the first call with these inputs); the returned tensors are the
+    graph's own and are overwritten by the next such call."""
     return _offsets_call("fknn_knn_offsets", xyz, offset, k, voxel, num_down, new_xyz,
-                         new_offset, float(cut_r2), config, validate)
+                         new_offset, float(cut_r2), config, validate, graph)
 
 
 def ball_query_offsets(xyz, offset, nsample, max_radius, voxel, num_down=2, new_xyz=None,
@@ -57,7 +116,7 @@ def ball_query_offsets(xyz, offset, nsample, max_radius, voxel, num_down=2, new_
 
 
 def _offsets_call(entry, xyz, offset, k, voxel, num_down, new_xyz, new_offset, last, config,
-                  validate):
+                  validate, graph=False):
     lib = _lib.load()
     xyz = _require(xyz, "xyz", torch.float32, 2, 3)
     dev = xyz.device
@@ -73,28 +132,42 @@ def _offsets_call(entry, xyz, offset, k, voxel, num_down, new_xyz, new_offset, l
     n = xyz.shape[0]
     m = new_xyz.shape[0] if general else n
     b = offset.numel()
-    idx = torch.empty((m, k), dtype=torch.int32, device=dev)
-    dist = torch.empty((m, k), dtype=torch.float32, device=dev)
     kind = _lib.QUERY_GENERAL if general else _lib.QUERY_SELF
     nbytes = lib.fknn_workspace_bytes(n, m, max(b, 1), kind)
-    ws = _lib.WORKSPACE.get(nbytes, dev)
-    _, cfg = _config_ptr(config)
-    rc = getattr(lib, entry)(ptr(xyz), n, ptr(offset), b, ptr(new_xyz), m, ptr(new_offset), k,
-                             float(voxel), num_down, last, ptr(idx), ptr(dist), ptr(ws),
-                             ws.numel(), cfg, stream_handle(dev))
-    check(rc, entry)
+    c, cfg = _config_ptr(config)
+
+    def outputs():
+        return (torch.empty((m, k), dtype=torch.int32, device=dev),
+                torch.empty((m, k), dtype=torch.float32, device=dev))
+
+    def launch(ws, idx, dist):
+        rc = getattr(lib, entry)(ptr(xyz), n, ptr(offset), b, ptr(new_xyz), m, ptr(new_offset),
+                                 k, float(voxel), num_down, last, ptr(idx), ptr(dist), ptr(ws),
+                                 ws.numel(), cfg, stream_handle(dev))
+        check(rc, entry)
+
+    if graph:
+        key = (entry, dev.index, ptr(xyz), n, ptr(offset), b, ptr(new_xyz), m, ptr(new_offset),
+               k, float(voxel), num_down, last, None if c is None else c.as_tuple())
+        (idx, dist), ws = GRAPHS.run(key, dev, nbytes, outputs, launch)
+    else:
+        ws = _lib.WORKSPACE.get(nbytes, dev)
+        idx, dist = outputs()
+        launch(ws, idx, dist)
     if validate:
         _lib.raise_on_status(ws, entry)
     return idx, dist
 
 
 def knn_grid(xyz, grid_coord, batch_idx, k, num_down=2, cut_r2=math.inf, query_indices=None,
-             idx_dtype=torch.int64, config=None, validate=False, candidate_stats=None):
+             idx_dtype=torch.int64, config=None, validate=False, candidate_stats=None,
+             graph=False):
     """FlashKNN.query / selected_query on caller-voxelised grid coordinates.
 
     Returns (idx [m,k] of ``idx_dtype`` in original point numbering, dist2 f32).
     With ``candidate_stats`` (a list) a self query appends (candidate total,
     parent cells) read back from the device (one synchronisation).
+    ``graph=True`` replays a cached CUDA graph, as ``knn_offsets``.
     """
     lib = _lib.load()
     grid_coord = _require(grid_coord, "grid_coord", torch.int64, 2, 3)
@@ -113,16 +186,30 @@ def knn_grid(xyz, grid_coord, batch_idx, k, num_down=2, cut_r2=math.inf, query_i
     m = query_indices.numel() if selected else n
     if idx_dtype not in (torch.int32, torch.int64):
         raise ValueError("idx_dtype must be torch.int32 or torch.int64")
-    idx = torch.empty((m, k), dtype=idx_dtype, device=dev)
-    dist = torch.empty((m, k), dtype=torch.float32, device=dev)
     kind = _lib.QUERY_SELECTED if selected else _lib.QUERY_SELF
     nbytes = lib.fknn_workspace_bytes(n, m, 32768, kind)
-    ws = _lib.WORKSPACE.get(nbytes, dev)
-    _, cfg = _config_ptr(config)
-    rc = lib.fknn_knn_grid(ptr(xyz), ptr(grid_coord), ptr(batch_idx), n, ptr(query_indices), m, k,
-                           num_down, float(cut_r2), 64 if idx_dtype == torch.int64 else 32,
-                           ptr(idx), ptr(dist), ptr(ws), ws.numel(), cfg, stream_handle(dev))
-    check(rc, "fknn_knn_grid")
+    c, cfg = _config_ptr(config)
+    bits = 64 if idx_dtype == torch.int64 else 32
+
+    def outputs():
+        return (torch.empty((m, k), dtype=idx_dtype, device=dev),
+                torch.empty((m, k), dtype=torch.float32, device=dev))
+
+    def launch(ws, idx, dist):
+        rc = lib.fknn_knn_grid(ptr(xyz), ptr(grid_coord), ptr(batch_idx), n, ptr(query_indices),
+                               m, k, num_down, float(cut_r2), bits, ptr(idx), ptr(dist),
+                               ptr(ws), ws.numel(), cfg, stream_handle(dev))
+        check(rc, "fknn_knn_grid")
+
+    if graph:
+        key = ("fknn_knn_grid", dev.index, ptr(xyz), ptr(grid_coord), ptr(batch_idx), n,
+               ptr(query_indices), m, k, num_down, float(cut_r2), bits,
+               None if c is None else c.as_tuple())
+        (idx, dist), ws = GRAPHS.run(key, dev, nbytes, outputs, launch)
+    else:
+        ws = _lib.WORKSPACE.get(nbytes, dev)
+        idx, dist = outputs()
+        launch(ws, idx, dist)
     if validate:
         _lib.raise_on_status(ws, "knn_grid")
     if candidate_stats is not None:
@@ -131,12 +218,15 @@ def knn_grid(xyz, grid_coord, batch_idx, k, num_down=2, cut_r2=math.inf, query_i
 
 
 def back_query(xyz, sel_indices, query_grid_size, k, batch_idx=None, idx_dtype=torch.int64,
-               config=None, validate=False):
+               config=None, validate=False, status_into=None):
     """FlashKNN.back_query kernels: for every point of ``xyz`` the k nearest
     points of the subset ``sel_indices`` in the 27 cells around its cell
     (cells = trunc(xyz / query_grid_size)).  Returns (idx [n,k] positions in
     ``sel_indices``, dist2 f32 [n,k], empty) where ``empty`` is True when some
-    point had no subset point around it (its row is (-1, +inf))."""
+    point had no subset point around it (its row is (-1, +inf)).  With
+    ``status_into`` (an int32 CUDA tensor of one element) the device status
+    word is OR-ed into it on the stream instead of being read back, so
+    several calls can be checked with one synchronisation."""
     lib = _lib.load()
     xyz = _require(xyz, "xyz", torch.float32, 2, 3)
     dev = xyz.device
@@ -157,6 +247,8 @@ def back_query(xyz, sel_indices, query_grid_size, k, batch_idx=None, idx_dtype=t
                              float(query_grid_size), k, 64 if idx_dtype == torch.int64 else 32,
                              ptr(idx), ptr(dist), ptr(ws), ws.numel(), cfg, stream_handle(dev))
     check(rc, "fknn_back_query")
+    if status_into is not None:
+        status_into.bitwise_or_(ws[:4].view(torch.int32))
     empty = None
     if validate:
         _lib.raise_on_status(ws, "back_query")
@@ -225,9 +317,13 @@ def voxel_first(xyz, voxel, batch_idx=None, validate=False):
     rc = lib.fknn_voxel_first(ptr(xyz), n, ptr(batch_idx), float(voxel), ptr(out), ptr(count),
                               ptr(ws), ws.numel(), stream_handle(dev))
     check(rc, "fknn_voxel_first")
-    if validate:
-        _lib.raise_on_status(ws, "voxel_first")
-    return out[: int(count.item())]
+    # one read-back for both the count and the device status word
+    status = ws[:4].view(torch.int32).to(torch.int64)
+    got = torch.cat([count, status]).cpu()
+    bits = int(got[1]) & ~_lib.DEVICE_NO_CANDIDATES
+    if validate and bits:
+        raise FknnError(f"voxel_first: device reported {_lib.status_text(bits)} (status {bits})")
+    return out[: int(got[0])]
 
 
 def adaptive_query(grid_coord, batch_idx, k, xyz=None, min_factor=2, max_factor=8,
@@ -288,6 +384,39 @@ def query_tables(xyz_sorted, steps, neigh, cnt, k, cut_r2=math.inf, config=None,
     check(rc, "fknn_query_tables")
     if validate:
         _lib.raise_on_status(ws, "query_tables")
+    return idx, dist
+
+
+def general_query_tables(xyz_support, xyz_query, steps, steps_query, neigh, cnt, k,
+                         pad_index=None, cut_r2=math.inf, config=None, validate=False):
+    """Separate query points over caller tables (FlashKNN_Query_GM and the
+    back-query table kernels): (idx int32 [m,k] rows of xyz_support, dist2)."""
+    lib = _lib.load()
+    xyz_support = _require(xyz_support, "xyz_support", torch.float32, 2, 3)
+    dev = xyz_support.device
+    xyz_query = _require(xyz_query, "xyz_query", torch.float32, 2, 3)
+    steps = _require(steps, "steps", torch.int32, 1)
+    steps_query = _require(steps_query, "steps_query", torch.int32, 1)
+    neigh = _require(neigh, "neigh", torch.int32, 2, 27)
+    cnt = _require(cnt, "cnt", torch.int32, 2, 28)
+    n, m, p = xyz_support.shape[0], xyz_query.shape[0], neigh.shape[0]
+    if steps.numel() != p + 1 or steps_query.numel() != p + 1 or cnt.shape[0] != p:
+        raise ValueError("steps and steps_query must have P+1 entries and cnt P rows")
+    if pad_index is not None:
+        pad_index = _require(pad_index, "pad_index", torch.int32, 1)
+        if pad_index.numel() != m:
+            raise ValueError("pad_index must have one entry per query")
+    idx = torch.empty((m, k), dtype=torch.int32, device=dev)
+    dist = torch.empty((m, k), dtype=torch.float32, device=dev)
+    ws = _lib.WORKSPACE.get(lib.fknn_tables_workspace_bytes(n, m, p), dev)
+    _, cfg = _config_ptr(config)
+    rc = lib.fknn_general_query_tables(ptr(xyz_support), n, ptr(xyz_query), m, ptr(pad_index),
+                                       ptr(steps), ptr(steps_query), ptr(neigh), ptr(cnt), p, k,
+                                       float(cut_r2), ptr(idx), ptr(dist), ptr(ws), ws.numel(),
+                                       cfg, stream_handle(dev))
+    check(rc, "fknn_general_query_tables")
+    if validate:
+        _lib.raise_on_status(ws, "general_query_tables")
     return idx, dist
 
 

@@ -85,7 +85,7 @@ class FlashKNN:
     def query(self, grid_coord, batch_idx, xyz=None, dynamic_load=True, cut_radius=math.inf,
               batch_for_prune=1, memory_mode="SM", sorting_mode="PS", candidate_mode="register",
               enable_skip=True, thread_group_size=None, traverse_info=None,
-              return_distances=False, validate=False):
+              return_distances=False, validate=False, graph=False):
         """Self query: the K nearest neighbours of every point among the points
         of the 27 parent cells around its own parent cell (parent = grid >>
         num_down).  Returns int64 [N, K] original indices; with
@@ -94,7 +94,10 @@ class FlashKNN:
         the reference kernel.  ``traverse_info[0]`` receives the mean number
         of candidates per parent cell (the points of its 27 neighbour cells),
         as FlashKnnWrapper.py:351-352 writes it: summed exactly on the device
-        and rounded to FP32 (the reference takes an FP32 mean).
+        and rounded to FP32 (the reference takes an FP32 mean).  ``graph=True``
+        replays a CUDA graph cached per input tensors (for small, repeated
+        problems whose time is mostly kernel launches); the result then is
+        the graph's own tensor, overwritten by the next such call.
         """
         self._check_modes(memory_mode, sorting_mode, candidate_mode, enable_skip,
                           thread_group_size)
@@ -105,7 +108,7 @@ class FlashKNN:
             coords, grid_coord, batch_idx, self.num_nbr, self.num_down,
             cut_r2=float(cut_radius) * float(cut_radius),
             idx_dtype=torch.int32 if return_distances else torch.int64,
-            config=self.config, validate=validate, candidate_stats=stats)
+            config=self.config, validate=validate, candidate_stats=stats, graph=graph)
         if traverse_info is not None:
             total, cells = stats[0]
             mean = total / cells if cells else float("nan")

@@ -283,6 +283,28 @@ FKNN_API int fknn_selected_query_tables(const float* xyz_sorted, int64_t n, cons
                                void* workspace, size_t workspace_bytes,
                                const fknn_config* config, void* stream);
 
+/* Queries that are separate points over caller tables.  Replaces
+ * FlashKNN_Query_GM (FlashKNN/csrc/flash_knn_query.h:220-233) and the
+ * back-query table kernels FlashKNN_Nearest_Back_Query_DL /
+ * FlashKNN_Back_Query_DL (flash_knn_query.h:183-204): xyz_query f32 [m,3]
+ * grouped by parent through steps_query int32 [p+1]; candidates are the
+ * points of xyz_support f32 [n,3] in the 27 runs of the query's parent
+ * (steps int32 [p+1] support starts, neigh int32 [p,27], cnt int32 [p,28]
+ * over the support counts).  idx_out int32 [m,k] (rows of xyz_support) and
+ * dist_out f32 [m,k], ascending by (distance, index); a row with fewer than k
+ * candidates is padded with (pad_index[r], +inf), or (-1, +inf) when
+ * pad_index is NULL.  (The reference's back-query kernels leave K > 1 rows in
+ * heap order and its nearest kernel pads with (0, -1).)  Workspace:
+ * fknn_tables_workspace_bytes(n, m, p). */
+FKNN_API int fknn_general_query_tables(const float* xyz_support, int64_t n,
+                                       const float* xyz_query, int64_t m,
+                                       const int32_t* pad_index, const int32_t* steps,
+                                       const int32_t* steps_query, const int32_t* neigh,
+                                       const int32_t* cnt, int64_t p, int32_t k, float cut_r2,
+                                       int32_t* idx_out, float* dist_out, void* workspace,
+                                       size_t workspace_bytes, const fknn_config* config,
+                                       void* stream);
+
 /* ------------------------------------------------- construction (a1..a6)
  * Replaces FlashKNN_Morton_Encode (FlashKNN/csrc/flash_knn_construction.h:7-9,
  * kernel flash_knn_construction.cu:29-40): keys int64 [n]; batch NULL = 0. */

@@ -277,3 +277,36 @@ def test_backward_list_lengths(fk, k):
                             g.cpu().numpy().astype(np.float64))
     assert _rel_max(outs[0][0], wq) <= 1e-5
     assert _rel_max(outs[0][1], wp) <= 1e-5
+
+
+def test_buckets_beyond_the_stage_and_a_point_beyond_it(fk):
+    """Arbitrary neighbour tables (the backward takes any idx): one point
+    named by 20,000 rows (more entries than a bucket's whole shared-memory
+    stage: summed by a warp streaming the runs) and forty points named by 500
+    rows each (one bucket holding more than the stage: several point ranges),
+    the rest random.  Against the oracle's FP64 backward, bitwise identical
+    run to run."""
+    rng = np.random.default_rng(21)
+    m, n, k = 40000, 30000, 8
+    q = rng.random((m, 3), dtype=np.float32)
+    p = rng.random((n, 3), dtype=np.float32)
+    idx = rng.integers(100, n, size=(m, k)).astype(np.int32)
+    idx[:20000, 0] = 0                                   # the hub
+    idx[20000:, 1] = 1 + (np.arange(m - 20000) % 40)     # 40 points x 500 rows
+    dist = ((q[:, None, :] - p[idx]) ** 2).sum(-1).astype(np.float32)
+    dist[rng.random((m, k)) < 0.01] = np.inf             # some padding entries
+    g = rng.standard_normal((m, k)).astype(np.float32)
+    Q, P, I, D, G = (torch.from_numpy(a).to(DEV) for a in (q, p, idx, dist, g))
+    outs = []
+    for _ in range(2):
+        gq = torch.empty_like(Q)
+        gp = torch.empty_like(P)
+        fk.ops.backward(Q, P, I, D, G, grad_q=gq, grad_p=gp)
+        outs.append((gq.cpu().numpy(), gp.cpu().numpy()))
+    for a, b in zip(outs[0], outs[1]):
+        assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+    wq, wp = O.backward_f64(q, p, idx, dist, g.astype(np.float64))
+    assert _rel_max(outs[0][0], wq) <= 1e-5
+    # the hub's gradient is a sequential FP32 sum of 20,000 terms: its
+    # rounding error grows like sqrt(20000) * 2^-24 of the result
+    assert _rel_max(outs[0][1], wp) <= 5e-5

@@ -70,3 +70,25 @@ def test_traverse_info_is_the_mean_candidate_count(fk, case):
     f.query(torch.from_numpy(z["grid"]).cuda(), torch.from_numpy(z["batch"]).cuda(),
             torch.from_numpy(z["xyz"]).cuda(), traverse_info=info)
     assert info[0] == pytest.approx(float(want), rel=1e-6)
+
+
+def test_graph_mode_replays_the_eager_pipeline(fk):
+    """graph=True: the first call captures, later calls replay; the results
+    equal the eager call's bit for bit, also after the input values change
+    in place (same pointers, same graph) and for a second input."""
+    from flashknn_exprepo_b200 import synthetic as S
+    xyz = torch.from_numpy(S.uniform_cube()).cuda()
+    off = torch.tensor([xyz.shape[0]], device="cuda")
+    want = fk.ops.knn_offsets(xyz, off, 16, S.C1_VOXEL, 2)
+    for _ in range(3):
+        got = fk.ops.knn_offsets(xyz, off, 16, S.C1_VOXEL, 2, graph=True, validate=True)
+        assert torch.equal(got[0], want[0]) and torch.equal(got[1], want[1])
+    xyz.mul_(0.5).add_(0.25)  # new values at the same address: the same graph
+    want = fk.ops.knn_offsets(xyz, off, 16, S.C1_VOXEL, 2)
+    got = fk.ops.knn_offsets(xyz, off, 16, S.C1_VOXEL, 2, graph=True)
+    assert torch.equal(got[0], want[0]) and torch.equal(got[1], want[1])
+    grid = torch.floor(xyz / S.C1_VOXEL).long()
+    f = fk.FlashKNN(num_nbr=8, num_down=2)
+    want = f.query(grid, None, xyz)
+    for _ in range(2):
+        assert torch.equal(f.query(grid, None, xyz, graph=True), want)
