@@ -45,9 +45,9 @@ __global__ void __launch_bounds__(256)
 // buffer holds; k_scan_segments clamps the count to match).
 __global__ void __launch_bounds__(256)
     k_pack(const int32_t* __restrict__ group_start, const int32_t* __restrict__ cands,
-           const int* group_count_ptr, int tile, int64_t n_queries, int64_t capacity,
-           uint32_t* __restrict__ seg_counts, const uint32_t* __restrict__ seg_offsets,
-           int4* __restrict__ items, int* status) {
+           const int* group_count_ptr, int tile, int max_q, int64_t n_queries,
+           int64_t capacity, uint32_t* __restrict__ seg_counts,
+           const uint32_t* __restrict__ seg_offsets, int4* __restrict__ items, int* status) {
   const int n_groups = *group_count_ptr;
   const int64_t n_segs = (n_groups + kPackSegment - 1) / kPackSegment;
   for (int64_t seg = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; seg < n_segs;
@@ -88,14 +88,14 @@ __global__ void __launch_bounds__(256)
       while (pos < ge) {
         // An item spans the groups [cur_g0, g]: groups without queries inside
         // that span still count, because the kernel walks the span.
-        if (cur_gn > 0 && (cur_c + c > tile || cur_qn == 32 ||
+        if (cur_gn > 0 && (cur_c + c > tile || cur_qn >= max_q ||
                            g - cur_g0 + 1 > kMaxGroupsPerItem))
           flush();
         if (cur_gn == 0) {
           cur_q0 = pos;
           cur_g0 = g;
         }
-        const int take = min(ge - pos, 32 - cur_qn);
+        const int take = min(ge - pos, max_q - cur_qn);
         cur_qn += take;
         cur_gn = g - cur_g0 + 1;
         cur_c += c;
@@ -130,6 +130,25 @@ __global__ void __launch_bounds__(1024)
   }
 }
 
+// Queries per packed item.  A large problem fills every lane (32); a small
+// one -- fewer than 16 queries per resident query warp -- is cut into about
+// one item per resident warp (at least 4 queries each), so its few items do
+// not leave most warps idle while each one runs the whole scan.
+int item_query_cap(int64_t n_queries) {
+  static int sms = 0;
+  if (sms == 0) {
+    int dev = 0, v = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess &&
+        cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess)
+      sms = v;
+    if (sms <= 0) return 32;
+  }
+  const int64_t warps = static_cast<int64_t>(sms) * 20;  // resident at the default shape
+  if (n_queries >= warps * 16) return 32;
+  const int64_t cap = ceil_div(n_queries > 0 ? n_queries : 1, warps);
+  return static_cast<int>(cap < 4 ? 4 : (cap > 32 ? 32 : cap));
+}
+
 int launch_items(const int2* runs, const int32_t* group_start, const int32_t* group_row,
                  const int* group_count_ptr, int64_t max_groups, int tile, int32_t* cands,
                  uint32_t* seg_counts, int* n_items_ptr, int4* items, cudaStream_t s,
@@ -143,11 +162,12 @@ int launch_items(const int2* runs, const int32_t* group_start, const int32_t* gr
   if (!cands_ready)  // else the caller's run kernel wrote cands[g] already
     k_group_cands<<<gblocks, 256, 0, s>>>(runs, group_row, group_count_ptr, cands, status);
   const int64_t capacity = static_cast<int64_t>(items_capacity(max_groups, n_queries));
-  k_pack<<<sblocks, 256, 0, s>>>(group_start, cands, group_count_ptr, tile, n_queries, capacity,
-                                 seg_counts, nullptr, nullptr, status);
+  const int max_q = item_query_cap(n_queries);
+  k_pack<<<sblocks, 256, 0, s>>>(group_start, cands, group_count_ptr, tile, max_q, n_queries,
+                                 capacity, seg_counts, nullptr, nullptr, status);
   k_scan_segments<<<1, 1024, 0, s>>>(seg_counts, group_count_ptr, capacity, n_items_ptr, status);
-  k_pack<<<sblocks, 256, 0, s>>>(group_start, cands, group_count_ptr, tile, n_queries, capacity,
-                                 nullptr, seg_counts, items, status);
+  k_pack<<<sblocks, 256, 0, s>>>(group_start, cands, group_count_ptr, tile, max_q, n_queries,
+                                 capacity, nullptr, seg_counts, items, status);
   return cands_ready ? 3 : 4;
 }
 

@@ -117,7 +117,7 @@ def test_general_tables_pad_rules(fk):
     """A query whose parent has no candidates is padded with its pad index
     (or -1 without one) and +inf."""
     sx = T(np.array([[0.1, 0.1, 0.1], [0.2, 0.1, 0.1]], np.float32))
-    qx = T(np.array([[0.15, 0.1, 0.1], [5.0, 5.0, 5.0]], np.float32))
+    qx = T(np.array([[0.12, 0.1, 0.1], [5.0, 5.0, 5.0]], np.float32))  # nearer point 0
     steps = T(np.array([0, 2, 2], np.int32))          # parent 1 holds no support point
     steps_q = T(np.array([0, 1, 2], np.int32))
     neigh = np.full((2, 27), -1, np.int32)
