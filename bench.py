@@ -509,7 +509,7 @@ def _event_ms(torch, fn, flush, reps=5):
     return total / reps
 
 
-def rows_single_gpu(fk, torch, dev, flush, peak_gbs):
+def rows_single_gpu(fk, torch, dev, flush, peak_gbs, clouds=16):
     """The paths around the batched query, each on its own workload:
     adaptive-neighbourhood query (LiDAR scan), back query and voxel-first
     subsampling (16-cloud batch), the DeLA hierarchy builder (LiDAR scan),
@@ -557,8 +557,11 @@ def rows_single_gpu(fk, torch, dev, flush, peak_gbs):
                                   "points_per_level": {int(a): int(b) for a, b in
                                                        zip(lvl.tolist(), cnt.tolist())},
                                   "step": "CUDA-graph replay of the whole adaptive pipeline"}
-    # back query K=1 and voxel-first subsampling, 16-cloud batch
+    # back query K=1 and voxel-first subsampling, 16-cloud batch (or its
+    # first `clouds` clouds: smaller cases for profiling)
     b = synthetic.uneven_batch()
+    if clouds < len(b.counts):
+        b = synthetic.first_clouds(b, clouds)
     bx = T(b.xyz)
     bb = T(np.repeat(np.arange(len(b.counts)), b.counts).astype(np.int64))
     ms = _event_ms(torch, lambda: fk.ops.voxel_first(bx, 0.1, bb), flush)
@@ -690,6 +693,8 @@ def rows_only(args):
     torch.cuda.set_device(dev)
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
     b = synthetic.uneven_batch()
+    if args.clouds < len(b.counts):
+        b = synthetic.first_clouds(b, args.clouds)
     x = torch.from_numpy(b.xyz).to(dev)
     off = torch.from_numpy(b.offsets).to(dev)
     idx, d = fk.ops.knn_offsets(x, off, args.k, synthetic.C4_VOXEL, 2)
@@ -698,8 +703,9 @@ def rows_only(args):
     grad = torch.zeros_like(x)
     ms = _event_ms(torch, lambda: fk.ops.backward(x, x, idx, d, g, grad_q=grad, grad_p=grad,
                                                   accumulate=True), flush)
-    return {"backward_ms": ms, "rows": rows_single_gpu(fk, torch, dev, flush,
-                                                       measured_peak_hbm()[0])}
+    return {"backward_ms": ms, "n_points": int(len(b.xyz)),
+            "rows": rows_single_gpu(fk, torch, dev, flush, measured_peak_hbm()[0],
+                                    clouds=args.clouds)}
 
 
 def fd_check(fk, torch, dev, batch, k, voxel, count=2048, h=1e-4):
