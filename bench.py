@@ -439,6 +439,23 @@ def extras_single_gpu(args, fk, torch, dev, batch, voxel, flush):
     res["per_cloud_graph"] = {"value": n / (gms * 1e-3), "unit": "queries/s", "ms_per_step": gms,
                               "what": "the same 16 per-cloud calls replayed from one CUDA graph"}
 
+    # the batched step at K=32 (the batch configuration's second K): one
+    # graph of construction + query, replayed, L2 flushed before each
+    xyz_all = torch.from_numpy(batch.xyz).to(dev)
+    off_all = torch.from_numpy(batch.offsets).to(dev)
+    with torch.cuda.stream(stream):
+        fk.ops.knn_offsets(xyz_all, off_all, 32, voxel, 2)
+        torch.cuda.synchronize(dev)
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph, stream=stream):
+            fk.ops.knn_offsets(xyz_all, off_all, 32, voxel, 2)
+    torch.cuda.current_stream(dev).wait_stream(stream)
+    torch.cuda.synchronize(dev)
+    kms = _event_ms(torch, graph.replay, flush, reps=reps)
+    del graph
+    res["batched_k32"] = {"value": n / (kms * 1e-3), "unit": "queries/s", "ms_per_step": kms,
+                          "what": "batched construction + query at K=32, one CUDA graph"}
+
     # forward + backward (loss = sum(w * d), w ~ N(0,1))
     xyz = torch.from_numpy(batch.xyz).to(dev)
     off = torch.from_numpy(batch.offsets).to(dev)
@@ -980,6 +997,8 @@ def main():
     if "per_cloud_graph" in out:
         line["per_cloud_graph"] = out["per_cloud_graph"]
         line["batched_vs_per_cloud_graph"] = out["value"] / out["per_cloud_graph"]["value"]
+    if "batched_k32" in out:
+        line["batched_k32"] = out["batched_k32"]
     if "fwd_bwd_ms" in out:
         line["fwd_bwd_ms"] = out["fwd_bwd_ms"]
     if "fd_check" in out:

@@ -45,7 +45,7 @@ __global__ void __launch_bounds__(256)
 // buffer holds; k_scan_segments clamps the count to match).
 __global__ void __launch_bounds__(256)
     k_pack(const int32_t* __restrict__ group_start, const int32_t* __restrict__ cands,
-           const int* group_count_ptr, int tile, int max_q, int64_t n_queries,
+           const int* group_count_ptr, int tile, int max_q, int max_qc, int64_t n_queries,
            int64_t capacity, uint32_t* __restrict__ seg_counts,
            const uint32_t* __restrict__ seg_offsets, int4* __restrict__ items, int* status) {
   const int n_groups = *group_count_ptr;
@@ -81,7 +81,7 @@ __global__ void __launch_bounds__(256)
       if (ge <= gs) continue;
       if (c > tile) {  // streams its candidates: items of its own
         flush();
-        for (int q = gs; q < ge; q += 32) emit(q, min(32, ge - q), g, 1, kItemChunked);
+        for (int q = gs; q < ge; q += max_qc) emit(q, min(max_qc, ge - q), g, 1, kItemChunked);
         continue;
       }
       int pos = gs;
@@ -149,6 +149,25 @@ int item_query_cap(int64_t n_queries) {
   return static_cast<int>(cap < 4 ? 4 : (cap > 32 ? 32 : cap));
 }
 
+// Queries per chunked item (a group whose candidates exceed a tile: every
+// query scans many of them).  An item of q queries gives each query 32 / q
+// lanes.  A problem with fewer than 32 queries per resident query warp is
+// cut into about two items per warp (at least 4 queries each), so a dense
+// but small problem spreads every query's scan over several lanes instead
+// of one lane walking all its candidates; larger ones keep full items
+// (measured: the LiDAR scan at alpha 8, 118k points, is faster with full
+// items; the DeLA levels of 3.7k-72k points with split ones).
+int chunked_query_cap(int64_t n_queries) {
+  int dev = 0, sms = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0)
+    return 32;
+  const int64_t warps = static_cast<int64_t>(sms) * 20;
+  if (n_queries >= warps * 32) return 32;
+  const int64_t cap = ceil_div(n_queries > 0 ? n_queries : 1, 2 * warps);
+  return static_cast<int>(cap < 4 ? 4 : (cap > 32 ? 32 : cap));
+}
+
 int launch_items(const int2* runs, const int32_t* group_start, const int32_t* group_row,
                  const int* group_count_ptr, int64_t max_groups, int tile, int32_t* cands,
                  uint32_t* seg_counts, int* n_items_ptr, int4* items, cudaStream_t s,
@@ -163,11 +182,12 @@ int launch_items(const int2* runs, const int32_t* group_start, const int32_t* gr
     k_group_cands<<<gblocks, 256, 0, s>>>(runs, group_row, group_count_ptr, cands, status);
   const int64_t capacity = static_cast<int64_t>(items_capacity(max_groups, n_queries));
   const int max_q = item_query_cap(n_queries);
-  k_pack<<<sblocks, 256, 0, s>>>(group_start, cands, group_count_ptr, tile, max_q, n_queries,
-                                 capacity, seg_counts, nullptr, nullptr, status);
+  const int max_qc = chunked_query_cap(n_queries);
+  k_pack<<<sblocks, 256, 0, s>>>(group_start, cands, group_count_ptr, tile, max_q, max_qc,
+                                 n_queries, capacity, seg_counts, nullptr, nullptr, status);
   k_scan_segments<<<1, 1024, 0, s>>>(seg_counts, group_count_ptr, capacity, n_items_ptr, status);
-  k_pack<<<sblocks, 256, 0, s>>>(group_start, cands, group_count_ptr, tile, max_q, n_queries,
-                                 capacity, nullptr, seg_counts, items, status);
+  k_pack<<<sblocks, 256, 0, s>>>(group_start, cands, group_count_ptr, tile, max_q, max_qc,
+                                 n_queries, capacity, nullptr, seg_counts, items, status);
   return cands_ready ? 3 : 4;
 }
 

@@ -283,12 +283,13 @@ __device__ __forceinline__ int2 load_run(const QueryLaunch& a, int row, int lane
 
 // Record of query qi of a chunked item (queries q0 .. q0+qn-1 of group g0):
 // the group's queries taken in octant-major order around their centroid
-// (item j of the group = positions 32j .. 32j+31 of that order), so every
-// query belongs to exactly one item and an item's queries are close
-// together.  Groups of at most 32 or more than kMaxOrderedGroup queries, and
-// items not cut at multiples of 32, keep record order.  qlist: 32 ints of
-// scratch; hist: 8 counters.  Kept out of line so its registers do not add
-// to the packed path's.
+// (the packer cuts a chunked group into consecutive items from its first
+// query, so the item covering positions [q0 - start, q0 - start + qn) of
+// that order takes those queries), so every query belongs to exactly one
+// item and an item's queries are close together.  A group the item holds
+// whole, or one of more than kMaxOrderedGroup queries, keeps record order.
+// qlist: 32 ints of scratch; hist: 8 counters.  Kept out of line so its
+// registers do not add to the packed path's.
 __device__ __noinline__ int ordered_query_row(const float4* __restrict__ qrec,
                                               const int32_t* __restrict__ group_start, int g0,
                                               int q0, int qn, int qi, bool active, int* qlist,
@@ -296,8 +297,7 @@ __device__ __noinline__ int ordered_query_row(const float4* __restrict__ qrec,
   const int lane = threadIdx.x & 31;
   const int gq0 = group_start[g0], gq1 = group_start[g0 + 1];
   const int nqg = gq1 - gq0;
-  if (!(nqg > 32 && nqg <= kMaxOrderedGroup && q0 >= gq0 && q0 + qn <= gq1 &&
-        (q0 - gq0) % 32 == 0))
+  if (!(nqg > qn && nqg <= kMaxOrderedGroup && q0 >= gq0 && q0 + qn <= gq1))
     return q0 + qi;
   float gx = 0.f, gy = 0.f, gz = 0.f;
   for (int t = lane; t < nqg; t += 32) {
@@ -380,8 +380,8 @@ __device__ __noinline__ int chunked_item(const QueryLaunch& a, int T, int min_ca
   const int qi = lane >> lg, sub = lane & (G - 1);
   const bool active = qi < qn;
   const bool takes = active && cut_accepts_any(a.cut_r2);
-  // The packer cuts the group's queries into items of 32 in record order
-  // (item j = positions 32j..): take them instead in octant-major order
+  // The packer cuts the group's queries into items in record order: take
+  // them instead in octant-major order
   // (ordered_query_row), so an item's queries are close together and the
   // phase-B sphere below stays small.
   const int qrow = ordered_query_row(a.qrec, a.group_start, g0, q0, qn, qi, active,
