@@ -9,7 +9,7 @@
 // stream their candidates tile by tile.
 //
 // Packing is a sequential greedy pass over the groups in key order; it runs
-// in parallel over segments of kPackSegment groups (one thread each): a
+// in parallel over segments of kPackSegment groups (one warp each): a
 // count pass, a scan of the per-segment counts, and a write pass.  Items
 // therefore keep the spatial order of the groups.
 #include "fknn_common.cuh"
@@ -36,52 +36,73 @@ __global__ void __launch_bounds__(256)
   }
 }
 
-// One thread per segment of kPackSegment groups.  With items == nullptr it
+// One warp per segment of kPackSegment groups.  With items == nullptr it
 // only counts (seg_counts[seg]); otherwise it writes its items at
 // seg_offsets[seg].  Item = (q_start, q_count, g_first, g_count | flags).
+// The segment's group ranges and candidate counts are loaded once (one
+// group per lane); every lane then walks the greedy pass with the same
+// values, lane 0 writes packed items and the whole warp writes a chunked
+// group's items, so a group of many chunked items costs no serial stores.
 // Caller tables can be malformed: a group whose query range leaves
 // [0, n_queries] is reported and skipped, and no item is written at or past
 // `capacity` (overlapping ranges could otherwise ask for more items than the
 // buffer holds; k_scan_segments clamps the count to match).
+static_assert(kPackSegment <= 32, "one group per lane");
 __global__ void __launch_bounds__(256)
     k_pack(const int32_t* __restrict__ group_start, const int32_t* __restrict__ cands,
            const int* group_count_ptr, int tile, int max_q, int max_qc, int64_t n_queries,
            int64_t capacity, uint32_t* __restrict__ seg_counts,
            const uint32_t* __restrict__ seg_offsets, int4* __restrict__ items, int* status) {
+  const int lane = threadIdx.x & 31;
   const int n_groups = *group_count_ptr;
   const int64_t n_segs = (n_groups + kPackSegment - 1) / kPackSegment;
-  for (int64_t seg = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; seg < n_segs;
-       seg += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+  const int64_t warps = (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5;
+  for (int64_t seg = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+       seg < n_segs; seg += warps) {
     const int64_t g_begin = seg * kPackSegment;
     const int64_t g_lim = g_begin + kPackSegment;
     const int g_end = static_cast<int>(g_lim < n_groups ? g_lim : n_groups);
-    uint32_t out = items ? seg_offsets[seg] : 0u;
+    const int n_here = g_end - static_cast<int>(g_begin);
+    int my_gs = 0, my_ge = 0, my_c = 0;
+    if (lane < n_here) {
+      my_gs = group_start[g_begin + lane];
+      my_ge = group_start[g_begin + lane + 1];
+      my_c = cands[g_begin + lane];
+    }
+    const uint32_t out = items ? seg_offsets[seg] : 0u;
     uint32_t count = 0;
     int cur_q0 = 0, cur_qn = 0, cur_g0 = 0, cur_gn = 0, cur_c = 0;
-    auto emit = [&](int q0, int qn, int g0, int gn, int flags) {
-      if (items) {
-        if (static_cast<int64_t>(out) + count < capacity)
-          items[out + count] = make_int4(q0, qn, g0, gn | flags);
-        else
-          raise_status(status, kStatusTable);
-      }
-      ++count;
+    auto put = [&](uint32_t slot, int q0, int qn, int g0, int gn, int flags) {
+      if (static_cast<int64_t>(out) + slot < capacity)
+        items[out + slot] = make_int4(q0, qn, g0, gn | flags);
+      else
+        raise_status(status, kStatusTable);
     };
     auto flush = [&]() {
-      if (cur_gn > 0) emit(cur_q0, cur_qn, cur_g0, cur_gn, 0);
+      if (cur_gn > 0) {
+        if (items && lane == 0) put(count, cur_q0, cur_qn, cur_g0, cur_gn, 0);
+        ++count;
+      }
       cur_qn = cur_gn = cur_c = 0;
     };
-    for (int g = static_cast<int>(g_begin); g < g_end; ++g) {
-      const int gs = group_start[g], ge = group_start[g + 1];
-      const int c = cands[g];
+    for (int j = 0; j < n_here; ++j) {
+      const int g = static_cast<int>(g_begin) + j;
+      const int gs = __shfl_sync(kFull, my_gs, j), ge = __shfl_sync(kFull, my_ge, j);
+      const int c = __shfl_sync(kFull, my_c, j);
       if (gs < 0 || ge > n_queries) {
-        if (items) raise_status(status, kStatusTable);
+        if (items && lane == 0) raise_status(status, kStatusTable);
         continue;
       }
       if (ge <= gs) continue;
       if (c > tile) {  // streams its candidates: items of its own
         flush();
-        for (int q = gs; q < ge; q += max_qc) emit(q, min(max_qc, ge - q), g, 1, kItemChunked);
+        const int n_it = (ge - gs + max_qc - 1) / max_qc;
+        if (items)
+          for (int t = lane; t < n_it; t += 32) {
+            const int q = gs + t * max_qc;
+            put(count + t, q, min(max_qc, ge - q), g, 1, kItemChunked);
+          }
+        count += n_it;
         continue;
       }
       int pos = gs;
@@ -103,7 +124,7 @@ __global__ void __launch_bounds__(256)
       }
     }
     flush();
-    if (!items) seg_counts[seg] = count;
+    if (!items && lane == 0) seg_counts[seg] = count;
   }
 }
 
@@ -176,8 +197,8 @@ int launch_items(const int2* runs, const int32_t* group_start, const int32_t* gr
   // grids for the host-side bound, capped: the device count drives the loops
   const int64_t gb = ceil_div(max_groups, 256);
   const int gblocks = static_cast<int>(gb < 2048 ? gb : 2048);
-  const int64_t sb = ceil_div(ceil_div(max_groups, kPackSegment), 256);
-  const int sblocks = static_cast<int>(sb < 1024 ? sb : 1024);
+  const int64_t sb = ceil_div(ceil_div(max_groups, kPackSegment), 8);  // 8 warps per block
+  const int sblocks = static_cast<int>(sb < 2048 ? sb : 2048);
   if (!cands_ready)  // else the caller's run kernel wrote cands[g] already
     k_group_cands<<<gblocks, 256, 0, s>>>(runs, group_row, group_count_ptr, cands, status);
   const int64_t capacity = static_cast<int64_t>(items_capacity(max_groups, n_queries));
