@@ -171,16 +171,16 @@ __device__ __forceinline__ Box6 box_reduce(Box6 box, int (*sh)[6]) {
   return box;
 }
 
-// 256 threads x 8 points.  Writes the parent cell and cloud of every point
-// and grows the per-cloud boxes.  Most tiles hold one or two clouds (offset
+// 256 threads x ppt points (1, 2, 4 or 8).  Writes the parent cell and cloud
+// of every point and grows the per-cloud boxes.  Most tiles hold one or two clouds (offset
 // batching): those are reduced in the block, other clouds go straight to
 // global atomics.
 __global__ void __launch_bounds__(256) k_bbox(PointSrc p, int4* __restrict__ pc,
-                                              int* __restrict__ bbox, Meta* meta) {
+                                              int* __restrict__ bbox, Meta* meta, int ppt) {
   __shared__ int sh[8][6];
   int* status = &meta->status;
-  const int64_t base = static_cast<int64_t>(blockIdx.x) * 2048;
-  const int64_t last = min(base + 2047, p.n - 1);
+  const int64_t base = static_cast<int64_t>(blockIdx.x) * 256 * ppt;
+  const int64_t last = min(base + 256 * ppt - 1, p.n - 1);
   const int b_lo = cloud_of(p, base, status);
   const int b_hi = cloud_of(p, last, status);
   // offset batching: a point of this tile below the end of b_lo is in b_lo,
@@ -192,7 +192,7 @@ __global__ void __launch_bounds__(256) k_bbox(PointSrc p, int4* __restrict__ pc,
   lo.reset();
   hi.reset();
 #pragma unroll 2
-  for (int r = 0; r < 8; ++r) {
+  for (int r = 0; r < ppt; ++r) {
     const int64_t i = base + r * 256 + threadIdx.x;
     if (i >= p.n) break;
     const int gx = grid_axis(p, i, 0, status) >> p.num_down;
@@ -300,7 +300,7 @@ __device__ __forceinline__ uint32_t hash_slot(uint64_t key, uint32_t mask) {
   return static_cast<uint32_t>(key) & mask;
 }
 
-// Warp-cooperative insertion of 2048 points per 256-thread CTA.  Lanes with
+// Warp-cooperative insertion of 256 x ppt points per CTA (ppt <= 8).  Lanes with
 // the same cell key elect one leader, which probes once and adds the group's
 // size to the cell count; slot_of[i] / rank_of[i] = the point's slot and its
 // rank in the cell.  cell_slot[id] = slot of cell id; *cell_count = cells.
@@ -308,7 +308,7 @@ __global__ void __launch_bounds__(256)
     k_cell_insert(const int4* __restrict__ pc, int64_t n, const int* __restrict__ bbox,
                   Meta* meta, HashSlot* __restrict__ table, uint32_t mask,
                   uint32_t* __restrict__ slot_of, uint32_t* __restrict__ rank_of,
-                  uint32_t* __restrict__ cell_slot, int* cell_count) {
+                  uint32_t* __restrict__ cell_slot, int* cell_count, int ppt) {
   __shared__ uint32_t s_new;
   __shared__ uint32_t s_base;
   __shared__ uint32_t s_list[2048];
@@ -316,9 +316,9 @@ __global__ void __launch_bounds__(256)
   __syncthreads();
   const int bpa = meta->bpa;
   const int lane = threadIdx.x & 31;
-  const int64_t base = static_cast<int64_t>(blockIdx.x) * 2048;
+  const int64_t base = static_cast<int64_t>(blockIdx.x) * 256 * ppt;
 #pragma unroll 2
-  for (int r = 0; r < 8; ++r) {
+  for (int r = 0; r < ppt; ++r) {
     const int64_t i = base + r * 256 + threadIdx.x;
     const bool valid = i < n;
     const unsigned vmask = __ballot_sync(kFull, valid);
@@ -363,18 +363,19 @@ __global__ void __launch_bounds__(256)
   for (uint32_t j = threadIdx.x; j < s_new; j += blockDim.x) cell_slot[s_base + j] = s_list[j];
 }
 
-// Points per 2048 cell ids (8 per thread): tile_counts[tile].
+// Points per 256 x ppt cell ids (ppt per thread): tile_counts[tile].
 __global__ void __launch_bounds__(256)
     k_cell_tiles(const int* cell_count_ptr, const uint32_t* __restrict__ cell_slot,
-                 const HashSlot* __restrict__ table, uint32_t* __restrict__ tile_counts) {
+                 const HashSlot* __restrict__ table, uint32_t* __restrict__ tile_counts, int ppt) {
   __shared__ uint32_t warp_sums[32];
   __shared__ uint32_t s_total;
   const int cells = *cell_count_ptr;
-  const int64_t base = static_cast<int64_t>(blockIdx.x) * 2048 + threadIdx.x * 8;
+  const int64_t base = (static_cast<int64_t>(blockIdx.x) * 256 + threadIdx.x) * ppt;
   uint32_t c = 0;
 #pragma unroll
   for (int r = 0; r < 8; ++r)
-    if (base + r < cells) c += static_cast<uint32_t>(table[cell_slot[base + r]].run.y);
+    if (r < ppt && base + r < cells)
+      c += static_cast<uint32_t>(table[cell_slot[base + r]].run.y);
   block_inclusive_scan(c, warp_sums, &s_total);
   if (threadIdx.x == 0) tile_counts[blockIdx.x] = s_total;
 }
@@ -386,16 +387,16 @@ __global__ void __launch_bounds__(256)
     k_cell_starts(const int* cell_count_ptr, const uint32_t* __restrict__ cell_slot,
                   HashSlot* __restrict__ table, const uint32_t* __restrict__ tile_offsets,
                   int64_t n, uint64_t* __restrict__ cell_key, int32_t* __restrict__ cell_start,
-                  uint32_t* __restrict__ slot_cell, uint32_t* __restrict__ zero_per_cell) {
+                  uint32_t* __restrict__ slot_cell, uint32_t* __restrict__ zero_per_cell, int ppt) {
   __shared__ uint32_t warp_sums[32];
   const int cells = *cell_count_ptr;
-  const int64_t base = static_cast<int64_t>(blockIdx.x) * 2048 + threadIdx.x * 8;
+  const int64_t base = (static_cast<int64_t>(blockIdx.x) * 256 + threadIdx.x) * ppt;
   uint32_t cnt[8], slot[8], sum = 0;
 #pragma unroll
   for (int r = 0; r < 8; ++r) {
     cnt[r] = 0u;
     slot[r] = 0u;
-    if (base + r < cells) {
+    if (r < ppt && base + r < cells) {
       slot[r] = cell_slot[base + r];
       cnt[r] = static_cast<uint32_t>(table[slot[r]].run.y);
     }
@@ -406,7 +407,7 @@ __global__ void __launch_bounds__(256)
 #pragma unroll
   for (int r = 0; r < 8; ++r) {
     const int64_t c = base + r;
-    if (c >= cells) break;
+    if (r >= ppt || c >= cells) break;
     HashSlot& hs = table[slot[r]];
     hs.run.x = static_cast<int>(start);
     cell_key[c] = hs.key - 1;
@@ -674,7 +675,7 @@ Bufs layout(void* ws, int64_t n, int64_t m, int64_t n_clouds, int kind, size_t* 
   b.slot_of = a.take<uint32_t>(nm);
   b.rank_of = a.take<uint32_t>(nm);
   b.cell_slot = a.take<uint32_t>(nm);
-  b.tile_counts = a.take<uint32_t>(static_cast<size_t>(ceil_div(nm > 0 ? nm : 1, 2048)));
+  b.tile_counts = a.take<uint32_t>(static_cast<size_t>(ceil_div(nm > 0 ? nm : 1, 256)));
   b.tile_counts2 = a.take<uint32_t>(static_cast<size_t>(ceil_div(nm > 0 ? nm : 1, 2048)));
   b.srec = a.take<float4>(n);
   b.cell_key = a.take<uint64_t>(n);
@@ -716,6 +717,25 @@ inline int blocks_for(int64_t n, int per_block) {
   return static_cast<int>(ceil_div(n > 0 ? n : 1, per_block));
 }
 
+// Points (or cells) per thread of the construction kernels: 8 once the
+// problem gives at least two 2048-point CTAs per SM, fewer for smaller
+// problems so that their CTAs still spread over the SMs instead of a few
+// threads walking eight points each.
+int points_per_thread(int64_t n) {
+  static int sms = 0;
+  if (sms == 0) {
+    int dev = 0, v = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess &&
+        cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess && v > 0)
+      sms = v;
+    else
+      return 8;
+  }
+  int ppt = 8;
+  while (ppt > 1 && ceil_div(n > 0 ? n : 1, 256 * ppt) < 2 * sms) ppt >>= 1;
+  return ppt;
+}
+
 // Grid for kernels whose real extent is only known on the device: enough
 // blocks to fill the GPU, a grid-stride loop covers the rest.
 inline int capped_blocks(int64_t upper_threads) {
@@ -751,14 +771,16 @@ int run_fused(const FusedArgs& f, void* ws, size_t ws_bytes, const QueryShape& s
   const float inv_voxel = 1.0f / f.voxel;  // host FP32 division, correctly rounded
   PointSrc ps{f.xyz, f.grid, f.batch, f.offsets, n_clouds, n, inv_voxel, f.num_down,
               f.sindex, f.n_src, f.trunc_grid};
+  const int ppt_s = points_per_thread(n);
   if (n > 0) {
-    k_bbox<<<blocks_for(n, 2048), 256, 0, s>>>(ps, b.pc_s, b.bbox, b.meta);
+    k_bbox<<<blocks_for(n, 256 * ppt_s), 256, 0, s>>>(ps, b.pc_s, b.bbox, b.meta, ppt_s);
     ++nl;
   }
   PointSrc pq{f.qxyz, nullptr, f.qbatch, f.qbatch ? nullptr : f.qoffsets, n_clouds, m, inv_voxel,
               f.num_down, nullptr, m, f.trunc_grid};
+  const int ppt_q = points_per_thread(m);
   if (kind == FKNN_QUERY_GENERAL && m > 0) {
-    k_bbox<<<blocks_for(m, 2048), 256, 0, s>>>(pq, b.pc_q, b.bbox, b.meta);
+    k_bbox<<<blocks_for(m, 256 * ppt_q), 256, 0, s>>>(pq, b.pc_q, b.bbox, b.meta, ppt_q);
     ++nl;
   }
   k_meta<<<1, 1024, 0, s>>>(b.bbox, n_clouds, b.meta);
@@ -772,13 +794,14 @@ int run_fused(const FusedArgs& f, void* ws, size_t ws_bytes, const QueryShape& s
       note_cuda_error(e);
       return FKNN_ERR_CUDA;
     }
-    const int tiles = blocks_for(n, 2048);
+    const int tiles = blocks_for(n, 256 * ppt_s);
     k_cell_insert<<<tiles, 256, 0, s>>>(b.pc_s, n, b.bbox, b.meta, b.hslots, hmask, b.slot_of,
-                                        b.rank_of, b.cell_slot, &b.meta->n_cells);
-    k_cell_tiles<<<tiles, 256, 0, s>>>(&b.meta->n_cells, b.cell_slot, b.hslots, b.tile_counts);
+                                        b.rank_of, b.cell_slot, &b.meta->n_cells, ppt_s);
+    k_cell_tiles<<<tiles, 256, 0, s>>>(&b.meta->n_cells, b.cell_slot, b.hslots, b.tile_counts,
+                                       ppt_s);
     k_scan_tiles<<<1, 1024, 0, s>>>(b.tile_counts, tiles, &b.meta->n_points_scanned);
     k_cell_starts<<<tiles, 256, 0, s>>>(&b.meta->n_cells, b.cell_slot, b.hslots, b.tile_counts, n,
-                                        b.cell_key, b.cell_start, b.slot_cell, b.qcount);
+                                        b.cell_key, b.cell_start, b.slot_cell, b.qcount, ppt_s);
     k_scatter<<<blocks_for(n, 256), 256, 0, s>>>(f.xyz, f.sindex, f.n_src, n, b.slot_of,
                                                  b.rank_of, b.hslots, b.slot_cell, b.srec,
                                                  b.pos_of, b.cell_of, &b.meta->status);
@@ -856,15 +879,15 @@ int run_fused(const FusedArgs& f, void* ws, size_t ws_bytes, const QueryShape& s
         return FKNN_ERR_CUDA;
       }
       const uint32_t qmask = static_cast<uint32_t>(b.qhash_cap - 1);
-      const int tiles = blocks_for(m, 2048);
+      const int tiles = blocks_for(m, 256 * ppt_q);
       k_cell_insert<<<tiles, 256, 0, s>>>(b.pc_q, m, b.bbox, b.meta, b.qslots, qmask, b.slot_of,
-                                          b.rank_of, b.cell_slot, &b.meta->n_groups);
+                                          b.rank_of, b.cell_slot, &b.meta->n_groups, ppt_q);
       k_cell_tiles<<<tiles, 256, 0, s>>>(&b.meta->n_groups, b.cell_slot, b.qslots,
-                                         b.tile_counts);
+                                         b.tile_counts, ppt_q);
       k_scan_tiles<<<1, 1024, 0, s>>>(b.tile_counts, tiles, &b.meta->n_points_scanned);
       k_cell_starts<<<tiles, 256, 0, s>>>(&b.meta->n_groups, b.cell_slot, b.qslots,
                                           b.tile_counts, m, b.group_key, b.group_start, nullptr,
-                                          nullptr);
+                                          nullptr, ppt_q);
       k_scatter<<<blocks_for(m, 256), 256, 0, s>>>(f.qxyz, nullptr, m, m, b.slot_of, b.rank_of,
                                                    b.qslots, nullptr, b.qrec, nullptr, nullptr,
                                                    &b.meta->status);
