@@ -9,6 +9,14 @@ nearest-point map from the full cloud to that level (``fknn_back_query``,
 K = 1), whose status words are combined on the device and read once.
 Output order and types follow the reference: ``forward + backward`` with
 int64 tensors.
+
+The caller's stream runs the chain of voxel-first levels; every level's self
+query and every back query only needs that level's points, so each runs on
+a side stream (a small pool per device) as soon as its level exists, while
+the chain goes on.  The caller's stream waits for all of them before the
+function returns, and every tensor handed between streams is recorded on
+the stream that uses it, so the caching allocator never reuses its memory
+early.
 """
 from __future__ import annotations
 
@@ -17,6 +25,20 @@ import math
 import torch
 
 from . import _lib, ops
+
+
+_SIDE: dict = {}
+_SIDE_STREAMS = 4
+
+
+def _side_streams(dev: torch.device) -> list:
+    """The side streams of a device (created once, reused by every call)."""
+    key = dev.index if dev.index is not None else torch.cuda.current_device()
+    pool = _SIDE.get(key)
+    if pool is None:
+        pool = [torch.cuda.Stream(device=dev) for _ in range(_SIDE_STREAMS)]
+        _SIDE[key] = pool
+    return pool
 
 
 def voxel_first(xyz: torch.Tensor, size: float, batch_idx: torch.Tensor | None = None
@@ -44,27 +66,57 @@ def build_flash_hierarchy(metric_xyz: torch.Tensor,
     full_xyz = metric_xyz.float().contiguous()
     current = full_xyz
     dev = full_xyz.device
+    main = torch.cuda.current_stream(dev)
+    side = _side_streams(dev)
     cumulative = torch.arange(len(full_xyz), device=dev)
     forward: list[torch.Tensor] = []
     levels: list[torch.Tensor] = []
+    made_on_side: list[torch.Tensor] = []
     for level, (size, k) in enumerate(zip(voxel_sizes, ks)):
         if level:
-            local = voxel_first(current, size)
+            local = voxel_first(current, size)   # reads the level's size back
             current = current[local].contiguous()
             cumulative = cumulative[local]
             forward.append(local)
             levels.append(cumulative)
-        offsets = torch.full((1,), len(current), dtype=torch.int64, device=dev)  # no host copy
-        idx, _ = ops.knn_offsets(current, offsets, int(k), float(size), exponent)
-        forward.append(idx.long())
+        s = side[level % len(side)]
+        s.wait_stream(main)
+        current.record_stream(s)
+        with torch.cuda.stream(s):
+            offsets = torch.full((1,), len(current), dtype=torch.int64, device=dev)
+            idx, _ = ops.knn_offsets(current, offsets, int(k), float(size), exponent)
+            nbr = idx.long()
+        forward.append(nbr)
+        made_on_side.append(nbr)
     backward: list[torch.Tensor] = []
-    # the back queries' status words are OR-ed on the device and read once
-    status = torch.zeros(1, dtype=torch.int32, device=dev)
-    for level in range(len(levels) - 1, -1, -1):
+    # every back query ORs its status word into its own flag; the flags are
+    # combined on the caller's stream and read once
+    flags: list[torch.Tensor] = []
+    for j, level in enumerate(range(len(levels) - 1, -1, -1)):
         size = voxel_sizes[level + 1]
-        idx, _, _ = ops.back_query(full_xyz, levels[level], size * 2, 1, status_into=status)
-        backward.append(idx[:, 0])
-    bits = int(status.item()) if levels else 0
+        # the streams of the smallest levels first: the first level's large
+        # self query keeps its stream busy the longest
+        s = side[(len(side) - 1 - j) % len(side)]
+        s.wait_stream(main)
+        full_xyz.record_stream(s)
+        levels[level].record_stream(s)
+        with torch.cuda.stream(s):
+            flag = torch.zeros(1, dtype=torch.int32, device=dev)
+            idx, _, _ = ops.back_query(full_xyz, levels[level], size * 2, 1, status_into=flag)
+            back = idx[:, 0]
+        flags.append(flag)
+        backward.append(back)
+        made_on_side.append(back)
+    for s in side:
+        main.wait_stream(s)
+    for t in made_on_side + flags:
+        t.record_stream(main)
+    bits = 0
+    if flags:
+        status = flags[0]
+        for f in flags[1:]:
+            status = status | f
+        bits = int(status.item())
     if bits & ~_lib.DEVICE_NO_CANDIDATES:
         raise _lib.FknnError(f"back_query: device reported {_lib.status_text(bits)}")
     if bits & _lib.DEVICE_NO_CANDIDATES:
