@@ -26,6 +26,30 @@ __device__ __forceinline__ void raise_status(int* status, int bit) {
   if (status) atomicOr(status, bit);
 }
 
+// ------------------------------------------- programmatic dependent launch
+// A kernel launched with launch_chained() may be scheduled while the kernel
+// before it in the stream is still finishing (its launch overlaps that
+// kernel's tail); it calls chain_wait() before it touches global memory,
+// which returns once the previous kernel has completed and its writes are
+// visible.  Launched the ordinary way, chain_wait() returns at once.
+__device__ __forceinline__ void chain_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_chained(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem,
+                                  cudaStream_t stream, Args... args) {
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = stream;
+  cudaLaunchAttribute attr{};
+  attr.id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr.val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = &attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
+}
+
 // ------------------------------------------------------------ morton codes
 // Interleave the low 16 bits of x, y, z: x bit b -> 3b+2, y -> 3b+1, z -> 3b.
 // Same bit layout as the reference's morton_key

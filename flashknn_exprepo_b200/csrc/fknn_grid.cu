@@ -118,6 +118,7 @@ __device__ __forceinline__ int cloud_of(const PointSrc& p, int64_t i, int* statu
 // ------------------------------------------------------------------ init
 
 __global__ void k_init(Meta* meta, int* bbox, int64_t n_clouds) {
+  chain_wait();
   const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
   if (t < static_cast<int64_t>(sizeof(Meta) / sizeof(int))) reinterpret_cast<int*>(meta)[t] = 0;
@@ -177,6 +178,7 @@ __device__ __forceinline__ Box6 box_reduce(Box6 box, int (*sh)[6]) {
 // global atomics.
 __global__ void __launch_bounds__(256) k_bbox(PointSrc p, int4* __restrict__ pc,
                                               int* __restrict__ bbox, Meta* meta, int ppt) {
+  chain_wait();
   __shared__ int sh[8][6];
   int* status = &meta->status;
   const int64_t base = static_cast<int64_t>(blockIdx.x) * 256 * ppt;
@@ -225,6 +227,7 @@ __global__ void __launch_bounds__(256) k_bbox(PointSrc p, int4* __restrict__ pc,
 // One CTA: bits per axis of the largest per-cloud extent, batch bits.
 __global__ void __launch_bounds__(1024) k_meta(const int* __restrict__ bbox, int64_t n_clouds,
                                                Meta* meta) {
+  chain_wait();
   __shared__ int s_ext[32], s_b[32];
   int ext = 0, maxb = 0;
   for (int64_t c = threadIdx.x; c < n_clouds; c += blockDim.x) {
@@ -309,6 +312,7 @@ __global__ void __launch_bounds__(256)
                   Meta* meta, HashSlot* __restrict__ table, uint32_t mask,
                   uint32_t* __restrict__ slot_of, uint32_t* __restrict__ rank_of,
                   uint32_t* __restrict__ cell_slot, int* cell_count, int ppt) {
+  chain_wait();
   __shared__ uint32_t s_new;
   __shared__ uint32_t s_base;
   __shared__ uint32_t s_list[2048];
@@ -367,6 +371,7 @@ __global__ void __launch_bounds__(256)
 __global__ void __launch_bounds__(256)
     k_cell_tiles(const int* cell_count_ptr, const uint32_t* __restrict__ cell_slot,
                  const HashSlot* __restrict__ table, uint32_t* __restrict__ tile_counts, int ppt) {
+  chain_wait();
   __shared__ uint32_t warp_sums[32];
   __shared__ uint32_t s_total;
   const int cells = *cell_count_ptr;
@@ -388,6 +393,7 @@ __global__ void __launch_bounds__(256)
                   HashSlot* __restrict__ table, const uint32_t* __restrict__ tile_offsets,
                   int64_t n, uint64_t* __restrict__ cell_key, int32_t* __restrict__ cell_start,
                   uint32_t* __restrict__ slot_cell, uint32_t* __restrict__ zero_per_cell, int ppt) {
+  chain_wait();
   __shared__ uint32_t warp_sums[32];
   const int cells = *cell_count_ptr;
   const int64_t base = (static_cast<int64_t>(blockIdx.x) * 256 + threadIdx.x) * ppt;
@@ -427,6 +433,7 @@ __global__ void __launch_bounds__(256)
               const HashSlot* __restrict__ table, const uint32_t* __restrict__ slot_cell,
               float4* __restrict__ rec, int32_t* __restrict__ pos_of,
               int32_t* __restrict__ cell_of, int* status) {
+  chain_wait();
   const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const uint32_t slot = slot_of[i];
@@ -471,6 +478,7 @@ __global__ void __launch_bounds__(256)
            const HashSlot* __restrict__ table, uint32_t hmask, const int* cell_count_ptr,
            Meta* meta, int2* __restrict__ runs, int32_t* __restrict__ cands,
            int* status) {
+  chain_wait();
   __shared__ unsigned long long block_total;
   if (threadIdx.x == 0) block_total = 0ull;
   __syncthreads();
@@ -529,6 +537,7 @@ __global__ void __launch_bounds__(256)
                 const int32_t* __restrict__ pos_of, const int32_t* __restrict__ cell_of,
                 Meta* meta, uint32_t* __restrict__ qcount, uint32_t* __restrict__ cell_r,
                 uint32_t* __restrict__ rank_r) {
+  chain_wait();
   const int64_t r = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   const bool valid = r < m;
   const unsigned vmask = __ballot_sync(kFull, valid);
@@ -553,6 +562,7 @@ __global__ void __launch_bounds__(256)
 __global__ void __launch_bounds__(256)
     k_sel_tiles(const int* cell_count_ptr, const uint32_t* __restrict__ qcount,
                 uint32_t* __restrict__ tile_groups, uint32_t* __restrict__ tile_queries) {
+  chain_wait();
   __shared__ uint32_t warp_sums[32];
   __shared__ uint32_t s_total;
   const int cells = *cell_count_ptr;
@@ -578,6 +588,7 @@ __global__ void __launch_bounds__(256)
                  const uint32_t* __restrict__ tile_goff, const uint32_t* __restrict__ tile_qoff,
                  int64_t m, const int* group_count_ptr, int32_t* __restrict__ group_start,
                  int32_t* __restrict__ group_row, uint32_t* __restrict__ qstart) {
+  chain_wait();
   __shared__ uint32_t warp_sums[32];
   const int cells = *cell_count_ptr;
   const int64_t base = static_cast<int64_t>(blockIdx.x) * 2048 + threadIdx.x * 8;
@@ -613,6 +624,7 @@ __global__ void __launch_bounds__(256)
                   const int32_t* __restrict__ pos_of, const float4* __restrict__ srec,
                   const uint32_t* __restrict__ cell_r, const uint32_t* __restrict__ rank_r,
                   const uint32_t* __restrict__ qstart, float4* __restrict__ qrec, int* status) {
+  chain_wait();
   const int64_t r = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (r >= m) return;
   int64_t qi = query_indices[r];
@@ -765,7 +777,7 @@ int run_fused(const FusedArgs& f, void* ws, size_t ws_bytes, const QueryShape& s
   cudaError_t e;
   const uint32_t hmask = static_cast<uint32_t>(b.hash_cap - 1);
 
-  k_init<<<64, 256, 0, s>>>(b.meta, b.bbox, n_clouds);
+  launch_chained(k_init, 64, 256, 0, s, b.meta, b.bbox, n_clouds);
   ++nl;
 
   const float inv_voxel = 1.0f / f.voxel;  // host FP32 division, correctly rounded
@@ -773,17 +785,19 @@ int run_fused(const FusedArgs& f, void* ws, size_t ws_bytes, const QueryShape& s
               f.sindex, f.n_src, f.trunc_grid};
   const int ppt_s = points_per_thread(n);
   if (n > 0) {
-    k_bbox<<<blocks_for(n, 256 * ppt_s), 256, 0, s>>>(ps, b.pc_s, b.bbox, b.meta, ppt_s);
+    launch_chained(k_bbox, blocks_for(n, 256 * ppt_s), 256, 0, s, ps, b.pc_s, b.bbox, b.meta,
+                   ppt_s);
     ++nl;
   }
   PointSrc pq{f.qxyz, nullptr, f.qbatch, f.qbatch ? nullptr : f.qoffsets, n_clouds, m, inv_voxel,
               f.num_down, nullptr, m, f.trunc_grid};
   const int ppt_q = points_per_thread(m);
   if (kind == FKNN_QUERY_GENERAL && m > 0) {
-    k_bbox<<<blocks_for(m, 256 * ppt_q), 256, 0, s>>>(pq, b.pc_q, b.bbox, b.meta, ppt_q);
+    launch_chained(k_bbox, blocks_for(m, 256 * ppt_q), 256, 0, s, pq, b.pc_q, b.bbox, b.meta,
+                   ppt_q);
     ++nl;
   }
-  k_meta<<<1, 1024, 0, s>>>(b.bbox, n_clouds, b.meta);
+  launch_chained(k_meta, 1, 1024, 0, s, b.bbox, n_clouds, b.meta);
   ++nl;
 
   // --- support cells
@@ -795,16 +809,15 @@ int run_fused(const FusedArgs& f, void* ws, size_t ws_bytes, const QueryShape& s
       return FKNN_ERR_CUDA;
     }
     const int tiles = blocks_for(n, 256 * ppt_s);
-    k_cell_insert<<<tiles, 256, 0, s>>>(b.pc_s, n, b.bbox, b.meta, b.hslots, hmask, b.slot_of,
-                                        b.rank_of, b.cell_slot, &b.meta->n_cells, ppt_s);
-    k_cell_tiles<<<tiles, 256, 0, s>>>(&b.meta->n_cells, b.cell_slot, b.hslots, b.tile_counts,
-                                       ppt_s);
-    k_scan_tiles<<<1, 1024, 0, s>>>(b.tile_counts, tiles, &b.meta->n_points_scanned);
-    k_cell_starts<<<tiles, 256, 0, s>>>(&b.meta->n_cells, b.cell_slot, b.hslots, b.tile_counts, n,
-                                        b.cell_key, b.cell_start, b.slot_cell, b.qcount, ppt_s);
-    k_scatter<<<blocks_for(n, 256), 256, 0, s>>>(f.xyz, f.sindex, f.n_src, n, b.slot_of,
-                                                 b.rank_of, b.hslots, b.slot_cell, b.srec,
-                                                 b.pos_of, b.cell_of, &b.meta->status);
+    launch_chained(k_cell_insert, tiles, 256, 0, s, b.pc_s, n, b.bbox, b.meta, b.hslots, hmask,
+                   b.slot_of, b.rank_of, b.cell_slot, &b.meta->n_cells, ppt_s);
+    launch_chained(k_cell_tiles, tiles, 256, 0, s,
+        &b.meta->n_cells, b.cell_slot, b.hslots, b.tile_counts, ppt_s);
+    launch_chained(k_scan_tiles, 1, 1024, 0, s, b.tile_counts, tiles, &b.meta->n_points_scanned);
+    launch_chained(k_cell_starts, tiles, 256, 0, s, &b.meta->n_cells, b.cell_slot, b.hslots,
+                   b.tile_counts, n, b.cell_key, b.cell_start, b.slot_cell, b.qcount, ppt_s);
+    launch_chained(k_scatter, blocks_for(n, 256), 256, 0, s, f.xyz, f.sindex, f.n_src, n, b.slot_of,
+        b.rank_of, b.hslots, b.slot_cell, b.srec, b.pos_of, b.cell_of, &b.meta->status);
     nl += 5;
   }
 
@@ -819,9 +832,9 @@ int run_fused(const FusedArgs& f, void* ws, size_t ws_bytes, const QueryShape& s
 
   if (kind == FKNN_QUERY_SELF) {
     if (n > 0) {
-      k_runs<<<capped_blocks(n * 32), 256, 0, s>>>(b.cell_key, &b.meta->n_cells, b.hslots, hmask,
-                                                   &b.meta->n_cells, b.meta, b.runs, b.cands,
-                                                   &b.meta->status);
+      launch_chained(k_runs, capped_blocks(n * 32), 256, 0, s, b.cell_key, &b.meta->n_cells,
+                     b.hslots, hmask, &b.meta->n_cells, b.meta, b.runs, b.cands,
+                     &b.meta->status);
       ++nl;
       nl += launch_items(b.runs, b.cell_start, nullptr, &b.meta->n_cells, n, shape.tile_records,
                          b.cands, b.seg_counts, &b.meta->n_items, b.items, s, &b.meta->status, n,
@@ -836,27 +849,26 @@ int run_fused(const FusedArgs& f, void* ws, size_t ws_bytes, const QueryShape& s
     group_row = b.group_row;
     group_count_ptr = &b.meta->n_groups;
     if (n > 0) {
-      k_runs<<<capped_blocks(n * 32), 256, 0, s>>>(b.cell_key, &b.meta->n_cells, b.hslots, hmask,
-                                                   &b.meta->n_cells, b.meta, b.runs, nullptr,
-                                                   nullptr);
+      launch_chained(k_runs, capped_blocks(n * 32), 256, 0, s, b.cell_key,
+          &b.meta->n_cells, b.hslots, hmask, &b.meta->n_cells, b.meta, b.runs, nullptr, nullptr);
       ++nl;
     }
     if (m > 0 && n > 0) {
       // per-query cell and rank in slot_of / rank_of (free again once the
       // support records are written)
       const int ctiles = blocks_for(n, 2048);
-      k_sel_count<<<blocks_for(m, 256), 256, 0, s>>>(f.query_indices, m, n, b.pos_of, b.cell_of,
-                                                     b.meta, b.qcount, b.slot_of, b.rank_of);
-      k_sel_tiles<<<ctiles, 256, 0, s>>>(&b.meta->n_cells, b.qcount, b.tile_counts,
-                                         b.tile_counts2);
-      k_scan_tiles<<<1, 1024, 0, s>>>(b.tile_counts, ctiles, &b.meta->n_groups);
-      k_scan_tiles<<<1, 1024, 0, s>>>(b.tile_counts2, ctiles, &b.meta->n_points_scanned);
-      k_sel_starts<<<ctiles, 256, 0, s>>>(&b.meta->n_cells, b.qcount, b.tile_counts,
-                                          b.tile_counts2, m, &b.meta->n_groups, b.group_start,
-                                          b.group_row, b.qstart);
-      k_sel_scatter<<<blocks_for(m, 256), 256, 0, s>>>(m, n, f.query_indices, b.pos_of, b.srec,
-                                                       b.slot_of, b.rank_of, b.qstart, b.qrec,
-                                                       &b.meta->status);
+      launch_chained(k_sel_count, blocks_for(m, 256), 256, 0, s, f.query_indices, m, n, b.pos_of,
+          b.cell_of, b.meta, b.qcount, b.slot_of, b.rank_of);
+      launch_chained(k_sel_tiles, ctiles, 256, 0, s,
+          &b.meta->n_cells, b.qcount, b.tile_counts, b.tile_counts2);
+      launch_chained(k_scan_tiles, 1, 1024, 0, s, b.tile_counts, ctiles, &b.meta->n_groups);
+      launch_chained(k_scan_tiles, 1, 1024, 0, s, b.tile_counts2, ctiles,
+                     &b.meta->n_points_scanned);
+      launch_chained(k_sel_starts, ctiles, 256, 0, s, &b.meta->n_cells, b.qcount, b.tile_counts,
+                     b.tile_counts2, m, &b.meta->n_groups, b.group_start, b.group_row,
+                     b.qstart);
+      launch_chained(k_sel_scatter, blocks_for(m, 256), 256, 0, s, m, n, f.query_indices, b.pos_of,
+          b.srec, b.slot_of, b.rank_of, b.qstart, b.qrec, &b.meta->status);
       nl += 6;
       nl += launch_items(b.runs, b.group_start, b.group_row, &b.meta->n_groups, m,
                          shape.tile_records, b.cands, b.seg_counts, &b.meta->n_items, b.items, s,
@@ -880,21 +892,19 @@ int run_fused(const FusedArgs& f, void* ws, size_t ws_bytes, const QueryShape& s
       }
       const uint32_t qmask = static_cast<uint32_t>(b.qhash_cap - 1);
       const int tiles = blocks_for(m, 256 * ppt_q);
-      k_cell_insert<<<tiles, 256, 0, s>>>(b.pc_q, m, b.bbox, b.meta, b.qslots, qmask, b.slot_of,
-                                          b.rank_of, b.cell_slot, &b.meta->n_groups, ppt_q);
-      k_cell_tiles<<<tiles, 256, 0, s>>>(&b.meta->n_groups, b.cell_slot, b.qslots,
-                                         b.tile_counts, ppt_q);
-      k_scan_tiles<<<1, 1024, 0, s>>>(b.tile_counts, tiles, &b.meta->n_points_scanned);
-      k_cell_starts<<<tiles, 256, 0, s>>>(&b.meta->n_groups, b.cell_slot, b.qslots,
-                                          b.tile_counts, m, b.group_key, b.group_start, nullptr,
-                                          nullptr, ppt_q);
-      k_scatter<<<blocks_for(m, 256), 256, 0, s>>>(f.qxyz, nullptr, m, m, b.slot_of, b.rank_of,
-                                                   b.qslots, nullptr, b.qrec, nullptr, nullptr,
-                                                   &b.meta->status);
+      launch_chained(k_cell_insert, tiles, 256, 0, s, b.pc_q, m, b.bbox, b.meta, b.qslots, qmask,
+          b.slot_of, b.rank_of, b.cell_slot, &b.meta->n_groups, ppt_q);
+      launch_chained(k_cell_tiles, tiles, 256, 0, s,
+          &b.meta->n_groups, b.cell_slot, b.qslots, b.tile_counts, ppt_q);
+      launch_chained(k_scan_tiles, 1, 1024, 0, s, b.tile_counts, tiles, &b.meta->n_points_scanned);
+      launch_chained(k_cell_starts, tiles, 256, 0, s, &b.meta->n_groups, b.cell_slot, b.qslots,
+                     b.tile_counts, m, b.group_key, b.group_start, nullptr, nullptr, ppt_q);
+      launch_chained(k_scatter, blocks_for(m, 256), 256, 0, s, f.qxyz, nullptr, m, m, b.slot_of,
+          b.rank_of, b.qslots, nullptr, b.qrec, nullptr, nullptr, &b.meta->status);
       nl += 5;
-      k_runs<<<capped_blocks(m * 32), 256, 0, s>>>(b.group_key, &b.meta->n_groups, b.hslots, hmask,
-                                                   &b.meta->n_cells, b.meta, b.runs, b.cands,
-                                                   &b.meta->status);
+      launch_chained(k_runs, capped_blocks(m * 32), 256, 0, s, b.group_key, &b.meta->n_groups,
+                     b.hslots, hmask, &b.meta->n_cells, b.meta, b.runs, b.cands,
+                     &b.meta->status);
       ++nl;
       nl += launch_items(b.runs, b.group_start, nullptr, &b.meta->n_groups, m, shape.tile_records,
                          b.cands, b.seg_counts, &b.meta->n_items, b.items, s, &b.meta->status, m,

@@ -23,6 +23,7 @@ namespace fknn {
 __global__ void __launch_bounds__(256)
     k_group_cands(const int2* __restrict__ runs, const int32_t* __restrict__ group_row,
                   const int* group_count_ptr, int32_t* __restrict__ cands, int* status) {
+  chain_wait();
   const int n_groups = *group_count_ptr;
   for (int64_t g = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; g < n_groups;
        g += static_cast<int64_t>(gridDim.x) * blockDim.x) {
@@ -53,6 +54,7 @@ __global__ void __launch_bounds__(256)
            const int* group_count_ptr, int tile, int max_q, int max_qc, int64_t n_queries,
            int64_t capacity, uint32_t* __restrict__ seg_counts,
            const uint32_t* __restrict__ seg_offsets, int4* __restrict__ items, int* status) {
+  chain_wait();
   const int lane = threadIdx.x & 31;
   const int n_groups = *group_count_ptr;
   const int64_t n_segs = (n_groups + kPackSegment - 1) / kPackSegment;
@@ -134,6 +136,7 @@ __global__ void __launch_bounds__(256)
 __global__ void __launch_bounds__(1024)
     k_scan_segments(uint32_t* __restrict__ seg_counts, const int* group_count_ptr,
                     int64_t capacity, int* __restrict__ total_out, int* status) {
+  chain_wait();
   __shared__ uint32_t warp_sums[32];
   __shared__ uint32_t s_total;
   const int n_segs = (*group_count_ptr + kPackSegment - 1) / kPackSegment;
@@ -200,15 +203,17 @@ int launch_items(const int2* runs, const int32_t* group_start, const int32_t* gr
   const int64_t sb = ceil_div(ceil_div(max_groups, kPackSegment), 8);  // 8 warps per block
   const int sblocks = static_cast<int>(sb < 2048 ? sb : 2048);
   if (!cands_ready)  // else the caller's run kernel wrote cands[g] already
-    k_group_cands<<<gblocks, 256, 0, s>>>(runs, group_row, group_count_ptr, cands, status);
+    launch_chained(k_group_cands, gblocks, 256, 0, s, runs, group_row, group_count_ptr, cands,
+        status);
   const int64_t capacity = static_cast<int64_t>(items_capacity(max_groups, n_queries));
   const int max_q = item_query_cap(n_queries);
   const int max_qc = chunked_query_cap(n_queries);
-  k_pack<<<sblocks, 256, 0, s>>>(group_start, cands, group_count_ptr, tile, max_q, max_qc,
-                                 n_queries, capacity, seg_counts, nullptr, nullptr, status);
-  k_scan_segments<<<1, 1024, 0, s>>>(seg_counts, group_count_ptr, capacity, n_items_ptr, status);
-  k_pack<<<sblocks, 256, 0, s>>>(group_start, cands, group_count_ptr, tile, max_q, max_qc,
-                                 n_queries, capacity, nullptr, seg_counts, items, status);
+  launch_chained(k_pack, sblocks, 256, 0, s, group_start, cands, group_count_ptr, tile, max_q,
+      max_qc, n_queries, capacity, seg_counts, nullptr, nullptr, status);
+  launch_chained(k_scan_segments, 1, 1024, 0, s, seg_counts, group_count_ptr, capacity, n_items_ptr,
+      status);
+  launch_chained(k_pack, sblocks, 256, 0, s, group_start, cands, group_count_ptr, tile, max_q,
+      max_qc, n_queries, capacity, nullptr, seg_counts, items, status);
   return cands_ready ? 3 : 4;
 }
 

@@ -794,6 +794,7 @@ __device__ __noinline__ void drain_after_timeout(Meta* meta, const WarpSmem& w, 
 template <int KCAP, bool EXACT, typename IdxT>
 __global__ void __maxnreg__(query_max_regs<KCAP>())
     k_query(const __grid_constant__ QueryLaunch a, int T, int min_cands_per_lane, int depth) {
+  chain_wait();
   extern __shared__ __align__(128) unsigned char smem_raw[];
   const int lane = threadIdx.x & 31;
   const WarpSmem w = warp_smem(smem_raw, T, depth);
@@ -937,8 +938,8 @@ int launch_t(const QueryLaunch& q, const QueryShape& shape, cudaStream_t s) {
   const int per_sm = shape.ctas_per_sm > 0 ? shape.ctas_per_sm : use.per_sm;
   const int grid = use.sms * per_sm;
   const int slot = profile_start(s);
-  kern<<<grid, threads, smem, s>>>(q, shape.tile_records, shape.min_candidates_per_lane,
-                                   shape.staging_depth);
+  launch_chained(kern, grid, threads, smem, s, q, shape.tile_records, shape.min_candidates_per_lane,
+      shape.staging_depth);
   e = cudaGetLastError();
   profile_stop(slot, s);
   return e;

@@ -31,6 +31,7 @@ template <typename KeyT>
 __global__ void __launch_bounds__(kSortThreads)
     k_sort_hist(const KeyT* __restrict__ keys, int64_t n, int pass, const int* nbits,
                 uint32_t* __restrict__ hist, uint32_t* __restrict__ totals, int n_tiles) {
+  chain_wait();
   if (pass * 8 >= *nbits) return;
   __shared__ uint32_t sh[256];
   sh[threadIdx.x] = 0;
@@ -88,6 +89,7 @@ __device__ __forceinline__ uint32_t block_inclusive_scan(uint32_t v, uint32_t* w
 static __global__ void __launch_bounds__(1024)
     k_sort_scan(uint32_t* __restrict__ hist, const uint32_t* __restrict__ totals, int n_tiles,
                 int pass, const int* nbits) {
+  chain_wait();
   if (pass * 8 >= *nbits) return;
   __shared__ uint32_t warp_sums[32];
   __shared__ uint32_t s_total;
@@ -110,6 +112,7 @@ __global__ void __launch_bounds__(kSortThreads)
     k_sort_scatter(const KeyT* __restrict__ kin, const uint32_t* __restrict__ vin,
                    KeyT* __restrict__ kout, uint32_t* __restrict__ vout, int64_t n, int pass,
                    const int* nbits, const uint32_t* __restrict__ offsets, int n_tiles) {
+  chain_wait();
   if (pass * 8 >= *nbits) return;
   constexpr int kWarps = kSortThreads / 32;
   __shared__ uint32_t cnt[kWarps][256];
@@ -215,6 +218,7 @@ inline size_t sort_hist_elems(int64_t n) {
 // per-item flags and adds its tile offset.
 static __global__ void __launch_bounds__(1024)
     k_scan_tiles(uint32_t* __restrict__ tile_counts, int n_tiles, int* __restrict__ total_out) {
+  chain_wait();
   __shared__ uint32_t warp_sums[32];
   __shared__ uint32_t s_total;
   uint32_t carry = 0;
