@@ -87,9 +87,22 @@ size_t items_capacity(int64_t max_groups, int64_t n_queries);
 // Bounded-wait self-test (fknn_selftest.cu): arms a barrier that never
 // completes and waits at most `limit` polls; sets kStatusTimeout.
 int run_selftest_wait(void* ws, size_t ws_bytes, uint32_t limit, cudaStream_t s);
+// Groups per packing segment (one warp walks a segment's groups in order):
+// kPackSegment for a large problem; a problem of fewer than
+// kPackSegment * kPackWarps groups uses shorter segments (at least
+// kPackSegmentMin groups), so its few groups still spread over about
+// kPackWarps warps and no warp walks a long serial chain.
 constexpr int kPackSegment = 16;
+constexpr int kPackSegmentMin = 4;
+constexpr int kPackWarps = 4096;
+__host__ __device__ inline int pack_segment_len(int n_groups) {
+  if (n_groups >= kPackSegment * kPackWarps) return kPackSegment;
+  const int len = n_groups / kPackWarps;
+  return len < kPackSegmentMin ? kPackSegmentMin : len;
+}
+// Segment counts to allocate for up to max_groups groups (every length).
 inline int64_t pack_segments(int64_t max_groups) {
-  return (max_groups + kPackSegment - 1) / kPackSegment;
+  return (max_groups + kPackSegmentMin - 1) / kPackSegmentMin;
 }
 
 // Bump allocator over a caller-provided workspace (256-byte aligned slices).

@@ -9,7 +9,8 @@
 // stream their candidates tile by tile.
 //
 // Packing is a sequential greedy pass over the groups in key order; it runs
-// in parallel over segments of kPackSegment groups (one warp each): a
+// in parallel over segments of consecutive groups (one warp each; the
+// segment length follows the group count, see pack_segment_len): a
 // count pass, a scan of the per-segment counts, and a write pass.  Items
 // therefore keep the spatial order of the groups.
 #include "fknn_common.cuh"
@@ -37,7 +38,7 @@ __global__ void __launch_bounds__(256)
   }
 }
 
-// One warp per segment of kPackSegment groups.  With items == nullptr it
+// One warp per segment of consecutive groups.  With items == nullptr it
 // only counts (seg_counts[seg]); otherwise it writes its items at
 // seg_offsets[seg].  Item = (q_start, q_count, g_first, g_count | flags).
 // The segment's group ranges and candidate counts are loaded once (one
@@ -57,12 +58,13 @@ __global__ void __launch_bounds__(256)
   chain_wait();
   const int lane = threadIdx.x & 31;
   const int n_groups = *group_count_ptr;
-  const int64_t n_segs = (n_groups + kPackSegment - 1) / kPackSegment;
+  const int seg_len = pack_segment_len(n_groups);
+  const int64_t n_segs = (n_groups + seg_len - 1) / seg_len;
   const int64_t warps = (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5;
   for (int64_t seg = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
        seg < n_segs; seg += warps) {
-    const int64_t g_begin = seg * kPackSegment;
-    const int64_t g_lim = g_begin + kPackSegment;
+    const int64_t g_begin = seg * seg_len;
+    const int64_t g_lim = g_begin + seg_len;
     const int g_end = static_cast<int>(g_lim < n_groups ? g_lim : n_groups);
     const int n_here = g_end - static_cast<int>(g_begin);
     int my_gs = 0, my_ge = 0, my_c = 0;
@@ -139,7 +141,9 @@ __global__ void __launch_bounds__(1024)
   chain_wait();
   __shared__ uint32_t warp_sums[32];
   __shared__ uint32_t s_total;
-  const int n_segs = (*group_count_ptr + kPackSegment - 1) / kPackSegment;
+  const int n_groups = *group_count_ptr;
+  const int seg_len = pack_segment_len(n_groups);
+  const int n_segs = (n_groups + seg_len - 1) / seg_len;
   uint32_t carry = 0;
   for (int t0 = 0; t0 < n_segs; t0 += blockDim.x) {
     const int t = t0 + threadIdx.x;
@@ -200,7 +204,7 @@ int launch_items(const int2* runs, const int32_t* group_start, const int32_t* gr
   // grids for the host-side bound, capped: the device count drives the loops
   const int64_t gb = ceil_div(max_groups, 256);
   const int gblocks = static_cast<int>(gb < 2048 ? gb : 2048);
-  const int64_t sb = ceil_div(ceil_div(max_groups, kPackSegment), 8);  // 8 warps per block
+  const int64_t sb = ceil_div(pack_segments(max_groups), 8);  // 8 warps per block
   const int sblocks = static_cast<int>(sb < 2048 ? sb : 2048);
   if (!cands_ready)  // else the caller's run kernel wrote cands[g] already
     launch_chained(k_group_cands, gblocks, 256, 0, s, runs, group_row, group_count_ptr, cands,
