@@ -51,6 +51,8 @@ def parse_args():
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the per-cloud, fwd+bwd and CPU-baseline legs")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer e2e leg")
+    ap.add_argument("--small-rows", action="store_true",
+                    help="only the uniform-cube and hierarchy rows (profiling)")
     ap.add_argument("--rows-only", action="store_true",
                     help="only the per-path rows and one distance backward (profiling)")
     ap.add_argument("--no-tune", action="store_true",
@@ -526,6 +528,39 @@ def _event_ms(torch, fn, flush, reps=5):
     return total / reps
 
 
+def row_hierarchy(fk, torch, dev):
+    """The DeLA hierarchy builder (4 levels, K=24, alpha 16) on the
+    voxel-first LiDAR scan: wall clock of one call, mean of 3."""
+    from flashknn_exprepo_b200 import hierarchy, synthetic
+    T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)  # noqa: E731
+    lid = T(synthetic.lidar(dedup=True))
+    hierarchy.build_flash_hierarchy(lid)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(3):
+        hierarchy.build_flash_hierarchy(lid)
+    torch.cuda.synchronize()
+    return {"value": (time.perf_counter() - t0) / 3 * 1e3, "unit": "ms",
+            "n_points": int(lid.shape[0]),
+            "what": "wall clock incl. one count read-back per level"}
+
+
+def row_cube(fk, torch, dev, flush):
+    """The uniform cube (16,384 points, K=16): one self-query call, eager and
+    replayed from its cached CUDA graph."""
+    from flashknn_exprepo_b200 import synthetic
+    T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)  # noqa: E731
+    cube = T(synthetic.uniform_cube())
+    co = torch.tensor([cube.shape[0]], device=dev)
+    ms = _event_ms(torch, lambda: fk.ops.knn_offsets(cube, co, 16, synthetic.C1_VOXEL, 2), flush)
+    gms = _event_ms(torch, lambda: fk.ops.knn_offsets(cube, co, 16, synthetic.C1_VOXEL, 2,
+                                                      graph=True), flush)
+    return {"value": cube.shape[0] / (ms * 1e-3), "unit": "queries/s",
+            "ms": ms, "n_points": int(cube.shape[0]), "graph_ms": gms,
+            "graph": "the same call with graph=True (a cached CUDA graph of the pipeline "
+                     "replayed)"}
+
+
 def rows_single_gpu(fk, torch, dev, flush, peak_gbs, clouds=16):
     """The paths around the batched query, each on its own workload:
     adaptive-neighbourhood query (LiDAR scan), back query and voxel-first
@@ -535,7 +570,7 @@ def rows_single_gpu(fk, torch, dev, flush, peak_gbs, clouds=16):
     uniform cube at K=16, the LiDAR scan at alpha 4 and 8, and neighbour
     feature grouping (16-cloud batch, 64 channels, forward with its HBM
     roofline, and backward)."""
-    from flashknn_exprepo_b200 import hierarchy, synthetic
+    from flashknn_exprepo_b200 import synthetic
     T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)  # noqa: E731
     rows = {}
     # adaptive neighbourhood, LiDAR scan ~118k points, K=16
@@ -589,17 +624,7 @@ def rows_single_gpu(fk, torch, dev, flush, peak_gbs, clouds=16):
     rows["back_query_batch_k1"] = {"value": len(b.xyz) / (ms * 1e-3), "unit": "queries/s",
                                    "ms": ms, "subset_points": int(sel.numel()),
                                    "query_grid_m": 0.2}
-    # DeLA hierarchy (4 levels, K=24, alpha 16) on the voxel-first LiDAR scan
-    lid = T(synthetic.lidar(dedup=True))
-    hierarchy.build_flash_hierarchy(lid)
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    for _ in range(3):
-        hierarchy.build_flash_hierarchy(lid)
-    torch.cuda.synchronize()
-    rows["hierarchy_lidar"] = {"value": (time.perf_counter() - t0) / 3 * 1e3, "unit": "ms",
-                               "n_points": int(lid.shape[0]),
-                               "what": "wall clock incl. one count read-back per level"}
+    rows["hierarchy_lidar"] = row_hierarchy(fk, torch, dev)
     # radius-limited query, room ~80k points, K=32, r=0.1 m
     room = T(synthetic.room())
     ro = torch.tensor([room.shape[0]], device=dev)
@@ -662,17 +687,7 @@ def rows_single_gpu(fk, torch, dev, flush, peak_gbs, clouds=16):
     nms = _event_ms(torch, lambda: fk.ops.morton_neighbor_keys(pgrid), flush)
     rows["morton_room"] = {"value": ms, "unit": "ms", "neighbor_keys_ms": nms,
                            "n_points": int(rgrid.shape[0]), "n_parents": int(pgrid.shape[0])}
-    # uniform cube (C1), 16,384 points, K=16
-    cube = T(synthetic.uniform_cube())
-    co = torch.tensor([cube.shape[0]], device=dev)
-    ms = _event_ms(torch, lambda: fk.ops.knn_offsets(cube, co, 16, synthetic.C1_VOXEL, 2), flush)
-    gms = _event_ms(torch, lambda: fk.ops.knn_offsets(cube, co, 16, synthetic.C1_VOXEL, 2,
-                                                      graph=True), flush)
-    rows["self_query_cube_k16"] = {"value": cube.shape[0] / (ms * 1e-3), "unit": "queries/s",
-                                   "ms": ms, "n_points": int(cube.shape[0]),
-                                   "graph_ms": gms,
-                                   "graph": "the same call with graph=True (a cached CUDA graph "
-                                            "of the pipeline replayed)"}
+    rows["self_query_cube_k16"] = row_cube(fk, torch, dev, flush)
     # LiDAR scan (C3), K=16, alpha 4 and alpha 8 (num_down 2 and 3)
     lo_ = torch.tensor([lx.shape[0]], device=dev)
     for nd, alpha in ((2, 4), (3, 8)):
@@ -698,6 +713,19 @@ def rows_single_gpu(fk, torch, dev, flush, peak_gbs, clouds=16):
     ms = _event_ms(torch, lambda: fk.ops.group_backward(g, idx, len(b.xyz), 64, False, gf), flush)
     rows["grouping_batch_c64_bwd"] = {"value": ms, "unit": "ms"}
     return rows
+
+
+def small_rows(args):
+    """Only the small-problem rows (the uniform cube and the DeLA hierarchy):
+    a short run for launch lists of those workloads."""
+    import torch
+
+    import flashknn_exprepo_b200 as fk
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
+    return {"rows": {"self_query_cube_k16": row_cube(fk, torch, dev, flush),
+                     "hierarchy_lidar": row_hierarchy(fk, torch, dev)}}
 
 
 def rows_only(args):
@@ -938,6 +966,9 @@ def main():
         print(json.dumps(run_reference(args)))
         return
 
+    if args.small_rows:
+        print(json.dumps(small_rows(args)))
+        return
     if args.rows_only:
         print(json.dumps(rows_only(args)))
         return
