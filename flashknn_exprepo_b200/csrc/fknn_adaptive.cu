@@ -94,6 +94,7 @@ __device__ __forceinline__ bool node_head(const uint64_t* key, int64_t p, int sh
 // ------------------------------------------------------------ boxes, keys
 
 __global__ void ka_init(Meta* meta, long long* box, uint32_t* totals, int n_totals) {
+  chain_wait();
   const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
   if (t < static_cast<int64_t>(sizeof(Meta) / sizeof(int))) reinterpret_cast<int*>(meta)[t] = 0;
@@ -119,6 +120,7 @@ __device__ __forceinline__ int batch_of(const int64_t* batch, int64_t i, int* st
 __global__ void __launch_bounds__(256)
     ka_box(const int64_t* __restrict__ grid, const int64_t* __restrict__ batch, int64_t n,
            long long* __restrict__ box, Meta* meta) {
+  chain_wait();
   __shared__ long long sh[2][6];
   int* status = &meta->status;
   const int64_t base = static_cast<int64_t>(blockIdx.x) * kTile;
@@ -190,6 +192,7 @@ __global__ void __launch_bounds__(256)
 // One CTA: top level S, key layout (bits per axis, batch bits), span check.
 __global__ void __launch_bounds__(1024)
     ka_meta(const long long* __restrict__ box, int max_shift, Meta* meta) {
+  chain_wait();
   __shared__ long long s_span[32];
   __shared__ int s_b[32];
   long long span = 0;
@@ -247,6 +250,7 @@ __global__ void __launch_bounds__(256)
     ka_keys(const int64_t* __restrict__ grid, const int64_t* __restrict__ batch, int64_t n,
             const long long* __restrict__ box, Meta* meta, uint64_t* __restrict__ keys,
             uint32_t* __restrict__ vals) {
+  chain_wait();
   const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const int b = batch_of(batch, i, &meta->status);
@@ -262,6 +266,7 @@ __global__ void __launch_bounds__(256)
     ka_records(const float* __restrict__ xyz, const int64_t* __restrict__ grid,
                const int64_t* __restrict__ batch, int64_t n, const long long* __restrict__ box,
                SortPair<uint64_t> sp, const int* bits, Meta* meta, float4* __restrict__ rec) {
+  chain_wait();
   const int64_t s = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (s >= n) return;
   const int64_t id = sorted_vals(sp, bits)[s];
@@ -294,6 +299,7 @@ struct LevelArgs {
 // 0..hb/3.  tile_counts[s * n_tiles + tile] = heads of level s in the tile.
 __global__ void __launch_bounds__(256)
     ka_heads_all(LevelArgs a, int n_tiles, uint32_t* __restrict__ tile_counts) {
+  chain_wait();
   __shared__ uint32_t hist[kMaxLevel + 1];
   if (threadIdx.x <= kMaxLevel) hist[threadIdx.x] = 0u;
   __syncthreads();
@@ -323,6 +329,7 @@ __global__ void __launch_bounds__(256)
 // level_nodes[s] = the level's node count.
 __global__ void __launch_bounds__(1024)
     ka_scan_all(uint32_t* __restrict__ tile_counts, int n_tiles, int* __restrict__ level_nodes) {
+  chain_wait();
   __shared__ uint32_t warp_sums[32];
   __shared__ uint32_t s_total;
   uint32_t* col = tile_counts + static_cast<int64_t>(blockIdx.x) * n_tiles;
@@ -408,6 +415,7 @@ __device__ __forceinline__ int* level_mask_word(Meta* m) { return &m->reserved[2
 // twice the largest possible node count.
 __global__ void ka_level_bases(const int* __restrict__ level_nodes, Meta* meta,
                                int* __restrict__ base, int64_t max_cap) {
+  chain_wait();
   if (threadIdx.x != 0) return;
   const int top = top_level(meta);
   int b = 0;
@@ -424,6 +432,7 @@ __global__ void ka_level_bases(const int* __restrict__ level_nodes, Meta* meta,
 
 __global__ void __launch_bounds__(256)
     ka_table_clear(Slot* __restrict__ slots, const Meta* meta) {
+  chain_wait();
   const int64_t cap = static_cast<int64_t>(static_cast<uint32_t>(meta->reserved[2])) + 1;
   for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < cap;
        i += static_cast<int64_t>(gridDim.x) * blockDim.x)
@@ -446,6 +455,7 @@ __global__ void __launch_bounds__(256)
     ka_nodes_all(LevelArgs a, int n_tiles, const uint32_t* __restrict__ tile_offsets,
                  const int* __restrict__ level_nodes, const int* __restrict__ base,
                  int32_t* __restrict__ node_start, int32_t* __restrict__ node_of) {
+  chain_wait();
   __shared__ uint32_t warp_sums[32];
   const int top = top_level(a.meta);
   const uint64_t* key = sorted_keys(a.sp, a.bits);
@@ -477,6 +487,7 @@ __global__ void __launch_bounds__(256)
 __global__ void __launch_bounds__(256)
     ka_insert_all(LevelArgs a, const int* __restrict__ base, const int32_t* __restrict__ node_start,
                   Slot* __restrict__ slots) {
+  chain_wait();
   const int top = top_level(a.meta);
   const uint32_t mask = static_cast<uint32_t>(a.meta->reserved[2]);
   const uint64_t* key = sorted_keys(a.sp, a.bits);
@@ -506,6 +517,7 @@ __global__ void __launch_bounds__(256)
     ka_counts_all(LevelArgs a, const int* __restrict__ base,
                   const int32_t* __restrict__ node_start, const Slot* __restrict__ slots,
                   int32_t* __restrict__ cand) {
+  chain_wait();
   const int top = top_level(a.meta);
   const uint32_t mask = static_cast<uint32_t>(a.meta->reserved[2]);
   const int bpa = a.meta->bpa;
@@ -561,6 +573,7 @@ __global__ void __launch_bounds__(256)
                   const int32_t* __restrict__ cand, int min_count, int max_count,
                   uint8_t* __restrict__ sel_out, uint8_t* __restrict__ group_flag,
                   int2* __restrict__ runs) {
+  chain_wait();
   const int top = top_level(a.meta);
   const uint32_t mask = static_cast<uint32_t>(a.meta->reserved[2]);
   const int bpa = a.meta->bpa;
@@ -600,6 +613,7 @@ __global__ void __launch_bounds__(256)
 
 __global__ void __launch_bounds__(256)
     ka_group_tiles(int64_t n, const uint8_t* __restrict__ flag, uint32_t* __restrict__ tile_counts) {
+  chain_wait();
   __shared__ uint32_t warp_sums[32];
   __shared__ uint32_t s_total;
   const int64_t base = static_cast<int64_t>(blockIdx.x) * kTile + threadIdx.x * 8;
@@ -615,6 +629,7 @@ __global__ void __launch_bounds__(256)
     ka_groups(int64_t n, const uint8_t* __restrict__ flag, const uint32_t* __restrict__ tile_offsets,
               const int* count_ptr, int32_t* __restrict__ group_start,
               int32_t* __restrict__ group_row) {
+  chain_wait();
   __shared__ uint32_t warp_sums[32];
   const int64_t base = static_cast<int64_t>(blockIdx.x) * kTile + threadIdx.x * 8;
   uint32_t bits = 0, c = 0;
@@ -642,6 +657,7 @@ __global__ void __launch_bounds__(256)
 __global__ void __launch_bounds__(256)
     ka_levels_out(int64_t n, const float4* __restrict__ rec, const uint8_t* __restrict__ sel,
                   int8_t* __restrict__ out) {
+  chain_wait();
   const int64_t p = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (p >= n) return;
   out[__float_as_int(rec[p].w)] = static_cast<int8_t>(sel[p]);
@@ -742,18 +758,18 @@ int run_adaptive(const AdaptiveArgs& f, void* ws, size_t ws_bytes, const QuerySh
   }
   int nl = 0;
   cudaError_t e;
-  ka_init<<<64, 256, 0, s>>>(b.meta, b.box, b.totals, kSortMaxPasses * 256);
-  ka_box<<<blocks_for(n, kTile), 256, 0, s>>>(f.grid, f.batch, n, b.box, b.meta);
-  ka_meta<<<1, 1024, 0, s>>>(b.box, f.max_shift, b.meta);
-  ka_keys<<<blocks_for(n, 256), 256, 0, s>>>(f.grid, f.batch, n, b.box, b.meta, b.keys[0],
-                                              b.vals[0]);
+  launch_chained(ka_init, 64, 256, 0, s, b.meta, b.box, b.totals, kSortMaxPasses * 256);
+  launch_chained(ka_box, blocks_for(n, kTile), 256, 0, s, f.grid, f.batch, n, b.box, b.meta);
+  launch_chained(ka_meta, 1, 1024, 0, s, b.box, f.max_shift, b.meta);
+  launch_chained(ka_keys, blocks_for(n, 256), 256, 0, s, f.grid, f.batch, n, b.box, b.meta,
+                 b.keys[0], b.vals[0]);
   nl += 4;
   const int* key_bits = &b.meta->key_bits;
   SortBuffers<uint64_t> sb{{b.keys[0], b.keys[1]}, {b.vals[0], b.vals[1]}, b.hist, b.totals};
   nl += launch_radix_sort(sb, n, key_bits, sort_passes_for_bits(3 * kMaxLevel + 15), s);
   const SortPair<uint64_t> sp{{b.keys[0], b.keys[1]}, {b.vals[0], b.vals[1]}};
-  ka_records<<<blocks_for(n, 256), 256, 0, s>>>(f.xyz, f.grid, f.batch, n, b.box, sp, key_bits,
-                                                b.meta, b.rec);
+  launch_chained(ka_records, blocks_for(n, 256), 256, 0, s, f.xyz, f.grid, f.batch, n, b.box, sp,
+                 key_bits, b.meta, b.rec);
   ++nl;
 
   const int tiles = blocks_for(n, kTile);
@@ -761,25 +777,25 @@ int run_adaptive(const AdaptiveArgs& f, void* ws, size_t ws_bytes, const QuerySh
   const int top_host = f.max_shift >= 0 ? f.max_shift : kMaxLevel;
   const LevelArgs la{sp, key_bits, b.meta, n, 0};
   const int64_t node_bound = static_cast<int64_t>(top_host + 1) * (n + 1);
-  ka_heads_all<<<tiles, 256, 0, s>>>(la, tiles, b.tile_counts);
-  ka_scan_all<<<kMaxLevel + 1, 1024, 0, s>>>(b.tile_counts, tiles, b.level_nodes);
-  ka_level_bases<<<1, 32, 0, s>>>(b.level_nodes, b.meta, b.level_base, b.cap);
-  ka_table_clear<<<capped_blocks(b.cap), 256, 0, s>>>(b.slots, b.meta);
-  ka_nodes_all<<<tiles, 256, 0, s>>>(la, tiles, b.tile_counts, b.level_nodes, b.level_base,
-                                     b.node_start, b.node_of);
-  ka_insert_all<<<capped_blocks(node_bound), 256, 0, s>>>(la, b.level_base, b.node_start,
-                                                          b.slots);
-  ka_counts_all<<<capped_blocks(node_bound * 32), 256, 0, s>>>(la, b.level_base, b.node_start,
-                                                               b.slots, b.cand);
-  ka_select_all<<<capped_blocks(n), 256, 0, s>>>(la, b.slots, b.node_of, b.cand, min_count,
-                                                 max_count, b.sel, b.group_flag, b.runs);
-  ka_group_tiles<<<tiles, 256, 0, s>>>(n, b.group_flag, b.tile_counts);
-  k_scan_tiles<<<1, 1024, 0, s>>>(b.tile_counts, tiles, &b.meta->n_groups);
-  ka_groups<<<tiles, 256, 0, s>>>(n, b.group_flag, b.tile_counts, &b.meta->n_groups,
-                                  b.group_start, b.group_row);
+  launch_chained(ka_heads_all, tiles, 256, 0, s, la, tiles, b.tile_counts);
+  launch_chained(ka_scan_all, kMaxLevel + 1, 1024, 0, s, b.tile_counts, tiles, b.level_nodes);
+  launch_chained(ka_level_bases, 1, 32, 0, s, b.level_nodes, b.meta, b.level_base, b.cap);
+  launch_chained(ka_table_clear, capped_blocks(b.cap), 256, 0, s, b.slots, b.meta);
+  launch_chained(ka_nodes_all, tiles, 256, 0, s, la, tiles, b.tile_counts, b.level_nodes,
+                 b.level_base, b.node_start, b.node_of);
+  launch_chained(ka_insert_all, capped_blocks(node_bound), 256, 0, s, la, b.level_base,
+                 b.node_start, b.slots);
+  launch_chained(ka_counts_all, capped_blocks(node_bound * 32), 256, 0, s, la, b.level_base,
+                 b.node_start, b.slots, b.cand);
+  launch_chained(ka_select_all, capped_blocks(n), 256, 0, s, la, b.slots, b.node_of, b.cand,
+                 min_count, max_count, b.sel, b.group_flag, b.runs);
+  launch_chained(ka_group_tiles, tiles, 256, 0, s, n, b.group_flag, b.tile_counts);
+  launch_chained(k_scan_tiles, 1, 1024, 0, s, b.tile_counts, tiles, &b.meta->n_groups);
+  launch_chained(ka_groups, tiles, 256, 0, s, n, b.group_flag, b.tile_counts, &b.meta->n_groups,
+                 b.group_start, b.group_row);
   nl += 11;
   if (f.level_out) {
-    ka_levels_out<<<blocks_for(n, 256), 256, 0, s>>>(n, b.rec, b.sel, f.level_out);
+    launch_chained(ka_levels_out, blocks_for(n, 256), 256, 0, s, n, b.rec, b.sel, f.level_out);
     ++nl;
   }
   nl += launch_items(b.runs, b.group_start, b.group_row, &b.meta->n_groups, n, shape.tile_records,

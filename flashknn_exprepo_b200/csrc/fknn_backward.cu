@@ -42,6 +42,7 @@ __global__ void __launch_bounds__(256)
                 int64_t n, const int32_t* __restrict__ idx, const float* __restrict__ dist,
                 const float* __restrict__ grad, int k, float* __restrict__ grad_q, int accumulate,
                 uint32_t* __restrict__ count, uint32_t* __restrict__ rank, int vec4) {
+  chain_wait();
   const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (i >= m) return;
   const float qx = q_xyz[3 * i], qy = q_xyz[3 * i + 1], qz = q_xyz[3 * i + 2];
@@ -95,6 +96,7 @@ __global__ void __launch_bounds__(256)
 __global__ void __launch_bounds__(kScanTile)
     k_bwd_tile_sums(const uint32_t* __restrict__ count, int64_t n,
                     uint32_t* __restrict__ tile_sums) {
+  chain_wait();
   __shared__ uint32_t warp_sums[32];
   __shared__ uint32_t s_total;
   const int64_t p = static_cast<int64_t>(blockIdx.x) * kScanTile + threadIdx.x;
@@ -108,6 +110,7 @@ __global__ void __launch_bounds__(kScanTile)
     k_bwd_starts(const uint32_t* __restrict__ count, int64_t n,
                  const uint32_t* __restrict__ tile_offsets, uint32_t* __restrict__ start,
                  uint32_t* __restrict__ cursor) {
+  chain_wait();
   __shared__ uint32_t warp_sums[32];
   const int64_t p = static_cast<int64_t>(blockIdx.x) * kScanTile + threadIdx.x;
   const uint32_t c = p < n ? count[p] : 0u;
@@ -127,6 +130,7 @@ __global__ void __launch_bounds__(256)
     k_bwd_scatter(int64_t total, const int32_t* __restrict__ idx,
                   const uint32_t* __restrict__ rank, const uint32_t* __restrict__ start,
                   uint32_t* __restrict__ seg, int vec4) {
+  chain_wait();
   const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
   auto put = [&](int64_t e, int32_t t, uint32_t r) {
     if (r == kNoEntry) return;
@@ -218,6 +222,7 @@ __global__ void __maxnreg__(96)
     k_bwd_support(const float* __restrict__ q_xyz, const float* __restrict__ p_xyz, int64_t n,
                   DivK k, const uint32_t* __restrict__ start, const uint32_t* __restrict__ seg,
                   const float* __restrict__ grad, float* __restrict__ grad_p, int accumulate) {
+  chain_wait();
   const int64_t p0 = static_cast<int64_t>(blockIdx.x) * blockDim.x;
   if (p0 >= n) return;  // whole warps leave together: n is the same for all
   const int64_t p = p0 + threadIdx.x;
@@ -310,9 +315,9 @@ size_t segment_tiles(int64_t n) { return static_cast<size_t>(ceil_div(n > 0 ? n 
 int launch_segment_starts(const uint32_t* count, int64_t n, uint32_t* tiles, int* total,
                           uint32_t* start, uint32_t* cursor, cudaStream_t s) {
   const int t = blocks_for(n, kScanTile);
-  k_bwd_tile_sums<<<t, kScanTile, 0, s>>>(count, n, tiles);
-  k_scan_tiles<<<1, 1024, 0, s>>>(tiles, t, total);
-  k_bwd_starts<<<t, kScanTile, 0, s>>>(count, n, tiles, start, cursor);
+  launch_chained(k_bwd_tile_sums, t, kScanTile, 0, s, count, n, tiles);
+  launch_chained(k_scan_tiles, 1, 1024, 0, s, tiles, t, total);
+  launch_chained(k_bwd_starts, t, kScanTile, 0, s, count, n, tiles, start, cursor);
   return 3;
 }
 
@@ -339,23 +344,22 @@ int run_backward(const BackwardArgs& a, void* ws, size_t ws_bytes, cudaStream_t 
   const auto al16 = [](const void* p) { return reinterpret_cast<uintptr_t>(p) % 16 == 0; };
   const bool vec4 = a.k % 4 == 0 && al16(a.idx) && al16(a.dist) && al16(a.grad);
   if (a.m > 0 && (a.grad_q || want_p)) {
-    k_bwd_query<<<blocks_for(a.m, 256), 256, 0, s>>>(a.q_xyz, a.m, a.p_xyz, a.n, a.idx, a.dist,
-                                                     a.grad, a.k, a.grad_q, a.accumulate,
-                                                     want_p ? b.count : nullptr,
-                                                     want_p ? b.rank : nullptr, vec4 ? 1 : 0);
+    launch_chained(k_bwd_query, blocks_for(a.m, 256), 256, 0, s, a.q_xyz, a.m, a.p_xyz, a.n, a.idx,
+                   a.dist, a.grad, a.k, a.grad_q, a.accumulate, want_p ? b.count : nullptr,
+                   want_p ? b.rank : nullptr, vec4 ? 1 : 0);
     ++nl;
   }
   if (want_p) {
     nl += launch_segment_starts(b.count, a.n, b.tiles, b.total, b.start, b.cursor, s);
     if (total > 0) {
       const int64_t sb = ceil_div(total, 256);
-      k_bwd_scatter<<<static_cast<int>(sb < 8192 ? sb : 8192), 256, 0, s>>>(
-          total, a.idx, b.rank, b.start, b.seg, vec4 ? 1 : 0);
+      launch_chained(k_bwd_scatter, static_cast<int>(sb < 8192 ? sb : 8192), 256, 0, s, total,
+                     a.idx, b.rank, b.start, b.seg, vec4 ? 1 : 0);
       ++nl;
     }
-    k_bwd_support<<<blocks_for(a.n, 128), 128, 0, s>>>(a.q_xyz, a.p_xyz, a.n,
-                                                       make_divk(static_cast<uint32_t>(a.k)), b.start,
-                                                       b.seg, a.grad, a.grad_p, a.accumulate);
+    launch_chained(k_bwd_support, blocks_for(a.n, 128), 128, 0, s, a.q_xyz, a.p_xyz, a.n,
+                   make_divk(static_cast<uint32_t>(a.k)), b.start, b.seg, a.grad, a.grad_p,
+                   a.accumulate);
     ++nl;
   }
   e = cudaGetLastError();

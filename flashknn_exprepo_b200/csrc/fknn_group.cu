@@ -54,6 +54,7 @@ __global__ void __launch_bounds__(256)
                int64_t rows, int k, const float* __restrict__ xyz,
                const float* __restrict__ new_xyz, int with_xyz, int tpr,
                float* __restrict__ out, int* status) {
+  chain_wait();
   const int off = with_xyz ? 3 : 0;
   const int cw = c + off;
   const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
@@ -96,6 +97,7 @@ __global__ void __launch_bounds__(256)
 __global__ void __launch_bounds__(256)
     kg_count(const int32_t* __restrict__ idx, int64_t total, int64_t n,
              uint32_t* __restrict__ count, int* status) {
+  chain_wait();
   for (int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; e < total;
        e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
     const int32_t t = idx[e];
@@ -106,6 +108,7 @@ __global__ void __launch_bounds__(256)
 __global__ void __launch_bounds__(256)
     kg_scatter(const int32_t* __restrict__ idx, int64_t total, int64_t n,
                uint32_t* __restrict__ cursor, uint32_t* __restrict__ seg) {
+  chain_wait();
   for (int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; e < total;
        e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
     const int32_t t = idx[e];
@@ -154,6 +157,7 @@ __global__ void __launch_bounds__(256)
     kg_support(const float* __restrict__ grad_out, int c, int with_xyz,
                const uint32_t* __restrict__ start, const uint32_t* __restrict__ seg, int64_t n,
                float* __restrict__ grad_feat, float* __restrict__ grad_xyz, int accumulate_xyz) {
+  chain_wait();
   using VT = typename Vec<V>::T;
   const int lane = threadIdx.x & 31;
   const int off = with_xyz ? 3 : 0;
@@ -221,6 +225,7 @@ __global__ void __launch_bounds__(256)
 __global__ void __launch_bounds__(256)
     kg_query(const float* __restrict__ grad_out, int c, const int32_t* __restrict__ idx,
              int64_t m, int k, int64_t n, float* __restrict__ grad_new_xyz, int accumulate) {
+  chain_wait();
   const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (i >= m) return;
   const int cw = c + 3;
@@ -304,9 +309,8 @@ int run_group_forward(const GroupArgs& g, void* ws, size_t ws_bytes, cudaStream_
       while (tpr < 32 && tpr < g.c / 4) tpr <<= 1;
     }
     const int64_t words = vec4 ? rows * tpr : rows * cw;
-    kg_forward<<<capped_blocks(words), 256, 0, s>>>(g.feat, g.n, g.c, g.idx, rows, g.k, g.xyz,
-                                                        g.new_xyz, g.with_xyz, tpr,
-                                                        g.out, &b.meta->status);
+    launch_chained(kg_forward, capped_blocks(words), 256, 0, s, g.feat, g.n, g.c, g.idx, rows, g.k,
+                   g.xyz, g.new_xyz, g.with_xyz, tpr, g.out, &b.meta->status);
     ++nl;
   }
   e = cudaGetLastError();
@@ -335,29 +339,28 @@ int run_group_backward(const GroupArgs& g, void* ws, size_t ws_bytes, cudaStream
     const int64_t eb = ceil_div(rows > 0 ? rows : 1, 256);
     const int eblocks = static_cast<int>(eb < 8192 ? eb : 8192);
     if (rows > 0) {
-      kg_count<<<eblocks, 256, 0, s>>>(g.idx, rows, g.n, b.count, &b.meta->status);
+      launch_chained(kg_count, eblocks, 256, 0, s, g.idx, rows, g.n, b.count, &b.meta->status);
       ++nl;
     }
     nl += launch_segment_starts(b.count, g.n, b.tiles, &b.meta->n_groups, b.start, b.cursor, s);
     if (rows > 0) {
-      kg_scatter<<<eblocks, 256, 0, s>>>(g.idx, rows, g.n, b.cursor, b.seg);
+      launch_chained(kg_scatter, eblocks, 256, 0, s, g.idx, rows, g.n, b.cursor, b.seg);
       ++nl;
     }
     const bool v2 = !g.with_xyz && g.c % 2 == 0 &&
                     reinterpret_cast<uintptr_t>(g.grad_out) % 8 == 0 &&
                     reinterpret_cast<uintptr_t>(g.grad_feat) % 8 == 0;
     if (v2)
-      kg_support<2><<<capped_warp_blocks(g.n), 256, 0, s>>>(g.grad_out, g.c, 0, b.start, b.seg,
-                                                            g.n, g.grad_feat, nullptr, 0);
+      launch_chained(kg_support<2>, capped_warp_blocks(g.n), 256, 0, s, g.grad_out, g.c, 0, b.start,
+                     b.seg, g.n, g.grad_feat, nullptr, 0);
     else
-      kg_support<1><<<capped_warp_blocks(g.n), 256, 0, s>>>(g.grad_out, g.c, g.with_xyz, b.start,
-                                                            b.seg, g.n, g.grad_feat, g.grad_xyz,
-                                                            g.accumulate_xyz);
+      launch_chained(kg_support<1>, capped_warp_blocks(g.n), 256, 0, s, g.grad_out, g.c, g.with_xyz,
+                     b.start, b.seg, g.n, g.grad_feat, g.grad_xyz, g.accumulate_xyz);
     ++nl;
   }
   if (g.with_xyz && g.grad_new_xyz && g.m > 0) {
-    kg_query<<<static_cast<int>(ceil_div(g.m, 256)), 256, 0, s>>>(
-        g.grad_out, g.c, g.idx, g.m, g.k, g.n, g.grad_new_xyz, g.accumulate_new_xyz);
+    launch_chained(kg_query, static_cast<int>(ceil_div(g.m, 256)), 256, 0, s, g.grad_out, g.c,
+                   g.idx, g.m, g.k, g.n, g.grad_new_xyz, g.accumulate_new_xyz);
     ++nl;
   }
   e = cudaGetLastError();

@@ -197,11 +197,11 @@ inline int launch_radix_sort(const SortBuffers<KeyT>& b, int64_t n, const int* n
   int launches = 0;
   for (int p = 0; p < max_passes; ++p) {
     const int src = p & 1, dst = src ^ 1;
-    k_sort_hist<KeyT><<<n_tiles, kSortThreads, 0, s>>>(b.keys[src], n, p, nbits, b.hist,
-                                                        b.totals, n_tiles);
-    k_sort_scan<<<256, 1024, 0, s>>>(b.hist, b.totals, n_tiles, p, nbits);
-    k_sort_scatter<KeyT><<<n_tiles, kSortThreads, 0, s>>>(
-        b.keys[src], b.vals[src], b.keys[dst], b.vals[dst], n, p, nbits, b.hist, n_tiles);
+    launch_chained(k_sort_hist<KeyT>, n_tiles, kSortThreads, 0, s, b.keys[src], n, p, nbits, b.hist,
+                   b.totals, n_tiles);
+    launch_chained(k_sort_scan, 256, 1024, 0, s, b.hist, b.totals, n_tiles, p, nbits);
+    launch_chained(k_sort_scatter<KeyT>, n_tiles, kSortThreads, 0, s, b.keys[src], b.vals[src],
+                   b.keys[dst], b.vals[dst], n, p, nbits, b.hist, n_tiles);
     launches += 3;
   }
   return launches;

@@ -26,6 +26,7 @@ __device__ __forceinline__ int ref_axis_offset(int position) {
 
 __global__ void k_morton_encode(const int64_t* __restrict__ grid, const int64_t* __restrict__ batch,
                                 int64_t n, int64_t* __restrict__ keys) {
+  chain_wait();
   const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (i >= n) return;
   keys[i] = static_cast<int64_t>(
@@ -34,6 +35,7 @@ __global__ void k_morton_encode(const int64_t* __restrict__ grid, const int64_t*
 
 __global__ void k_neighbor_keys(const int64_t* __restrict__ gd, const int64_t* __restrict__ pb,
                                 int64_t p, int64_t* __restrict__ keys) {
+  chain_wait();
   const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (t >= p * 27) return;
   const int64_t q = t / 27;
@@ -47,6 +49,7 @@ __global__ void k_neighbor_keys(const int64_t* __restrict__ gd, const int64_t* _
 // ------------------------------------------------- queries over tables
 
 __global__ void k_tab_records(const float* __restrict__ xyz, int64_t n, float4* __restrict__ rec) {
+  chain_wait();
   const int64_t s = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (s >= n) return;
   rec[s] = make_float4(xyz[3 * s], xyz[3 * s + 1], xyz[3 * s + 2],
@@ -59,6 +62,7 @@ __global__ void k_tab_records(const float* __restrict__ xyz, int64_t n, float4* 
 __global__ void k_tab_runs(const int32_t* __restrict__ steps, const int32_t* __restrict__ neigh,
                            const int32_t* __restrict__ cnt, int64_t p, Meta* meta,
                            int2* __restrict__ runs) {
+  chain_wait();
   const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (t == 0) meta->n_groups = static_cast<int>(p);
   if (t >= p * 27) return;
@@ -81,6 +85,7 @@ __global__ void k_tab_runs(const int32_t* __restrict__ steps, const int32_t* __r
 
 __global__ void k_tab_qrec(const float* __restrict__ xyz, int64_t n, const int32_t* __restrict__ qindex,
                            int64_t m, Meta* meta, float4* __restrict__ qrec) {
+  chain_wait();
   const int64_t r = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (r >= m) return;
   int64_t s = qindex[r];
@@ -95,6 +100,7 @@ __global__ void k_tab_qrec(const float* __restrict__ xyz, int64_t n, const int32
 // Separate query points (FlashKNN_Query_GM, the back-query kernels): row r
 // is qxyz[r], already grouped by the caller's steps_query.
 __global__ void k_tab_qxyz(const float* __restrict__ qxyz, int64_t m, float4* __restrict__ qrec) {
+  chain_wait();
   const int64_t r = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (r >= m) return;
   qrec[r] = make_float4(qxyz[3 * r], qxyz[3 * r + 1], qxyz[3 * r + 2],
@@ -154,16 +160,18 @@ int run_tables(const TablesArgs& t, void* ws, size_t ws_bytes, const QueryShape&
     return FKNN_ERR_CUDA;
   }
   if (t.n > 0) {
-    k_tab_records<<<blocks_for(t.n, 256), 256, 0, s>>>(t.xyz_sorted, t.n, b.srec);
+    launch_chained(k_tab_records, blocks_for(t.n, 256), 256, 0, s, t.xyz_sorted, t.n, b.srec);
     ++nl;
   }
-  k_tab_runs<<<blocks_for(t.p * 27, 256), 256, 0, s>>>(t.steps, t.neigh, t.cnt, t.p, b.meta, b.runs);
+  launch_chained(k_tab_runs, blocks_for(t.p * 27, 256), 256, 0, s, t.steps, t.neigh, t.cnt, t.p,
+                 b.meta, b.runs);
   ++nl;
   if (general && m > 0) {
-    k_tab_qxyz<<<blocks_for(m, 256), 256, 0, s>>>(t.qxyz, m, b.qrec);
+    launch_chained(k_tab_qxyz, blocks_for(m, 256), 256, 0, s, t.qxyz, m, b.qrec);
     ++nl;
   } else if (selected && m > 0) {
-    k_tab_qrec<<<blocks_for(m, 256), 256, 0, s>>>(t.xyz_sorted, t.n, t.qindex, m, b.meta, b.qrec);
+    launch_chained(k_tab_qrec, blocks_for(m, 256), 256, 0, s, t.xyz_sorted, t.n, t.qindex, m,
+                   b.meta, b.qrec);
     ++nl;
   }
   if (t.p > 0)
@@ -218,6 +226,7 @@ int run_tables(const TablesArgs& t, void* ws, size_t ws_bytes, const QueryShape&
 __global__ void k_ref_keys(const int64_t* __restrict__ grid, const int64_t* __restrict__ batch,
                            int64_t n, Meta* meta, unsigned long long* max_key,
                            uint64_t* __restrict__ keys, uint32_t* __restrict__ vals) {
+  chain_wait();
   const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   uint64_t key = 0;
   if (i < n) {
@@ -238,6 +247,7 @@ __global__ void k_ref_keys(const int64_t* __restrict__ grid, const int64_t* __re
 }
 
 __global__ void k_ref_bits(const unsigned long long* max_key, Meta* meta) {
+  chain_wait();
   const unsigned long long k = *max_key;
   meta->key_bits = k ? 64 - __clzll(static_cast<long long>(k)) : 0;
 }
@@ -246,6 +256,7 @@ __global__ void k_ref_bits(const unsigned long long* max_key, Meta* meta) {
 __global__ void __launch_bounds__(256)
     k_ref_order(int64_t n, SortPair<uint64_t> sp, const int* bits_ptr, int num_down,
                 int64_t* __restrict__ order, uint32_t* __restrict__ tile_counts) {
+  chain_wait();
   __shared__ uint32_t warp_sums[32];
   __shared__ uint32_t s_total;
   const int buf = sort_passes_for_bits(*bits_ptr) & 1;
@@ -274,6 +285,7 @@ __global__ void __launch_bounds__(256)
                   const int64_t* __restrict__ order, int32_t* __restrict__ steps,
                   int64_t* __restrict__ gd, int64_t* __restrict__ pb,
                   uint64_t* __restrict__ pkey, int64_t* __restrict__ n_parents) {
+  chain_wait();
   __shared__ uint32_t warp_sums[32];
   const uint64_t* keys = sp.key_buf(sort_passes_for_bits(*bits_ptr) & 1);
   const int64_t base = static_cast<int64_t>(blockIdx.x) * 2048 + threadIdx.x * 8;
@@ -318,6 +330,7 @@ __global__ void __launch_bounds__(256)
 __global__ void k_ref_neigh(const int64_t* __restrict__ gd, const int64_t* __restrict__ pb,
                             const uint64_t* __restrict__ pkey, const int* count_ptr,
                             int32_t* __restrict__ neigh) {
+  chain_wait();
   const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   const int p = *count_ptr;
   if (t >= static_cast<int64_t>(p) * 27) return;
@@ -337,6 +350,7 @@ __global__ void k_ref_neigh(const int64_t* __restrict__ gd, const int64_t* __res
 // cnt[p*28 + j] = exclusive prefix of the neighbour counts (FlashKnnWrapper.py:337).
 __global__ void k_ref_cnt(const int32_t* __restrict__ steps, const int32_t* __restrict__ neigh,
                           const int* count_ptr, int32_t* __restrict__ cnt) {
+  chain_wait();
   const int64_t q = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (q >= *count_ptr) return;
   int32_t acc = 0;
@@ -405,22 +419,23 @@ int run_build_tables(const BuildTablesArgs& t, void* ws, size_t ws_bytes, cudaSt
   int nl = 0;
   if (t.n > 0) {
     const int tiles = blocks_for(t.n, 2048);
-    k_ref_keys<<<blocks_for(t.n, 256), 256, 0, s>>>(t.grid, t.batch, t.n, b.meta, b.max_key,
-                                                    b.keys[0], b.vals[0]);
-    k_ref_bits<<<1, 1, 0, s>>>(b.max_key, b.meta);
+    launch_chained(k_ref_keys, blocks_for(t.n, 256), 256, 0, s, t.grid, t.batch, t.n, b.meta,
+                   b.max_key, b.keys[0], b.vals[0]);
+    launch_chained(k_ref_bits, 1, 1, 0, s, b.max_key, b.meta);
     nl += 2;
     SortBuffers<uint64_t> sb{{b.keys[0], b.keys[1]}, {b.vals[0], b.vals[1]}, b.hist, b.totals};
     nl += launch_radix_sort(sb, t.n, &b.meta->key_bits, kSortMaxPasses, s);
     const SortPair<uint64_t> sp{{b.keys[0], b.keys[1]}, {b.vals[0], b.vals[1]}};
-    k_ref_order<<<tiles, 256, 0, s>>>(t.n, sp, &b.meta->key_bits, t.num_down, t.order,
-                                      b.tile_counts);
-    k_scan_tiles<<<1, 1024, 0, s>>>(b.tile_counts, tiles, &b.meta->n_cells);
-    k_ref_parents<<<tiles, 256, 0, s>>>(t.n, sp, &b.meta->key_bits, t.num_down, b.tile_counts,
-                                        &b.meta->n_cells, t.grid, t.batch, t.order, t.steps,
-                                        b.gd, b.pb, b.pkey, t.n_parents);
-    k_ref_neigh<<<blocks_for(t.n * 27, 256), 256, 0, s>>>(b.gd, b.pb, b.pkey, &b.meta->n_cells,
-                                                          t.neigh);
-    k_ref_cnt<<<blocks_for(t.n, 256), 256, 0, s>>>(t.steps, t.neigh, &b.meta->n_cells, t.cnt);
+    launch_chained(k_ref_order, tiles, 256, 0, s, t.n, sp, &b.meta->key_bits, t.num_down, t.order,
+                   b.tile_counts);
+    launch_chained(k_scan_tiles, 1, 1024, 0, s, b.tile_counts, tiles, &b.meta->n_cells);
+    launch_chained(k_ref_parents, tiles, 256, 0, s, t.n, sp, &b.meta->key_bits, t.num_down,
+                   b.tile_counts, &b.meta->n_cells, t.grid, t.batch, t.order, t.steps, b.gd, b.pb,
+                   b.pkey, t.n_parents);
+    launch_chained(k_ref_neigh, blocks_for(t.n * 27, 256), 256, 0, s, b.gd, b.pb, b.pkey,
+                   &b.meta->n_cells, t.neigh);
+    launch_chained(k_ref_cnt, blocks_for(t.n, 256), 256, 0, s, t.steps, t.neigh, &b.meta->n_cells,
+                   t.cnt);
     nl += 5;
   } else {
     e = cudaMemsetAsync(t.steps, 0, sizeof(int32_t), s);
@@ -441,7 +456,7 @@ int run_build_tables(const BuildTablesArgs& t, void* ws, size_t ws_bytes, cudaSt
 int run_morton_encode(const int64_t* grid, const int64_t* batch, int64_t n, int64_t* keys,
                       cudaStream_t s) {
   if (n <= 0) return FKNN_OK;
-  k_morton_encode<<<blocks_for(n, 256), 256, 0, s>>>(grid, batch, n, keys);
+  launch_chained(k_morton_encode, blocks_for(n, 256), 256, 0, s, grid, batch, n, keys);
   const cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {
     note_cuda_error(e);
@@ -453,7 +468,7 @@ int run_morton_encode(const int64_t* grid, const int64_t* batch, int64_t n, int6
 int run_neighbor_keys(const int64_t* gd, const int64_t* pb, int64_t p, int64_t* keys,
                       cudaStream_t s) {
   if (p <= 0) return FKNN_OK;
-  k_neighbor_keys<<<blocks_for(p * 27, 256), 256, 0, s>>>(gd, pb, p, keys);
+  launch_chained(k_neighbor_keys, blocks_for(p * 27, 256), 256, 0, s, gd, pb, p, keys);
   const cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {
     note_cuda_error(e);

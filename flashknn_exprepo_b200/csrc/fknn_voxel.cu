@@ -52,6 +52,7 @@ __global__ void __launch_bounds__(256)
     kv_insert(const float* __restrict__ xyz, const int64_t* __restrict__ batch, int64_t n,
               float inv, Meta* meta, VoxelSlot* __restrict__ table, uint32_t mask,
               uint32_t* __restrict__ slot_of) {
+  chain_wait();
   const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   const bool valid = i < n;
   const unsigned vmask = __ballot_sync(kFull, valid);
@@ -101,6 +102,7 @@ __global__ void __launch_bounds__(256)
 __global__ void __launch_bounds__(256)
     kv_flags(int64_t n, const VoxelSlot* __restrict__ table, const uint32_t* __restrict__ slot_of,
              uint8_t* __restrict__ flag) {
+  chain_wait();
   const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (i >= n) return;
   flag[i] = (0xffffffffu - table[slot_of[i]].first) == static_cast<uint32_t>(i) ? 1 : 0;
@@ -108,6 +110,7 @@ __global__ void __launch_bounds__(256)
 
 __global__ void __launch_bounds__(256)
     kv_tiles(int64_t n, const uint8_t* __restrict__ flag, uint32_t* __restrict__ tile_counts) {
+  chain_wait();
   __shared__ uint32_t warp_sums[32];
   __shared__ uint32_t s_total;
   const int64_t base = static_cast<int64_t>(blockIdx.x) * kTile + threadIdx.x * 8;
@@ -123,6 +126,7 @@ __global__ void __launch_bounds__(256)
     kv_compact(int64_t n, const uint8_t* __restrict__ flag,
                const uint32_t* __restrict__ tile_offsets, const int* total,
                int64_t* __restrict__ out, int64_t* __restrict__ count_out) {
+  chain_wait();
   __shared__ uint32_t warp_sums[32];
   const int64_t base = static_cast<int64_t>(blockIdx.x) * kTile + threadIdx.x * 8;
   uint32_t bits = 0, c = 0;
@@ -193,14 +197,14 @@ int run_voxel_first(const VoxelArgs& v, void* ws, size_t ws_bytes, cudaStream_t 
   int nl = 0;
   if (v.n > 0) {
     const float inv = 1.0f / v.voxel;  // host FP32 division, correctly rounded
-    kv_insert<<<blocks_for(v.n, 256), 256, 0, s>>>(v.xyz, v.batch, v.n, inv, b.meta, b.table,
-                                                   static_cast<uint32_t>(b.cap - 1), b.slot_of);
+    launch_chained(kv_insert, blocks_for(v.n, 256), 256, 0, s, v.xyz, v.batch, v.n, inv, b.meta,
+                   b.table, static_cast<uint32_t>(b.cap - 1), b.slot_of);
     const int tiles = blocks_for(v.n, kTile);
-    kv_flags<<<blocks_for(v.n, 256), 256, 0, s>>>(v.n, b.table, b.slot_of, b.flag);
-    kv_tiles<<<tiles, 256, 0, s>>>(v.n, b.flag, b.tile_counts);
-    k_scan_tiles<<<1, 1024, 0, s>>>(b.tile_counts, tiles, &b.meta->n_cells);
-    kv_compact<<<tiles, 256, 0, s>>>(v.n, b.flag, b.tile_counts, &b.meta->n_cells, v.out,
-                                     v.count_out);
+    launch_chained(kv_flags, blocks_for(v.n, 256), 256, 0, s, v.n, b.table, b.slot_of, b.flag);
+    launch_chained(kv_tiles, tiles, 256, 0, s, v.n, b.flag, b.tile_counts);
+    launch_chained(k_scan_tiles, 1, 1024, 0, s, b.tile_counts, tiles, &b.meta->n_cells);
+    launch_chained(kv_compact, tiles, 256, 0, s, v.n, b.flag, b.tile_counts, &b.meta->n_cells,
+                   v.out, v.count_out);
     nl += 5;
   }
   e = cudaGetLastError();
