@@ -243,6 +243,20 @@ def test_sparse_cells_one_point_per_cell(fk, n):
     _offsets_case(fk, xyz, np.array([n]), 8, voxel, 2, q, np.array([n // 4]))
 
 
+@pytest.mark.parametrize("cells", [20000, 30000])
+def test_packer_middle_segment_lengths(fk, cells):
+    """Between 32,768 and 65,536 query groups the item packer walks
+    segments of 8 to 15 groups (4 below, 16 above), and batches of 160k and
+    240k points build their grids with 2 points per thread: two uniform
+    clouds over the same cube (about 39k and 58k occupied parent cells
+    together) still equal the oracle."""
+    rng = np.random.default_rng(31)
+    n = 8 * cells
+    xyz = rng.random((n, 3), dtype=np.float32)
+    voxel = float(np.float32(1.0 / (4.0 * cells ** (1.0 / 3.0))))
+    _offsets_case(fk, xyz, np.array([n // 3, n]), 16, voxel)
+
+
 def test_general_queries_outside_support(fk):
     rng = np.random.default_rng(11)
     a = rng.random((3000, 3), dtype=np.float32)
